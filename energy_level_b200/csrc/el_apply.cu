@@ -1,0 +1,873 @@
+// Generic fused H-apply kernel and the vector helpers used by the drivers.
+//
+// One thread handles one (row, vector) element of a block [dim][nvec]; the
+// nvec lanes of a row are adjacent, so every flip gather of a row block is a
+// contiguous nvec-element segment.  For each row the kernel
+//   - recovers the configuration code (arithmetic unranking or code table),
+//   - accumulates the delta part of the diagonal bit by bit,
+//   - gathers x[target] for every sigma^x flip whose target is in the basis
+//     (flip targets computed arithmetically or from the class tables),
+// and fuses the caller's recurrence  y = a*Hx + b*x + c*z,  acc += w*y  and
+// the FP64 dot products the drivers need (moments, alpha, beta, norms).
+// Channel semantics: channels.py:58-132 (diagonal delta n + V n n, sigma^x
+// amplitude Omega/2 into |r>, conj(Omega)/2 into |g>).
+#include "el_internal.cuh"
+
+namespace {
+
+using el::fail;
+
+template <typename S>
+struct HamArgs {
+  const S *diagV;
+  S delta[EL_MAX_SITES];
+  S up_re[EL_MAX_SITES];  // amplitude into a row whose bit k is 1: Omega/2
+  S up_im[EL_MAX_SITES];  // (into a row whose bit k is 0: conj(Omega)/2)
+};
+
+struct KArgs {
+  int64_t nvec;
+  int lognv;
+  const void *x;
+  const void *z;
+  void *y;
+  void *acc;
+  double a, b, c, w_re, w_im;
+  double *dots;
+  int want;
+  int skip_diag;
+  const void *probe;
+  double *partials;
+  unsigned int *counter;
+};
+
+template <typename S, bool C> struct Val;
+template <typename S> struct Val<S, false> {
+  S v;
+  __device__ static Val load(const void *p, int64_t i) { Val r; r.v = ((const S *)p)[i]; return r; }
+  __device__ void store(void *p, int64_t i) const { ((S *)p)[i] = v; }
+};
+template <typename S> struct Val<S, true> {
+  S re, im;
+  __device__ static Val load(const void *p, int64_t i) {
+    Val r; r.re = ((const S *)p)[2 * i]; r.im = ((const S *)p)[2 * i + 1]; return r;
+  }
+  __device__ void store(void *p, int64_t i) const { ((S *)p)[2 * i] = re; ((S *)p)[2 * i + 1] = im; }
+};
+
+// Block reduction of 4 doubles per thread into per-(vector, quantity) sums,
+// then a deterministic cross-block sum by the last block to finish.
+__device__ void reduce4(const KArgs &K, double q0, double q1, double q2, double q3) {
+  __shared__ double red[256][4];
+  __shared__ bool last;
+  const int tid = threadIdx.x;
+  red[tid][0] = q0; red[tid][1] = q1; red[tid][2] = q2; red[tid][3] = q3;
+  __syncthreads();
+  const int nv = (int)K.nvec;            // nvec divides 256
+  const int per = 256 / nv;
+  const int nout = nv * 4;
+  for (int o = tid; o < nout; o += 256) {
+    const int v = o >> 2, q = o & 3;
+    double s = 0.0;
+    for (int j = 0; j < per; ++j) s += red[v + j * nv][q];
+    K.partials[(size_t)blockIdx.x * nout + o] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(K.counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int o = tid; o < nout; o += 256) {
+    double s = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) s += __ldcg(&K.partials[(size_t)b * nout + o]);
+    K.dots[o] = s;
+  }
+  if (tid == 0) *K.counter = 0u;
+}
+
+template <typename S, bool C>
+__global__ void __launch_bounds__(256) k_apply(BasisDev B, HamArgs<S> H, KArgs K) {
+  typedef Val<S, C> V;
+  const int64_t total = B.dim * K.nvec;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const int64_t row = t >> K.lognv;
+    const int64_t v = t & (K.nvec - 1);
+    const uint64_t code = el::unrank_row(B, row);
+    const V xr = V::load(K.x, t);
+    S hre = 0, him = 0, dsum = 0;
+    for (int k = 0; k < B.n; ++k) {
+      const bool set = (code >> k) & 1ULL;
+      if (set) dsum += H.delta[k];
+      const S are = H.up_re[k];
+      const S aim = C ? (set ? H.up_im[k] : -H.up_im[k]) : S(0);
+      if (are == S(0) && aim == S(0)) continue;
+      const int64_t tg = el::flip_target(B, code, row, k);
+      if (tg < 0) continue;
+      const V xs = V::load(K.x, (tg << K.lognv) + v);
+      if constexpr (C) {
+        hre += are * xs.re - aim * xs.im;
+        him += are * xs.im + aim * xs.re;
+      } else {
+        hre += are * xs.v;
+      }
+    }
+    if (!K.skip_diag) {
+      dsum += H.diagV[row];
+      if constexpr (C) { hre += dsum * xr.re; him += dsum * xr.im; }
+      else { hre += dsum * xr.v; }
+    }
+    V yv;
+    if constexpr (C) {
+      yv.re = (S)K.a * hre + (S)K.b * xr.re;
+      yv.im = (S)K.a * him + (S)K.b * xr.im;
+      if (K.z) { const V zv = V::load(K.z, t); yv.re += (S)K.c * zv.re; yv.im += (S)K.c * zv.im; }
+      if (K.acc) {
+        V av = V::load(K.acc, t);
+        av.re += (S)K.w_re * yv.re - (S)K.w_im * yv.im;
+        av.im += (S)K.w_re * yv.im + (S)K.w_im * yv.re;
+        av.store(K.acc, t);
+      }
+    } else {
+      yv.v = (S)K.a * hre + (S)K.b * xr.v;
+      if (K.z) { const V zv = V::load(K.z, t); yv.v += (S)K.c * zv.v; }
+      if (K.acc) { V av = V::load(K.acc, t); av.v += (S)K.w_re * yv.v; av.store(K.acc, t); }
+    }
+    if (K.y) yv.store(K.y, t);
+    if (K.want) {
+      // FP32 values are widened before multiplying: the products are exact in
+      // FP64, so only the FP64 summation rounds.
+      if constexpr (C) {
+        const double xre = xr.re, xim = xr.im, yre = yv.re, yim = yv.im;
+        q0 += xre * xre + xim * xim;
+        q1 += xre * yre + xim * yim;
+        q2 += xre * yim - xim * yre;
+        q3 += yre * yre + yim * yim;
+      } else {
+        const double xd = xr.v, yd = yv.v;
+        q0 += xd * xd;
+        q1 += xd * yd;
+        q3 += yd * yd;
+        if (K.probe) q2 += yd * (double)V::load(K.probe, t).v;
+      }
+    }
+  }
+  if (K.want) reduce4(K, q0, q1, q2, q3);
+}
+
+template <typename S>
+HamArgs<S> ham_args(const el_ham *h, const S *diagV) {
+  HamArgs<S> A;
+  memset(&A, 0, sizeof A);
+  A.diagV = diagV;
+  for (int k = 0; k < h->n; ++k) {
+    A.delta[k] = (S)h->delta[k];
+    A.up_re[k] = (S)(0.5 * h->om_re[k]);
+    A.up_im[k] = (S)(0.5 * h->om_im[k]);
+  }
+  return A;
+}
+
+int ilog2(int64_t v) {
+  int l = 0;
+  while ((1LL << l) < v) ++l;
+  return l;
+}
+
+// ---------------------------------------------------------------- diagonal
+
+__global__ void k_diag_v(BasisDev B, int n, const double *__restrict__ Vg,
+                         double *out64, float *out32) {
+  extern __shared__ double Vs[];
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) Vs[i] = Vg[i];
+  __syncthreads();
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < B.dim;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t code = el::unrank_row(B, r);
+    double s = 0.0;
+    uint64_t m = code;
+    while (m) {
+      const int k = __ffsll((long long)m) - 1;
+      m &= m - 1;
+      uint64_t m2 = m;
+      while (m2) {
+        const int k2 = __ffsll((long long)m2) - 1;
+        m2 &= m2 - 1;
+        s += Vs[k * n + k2];
+      }
+    }
+    if (out64) out64[r] = s;
+    if (out32) out32[r] = (float)s;
+  }
+}
+
+template <typename S>
+__global__ void k_full_diag(BasisDev B, HamArgs<double> H, S *out) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < B.dim;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t code = el::unrank_row(B, r);
+    double d = H.diagV[r];
+    for (int k = 0; k < B.n; ++k) if ((code >> k) & 1ULL) d += H.delta[k];
+    out[r] = (S)d;
+  }
+}
+
+// Gershgorin interval: min_r (d_r - R_r), max_r (d_r + R_r).
+__global__ void k_gershgorin(BasisDev B, HamArgs<double> H, double *partials,
+                             unsigned int *counter, double *out) {
+  __shared__ double lo_s[256], hi_s[256];
+  __shared__ bool last;
+  double lo = 1e300, hi = -1e300;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < B.dim;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t code = el::unrank_row(B, r);
+    double d = H.diagV[r], R = 0.0;
+    for (int k = 0; k < B.n; ++k) {
+      if ((code >> k) & 1ULL) d += H.delta[k];
+      const double amp = sqrt(H.up_re[k] * H.up_re[k] + H.up_im[k] * H.up_im[k]);
+      if (amp == 0.0) continue;
+      if (el::flip_target(B, code, r, k) >= 0) R += amp;
+    }
+    lo = fmin(lo, d - R);
+    hi = fmax(hi, d + R);
+  }
+  lo_s[threadIdx.x] = lo;
+  hi_s[threadIdx.x] = hi;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      lo_s[threadIdx.x] = fmin(lo_s[threadIdx.x], lo_s[threadIdx.x + s]);
+      hi_s[threadIdx.x] = fmax(hi_s[threadIdx.x], hi_s[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = lo_s[0];
+    partials[2 * blockIdx.x + 1] = hi_s[0];
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double a = 1e300, b = -1e300;
+    for (unsigned i = 0; i < gridDim.x; ++i) {
+      a = fmin(a, __ldcg(&partials[2 * i]));
+      b = fmax(b, __ldcg(&partials[2 * i + 1]));
+    }
+    out[0] = a;
+    out[1] = b;
+    *counter = 0u;
+  }
+}
+
+// ------------------------------------------------------------ BLAS-like ops
+
+template <typename S, bool C>
+__global__ void k_axpby(int64_t len, double a_re, double a_im, const S *x,
+                        double b_re, double b_im, S *y, double *partials,
+                        unsigned int *counter, double *norm2) {
+  __shared__ double red[256];
+  __shared__ bool last;
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if constexpr (C) {
+      const double xr = x ? (double)x[2 * i] : 0.0, xi = x ? (double)x[2 * i + 1] : 0.0;
+      // beta == 0 must not read y: workspace may hold stale bits (NaN)
+      const bool ry = (b_re != 0.0 || b_im != 0.0);
+      const double yr = ry ? (double)y[2 * i] : 0.0, yi = ry ? (double)y[2 * i + 1] : 0.0;
+      const double r = a_re * xr - a_im * xi + b_re * yr - b_im * yi;
+      const double im = a_re * xi + a_im * xr + b_re * yi + b_im * yr;
+      const S rs = (S)r, is = (S)im;
+      y[2 * i] = rs;
+      y[2 * i + 1] = is;
+      acc += (double)rs * (double)rs + (double)is * (double)is;
+    } else {
+      const double xv = x ? (double)x[i] : 0.0;
+      const double yv = (b_re != 0.0) ? (double)y[i] : 0.0;
+      const S r = (S)(a_re * xv + b_re * yv);
+      y[i] = r;
+      acc += (double)r * (double)r;
+    }
+  }
+  if (!norm2) return;
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = red[0];
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double s = 0.0;
+    for (unsigned i = 0; i < gridDim.x; ++i) s += __ldcg(&partials[i]);
+    *norm2 = s;
+    *counter = 0u;
+  }
+}
+
+// partials[bx][j] (re, im) of <V_j, w> over the block's rows.
+constexpr int GJ = 8;
+template <typename S, bool C>
+__global__ void k_gemv_t(int64_t len, int k, const S *V, int64_t ld, const S *w,
+                         double *partials) {
+  __shared__ double red[256][2 * GJ];
+  const int j0 = blockIdx.y * GJ;
+  double accr[GJ], acci[GJ];
+#pragma unroll
+  for (int q = 0; q < GJ; ++q) { accr[q] = 0.0; acci[q] = 0.0; }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if constexpr (C) {
+      const double wr = w[2 * i], wi = w[2 * i + 1];
+#pragma unroll
+      for (int q = 0; q < GJ; ++q) {
+        if (j0 + q < k) {
+          const S *vj = V + (size_t)(j0 + q) * ld * 2;
+          const double vr = vj[2 * i], vi = vj[2 * i + 1];
+          accr[q] += vr * wr + vi * wi;
+          acci[q] += vr * wi - vi * wr;
+        }
+      }
+    } else {
+      const double wv = w[i];
+#pragma unroll
+      for (int q = 0; q < GJ; ++q)
+        if (j0 + q < k) accr[q] += (double)V[(size_t)(j0 + q) * ld + i] * wv;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < GJ; ++q) { red[threadIdx.x][2 * q] = accr[q]; red[threadIdx.x][2 * q + 1] = acci[q]; }
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int q = 0; q < 2 * GJ; ++q) red[threadIdx.x][q] += red[threadIdx.x + s][q];
+    __syncthreads();
+  }
+  if (threadIdx.x < 2 * GJ) {
+    const int q = threadIdx.x >> 1;
+    if (j0 + q < k) partials[((size_t)blockIdx.x * k + j0 + q) * 2 + (threadIdx.x & 1)] = red[0][threadIdx.x];
+  }
+}
+
+__global__ void k_sum_partials(int nparts, int k, const double *partials, double *out) {
+  for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < 2 * k; o += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < nparts; ++b) s += partials[(size_t)b * 2 * k + o];
+    out[o] = s;
+  }
+}
+
+// w -= sum_j coef_j V_j  (sub = true) or w = sum_j coef_j V_j (sub = false)
+template <typename S, bool C>
+__global__ void k_gemv_n(int64_t len, int k, const S *V, int64_t ld,
+                         const double *coef, S *w, bool sub) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double sr = 0.0, si = 0.0;
+    for (int j = 0; j < k; ++j) {
+      const double cr = coef[2 * j], ci = coef[2 * j + 1];
+      if constexpr (C) {
+        const S *vj = V + (size_t)j * ld * 2;
+        const double vr = vj[2 * i], vi = vj[2 * i + 1];
+        sr += cr * vr - ci * vi;
+        si += cr * vi + ci * vr;
+      } else {
+        sr += cr * (double)V[(size_t)j * ld + i];
+      }
+    }
+    if constexpr (C) {
+      if (sub) { w[2 * i] = (S)((double)w[2 * i] - sr); w[2 * i + 1] = (S)((double)w[2 * i + 1] - si); }
+      else { w[2 * i] = (S)sr; w[2 * i + 1] = (S)si; }
+    } else {
+      w[i] = sub ? (S)((double)w[i] - sr) : (S)sr;
+    }
+  }
+}
+
+// Gaussian start vector from a counter-based hash (Box-Muller).
+template <typename S>
+__global__ void k_fill_gauss(int64_t len, uint64_t seed, S *out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t h1 = el::counter_hash(seed, 0x5151, (uint64_t)i);
+    const uint64_t h2 = el::counter_hash(seed, 0xA7A7, (uint64_t)i);
+    const double u1 = ((h1 >> 11) + 1.0) * (1.0 / 9007199254740993.0);
+    const double u2 = (h2 >> 11) * (1.0 / 9007199254740992.0);
+    out[i] = (S)(sqrt(-2.0 * log(u1)) * cospi(2.0 * u2));
+  }
+}
+
+// Probe block [dim][nvec]; probes v >= nvalid are zero vectors.
+template <typename S>
+__global__ void k_fill_rademacher(int64_t dim, int nvec, uint64_t seed,
+                                  int64_t probe0, int nvalid, S *out) {
+  const int64_t total = dim * nvec;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = t / nvec, v = t % nvec;
+    out[t] = v < nvalid ? (S)el::rademacher(seed, (uint64_t)(probe0 + v), (uint64_t)r) : (S)0;
+  }
+}
+
+// probes_dev is [nvec][dim] int8; out is [dim][nvec]
+template <typename S>
+__global__ void k_probe_copy(int64_t dim, int nvec, const int8_t *probes, S *out) {
+  const int64_t total = dim * nvec;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = t / nvec, v = t % nvec;
+    out[t] = (S)probes[v * dim + r];
+  }
+}
+
+template <typename S>
+__global__ void k_scale(int64_t len, const double *scale, int invert_sqrt, S *x) {
+  const double s = invert_sqrt ? 1.0 / sqrt(*scale) : *scale;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = (S)((double)x[i] * s);
+}
+
+// out[k] = sum |psi_r|^2 bit_k(r) (k < n), out[n] = sum |psi_r|^2
+template <typename S, bool C>
+__global__ void k_observables(BasisDev B, const S *psi, double *partials,
+                              unsigned int *counter, double *out) {
+  __shared__ double ws[8][EL_MAX_SITES + 1];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n = B.n;
+  for (int k = threadIdx.x; k < 8 * (EL_MAX_SITES + 1); k += blockDim.x) (&ws[0][0])[k] = 0.0;
+  __syncthreads();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < B.dim; base += stride) {
+    const int64_t r = base + threadIdx.x;
+    double p = 0.0;
+    uint64_t code = 0;
+    if (r < B.dim) {
+      code = el::unrank_row(B, r);
+      if constexpr (C) { const double a = psi[2 * r], b = psi[2 * r + 1]; p = a * a + b * b; }
+      else { const double a = psi[r]; p = a * a; }
+    }
+    for (int k = 0; k <= n; ++k) {
+      double v = (k == n) ? p : (((code >> k) & 1ULL) ? p : 0.0);
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) ws[warp][k] += v;
+    }
+  }
+  __syncthreads();
+  const int nout = n + 1;
+  for (int k = threadIdx.x; k < nout; k += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += ws[w][k];
+    partials[(size_t)blockIdx.x * nout + k] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int k = threadIdx.x; k < nout; k += blockDim.x) {
+    double s = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) s += __ldcg(&partials[(size_t)b * nout + k]);
+    out[k] = s;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
+bool is_complex(int dtype) { return dtype == EL_C64 || dtype == EL_C128; }
+
+}  // namespace
+
+namespace el {
+
+int launch_apply(el_ctx *ctx, el_ham *h, const ApplyArgs &A) {
+  const int64_t nvec = A.nvec;
+  if (nvec < 1 || nvec > 256 || (nvec & (nvec - 1)))
+    return fail(ctx, EL_EINVAL, "nvec must be a power of two in [1, 256], got %lld", (long long)nvec);
+  if (!is_complex(A.dtype) && (h->complex_drive))
+    return fail(ctx, EL_EINVAL, "complex Omega needs a complex vector dtype");
+  BasisDev B = basis_dev(h->basis);
+  KArgs K;
+  K.nvec = nvec;
+  K.lognv = ilog2(nvec);
+  K.x = A.x; K.z = A.z; K.y = A.y; K.acc = A.acc;
+  K.a = A.a; K.b = A.b; K.c = A.c; K.w_re = A.w_re; K.w_im = A.w_im;
+  K.dots = A.dots;
+  K.want = A.dots ? (A.want_dots ? A.want_dots : 7) : 0;
+  K.skip_diag = A.skip_diag;
+  K.probe = A.probe;
+  K.counter = ctx->d_counter;
+  const int64_t total = h->basis->dim * nvec;
+  const int grid = grid_for(total, 256);
+  if (K.want) {
+    int rc = ensure_partials(ctx, (size_t)grid * nvec * 4);
+    if (rc) return rc;
+  }
+  K.partials = ctx->d_partials;
+  const bool single = (A.dtype == EL_F32 || A.dtype == EL_C64);
+  if (single) {
+    int rc = ham_diag32(ctx, h);
+    if (rc) return rc;
+  }
+  switch (A.dtype) {
+    case EL_F32:
+      k_apply<float, false><<<grid, 256, 0, ctx->stream>>>(B, ham_args<float>(h, h->d_diagV32), K);
+      break;
+    case EL_F64:
+      k_apply<double, false><<<grid, 256, 0, ctx->stream>>>(B, ham_args<double>(h, h->d_diagV64), K);
+      break;
+    case EL_C64:
+      k_apply<float, true><<<grid, 256, 0, ctx->stream>>>(B, ham_args<float>(h, h->d_diagV32), K);
+      break;
+    case EL_C128:
+      k_apply<double, true><<<grid, 256, 0, ctx->stream>>>(B, ham_args<double>(h, h->d_diagV64), K);
+      break;
+    default:
+      return fail(ctx, EL_EINVAL, "unknown dtype %d", A.dtype);
+  }
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_diag_v(el_ctx *ctx, el_ham *h) {
+  BasisDev B = basis_dev(h->basis);
+  const int n = h->n;
+  double *d_V = nullptr;
+  EL_CUDA_TRY(ctx, cudaMalloc(&d_V, (size_t)n * n * sizeof(double)));
+  cudaError_t e = cudaMemcpyAsync(d_V, h->Vbits.data(), (size_t)n * n * sizeof(double),
+                                  cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    k_diag_v<<<grid_for(B.dim, 256), 256, (size_t)n * n * sizeof(double), ctx->stream>>>(
+        B, n, d_V, h->d_diagV64, nullptr);
+    ctx->launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_V);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "diag_v");
+  return EL_OK;
+}
+
+__global__ void k_to_f32(int64_t len, const double *a, float *b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+int ham_diag32(el_ctx *ctx, el_ham *h) {
+  if (h->d_diagV32) return EL_OK;
+  const int64_t dim = h->basis->dim;
+  EL_CUDA_TRY(ctx, cudaMalloc(&h->d_diagV32, (size_t)dim * sizeof(float)));
+  k_to_f32<<<grid_for(dim, 256), 256, 0, ctx->stream>>>(dim, h->d_diagV64, h->d_diagV32);
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_full_diag(el_ctx *ctx, el_ham *h, int dtype, void *out) {
+  BasisDev B = basis_dev(h->basis);
+  HamArgs<double> H = ham_args<double>(h, h->d_diagV64);
+  if (dtype == EL_F64)
+    k_full_diag<double><<<grid_for(B.dim, 256), 256, 0, ctx->stream>>>(B, H, (double *)out);
+  else if (dtype == EL_F32)
+    k_full_diag<float><<<grid_for(B.dim, 256), 256, 0, ctx->stream>>>(B, H, (float *)out);
+  else
+    return fail(ctx, EL_EINVAL, "diagonal dtype must be EL_F32 or EL_F64");
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int gershgorin(el_ctx *ctx, el_ham *h, double *lo, double *hi) {
+  BasisDev B = basis_dev(h->basis);
+  HamArgs<double> H = ham_args<double>(h, h->d_diagV64);
+  const int grid = grid_for(B.dim, 256);
+  int rc = ensure_partials(ctx, (size_t)grid * 2);
+  if (rc) return rc;
+  k_gershgorin<<<grid, 256, 0, ctx->stream>>>(B, H, ctx->d_partials, ctx->d_counter, ctx->d_scalars);
+  EL_LAUNCH_CHECK(ctx);
+  EL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, 2 * sizeof(double),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  *lo = ctx->h_scalars[0];
+  *hi = ctx->h_scalars[1];
+  return EL_OK;
+}
+
+int launch_axpby(el_ctx *ctx, int dtype, int64_t len, double a_re, double a_im,
+                 const void *x, double b_re, double b_im, void *y, double *norm2_out) {
+  const int grid = grid_for(len, 256);
+  if (norm2_out) {
+    int rc = ensure_partials(ctx, (size_t)grid);
+    if (rc) return rc;
+  }
+  switch (dtype) {
+    case EL_F32: k_axpby<float, false><<<grid, 256, 0, ctx->stream>>>(len, a_re, a_im, (const float *)x, b_re, b_im, (float *)y, ctx->d_partials, ctx->d_counter, norm2_out); break;
+    case EL_F64: k_axpby<double, false><<<grid, 256, 0, ctx->stream>>>(len, a_re, a_im, (const double *)x, b_re, b_im, (double *)y, ctx->d_partials, ctx->d_counter, norm2_out); break;
+    case EL_C64: k_axpby<float, true><<<grid, 256, 0, ctx->stream>>>(len, a_re, a_im, (const float *)x, b_re, b_im, (float *)y, ctx->d_partials, ctx->d_counter, norm2_out); break;
+    case EL_C128: k_axpby<double, true><<<grid, 256, 0, ctx->stream>>>(len, a_re, a_im, (const double *)x, b_re, b_im, (double *)y, ctx->d_partials, ctx->d_counter, norm2_out); break;
+    default: return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
+  }
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_gemv_t(el_ctx *ctx, int dtype, int64_t len, int k, const void *V,
+                  int64_t ld, const void *w, double *dots_out) {
+  if (k <= 0) return EL_OK;
+  int gx = grid_for(len, 256);
+  if (gx > 296) gx = 296;
+  dim3 grid(gx, (k + GJ - 1) / GJ);
+  int rc = ensure_partials(ctx, (size_t)gx * k * 2);
+  if (rc) return rc;
+  switch (dtype) {
+    case EL_F32: k_gemv_t<float, false><<<grid, 256, 0, ctx->stream>>>(len, k, (const float *)V, ld, (const float *)w, ctx->d_partials); break;
+    case EL_F64: k_gemv_t<double, false><<<grid, 256, 0, ctx->stream>>>(len, k, (const double *)V, ld, (const double *)w, ctx->d_partials); break;
+    case EL_C64: k_gemv_t<float, true><<<grid, 256, 0, ctx->stream>>>(len, k, (const float *)V, ld, (const float *)w, ctx->d_partials); break;
+    case EL_C128: k_gemv_t<double, true><<<grid, 256, 0, ctx->stream>>>(len, k, (const double *)V, ld, (const double *)w, ctx->d_partials); break;
+    default: return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
+  }
+  EL_LAUNCH_CHECK(ctx);
+  k_sum_partials<<<(2 * k + 255) / 256, 256, 0, ctx->stream>>>(gx, k, ctx->d_partials, dots_out);
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_gemv_n_sub(el_ctx *ctx, int dtype, int64_t len, int k, const void *V,
+                      int64_t ld, const double *coef, void *w) {
+  if (k <= 0) return EL_OK;
+  const int grid = grid_for(len, 256);
+  switch (dtype) {
+    case EL_F32: k_gemv_n<float, false><<<grid, 256, 0, ctx->stream>>>(len, k, (const float *)V, ld, coef, (float *)w, true); break;
+    case EL_F64: k_gemv_n<double, false><<<grid, 256, 0, ctx->stream>>>(len, k, (const double *)V, ld, coef, (double *)w, true); break;
+    case EL_C64: k_gemv_n<float, true><<<grid, 256, 0, ctx->stream>>>(len, k, (const float *)V, ld, coef, (float *)w, true); break;
+    case EL_C128: k_gemv_n<double, true><<<grid, 256, 0, ctx->stream>>>(len, k, (const double *)V, ld, coef, (double *)w, true); break;
+    default: return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
+  }
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_gemv_n(el_ctx *ctx, int dtype, int64_t len, int k, const void *V,
+                  int64_t ld, const double *coef_dev, void *out) {
+  if (k <= 0) return EL_OK;
+  const int grid = grid_for(len, 256);
+  switch (dtype) {
+    case EL_F32: k_gemv_n<float, false><<<grid, 256, 0, ctx->stream>>>(len, k, (const float *)V, ld, coef_dev, (float *)out, false); break;
+    case EL_F64: k_gemv_n<double, false><<<grid, 256, 0, ctx->stream>>>(len, k, (const double *)V, ld, coef_dev, (double *)out, false); break;
+    case EL_C64: k_gemv_n<float, true><<<grid, 256, 0, ctx->stream>>>(len, k, (const float *)V, ld, coef_dev, (float *)out, false); break;
+    case EL_C128: k_gemv_n<double, true><<<grid, 256, 0, ctx->stream>>>(len, k, (const double *)V, ld, coef_dev, (double *)out, false); break;
+    default: return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
+  }
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_fill_gauss(el_ctx *ctx, int dtype, int64_t len, uint64_t seed, void *out) {
+  const int grid = grid_for(len, 256);
+  switch (dtype) {
+    case EL_F32: k_fill_gauss<float><<<grid, 256, 0, ctx->stream>>>(len, seed, (float *)out); break;
+    case EL_F64: k_fill_gauss<double><<<grid, 256, 0, ctx->stream>>>(len, seed, (double *)out); break;
+    case EL_C64: k_fill_gauss<float><<<grid_for(2 * len, 256), 256, 0, ctx->stream>>>(2 * len, seed, (float *)out); break;
+    case EL_C128: k_fill_gauss<double><<<grid_for(2 * len, 256), 256, 0, ctx->stream>>>(2 * len, seed, (double *)out); break;
+    default: return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
+  }
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_fill_rademacher(el_ctx *ctx, int dtype, int64_t dim, int nvec,
+                           uint64_t seed, int64_t probe0, int nvalid, void *out) {
+  const int grid = grid_for(dim * nvec, 256);
+  if (dtype == EL_F32)
+    k_fill_rademacher<float><<<grid, 256, 0, ctx->stream>>>(dim, nvec, seed, probe0, nvalid, (float *)out);
+  else if (dtype == EL_F64)
+    k_fill_rademacher<double><<<grid, 256, 0, ctx->stream>>>(dim, nvec, seed, probe0, nvalid, (double *)out);
+  else
+    return fail(ctx, EL_EINVAL, "probes need a real dtype");
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_probe_copy(el_ctx *ctx, int dtype, int64_t dim, int nvec,
+                      const int8_t *probes_dev, void *out) {
+  const int grid = grid_for(dim * nvec, 256);
+  if (dtype == EL_F32)
+    k_probe_copy<float><<<grid, 256, 0, ctx->stream>>>(dim, nvec, probes_dev, (float *)out);
+  else if (dtype == EL_F64)
+    k_probe_copy<double><<<grid, 256, 0, ctx->stream>>>(dim, nvec, probes_dev, (double *)out);
+  else
+    return fail(ctx, EL_EINVAL, "probes need a real dtype");
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_scale(el_ctx *ctx, int dtype, int64_t len, const double *scale_dev,
+                 int invert_sqrt, void *x) {
+  const int64_t n = is_complex(dtype) ? 2 * len : len;
+  const int grid = grid_for(n, 256);
+  if (dtype == EL_F32 || dtype == EL_C64)
+    k_scale<float><<<grid, 256, 0, ctx->stream>>>(n, scale_dev, invert_sqrt, (float *)x);
+  else
+    k_scale<double><<<grid, 256, 0, ctx->stream>>>(n, scale_dev, invert_sqrt, (double *)x);
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int launch_observables(el_ctx *ctx, el_ham *h, int dtype, const void *psi, double *out_dev) {
+  BasisDev B = basis_dev(h->basis);
+  const int grid = grid_for(B.dim, 256);
+  int rc = ensure_partials(ctx, (size_t)grid * (B.n + 1));
+  if (rc) return rc;
+  switch (dtype) {
+    case EL_F32: k_observables<float, false><<<grid, 256, 0, ctx->stream>>>(B, (const float *)psi, ctx->d_partials, ctx->d_counter, out_dev); break;
+    case EL_F64: k_observables<double, false><<<grid, 256, 0, ctx->stream>>>(B, (const double *)psi, ctx->d_partials, ctx->d_counter, out_dev); break;
+    case EL_C64: k_observables<float, true><<<grid, 256, 0, ctx->stream>>>(B, (const float *)psi, ctx->d_partials, ctx->d_counter, out_dev); break;
+    case EL_C128: k_observables<double, true><<<grid, 256, 0, ctx->stream>>>(B, (const double *)psi, ctx->d_partials, ctx->d_counter, out_dev); break;
+    default: return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
+  }
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+}  // namespace el
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" {
+
+int el_ham_create(el_ctx *ctx, el_basis *basis, const double *omega_re,
+                  const double *omega_im, const double *delta, int n_pairs,
+                  const int32_t *pi, const int32_t *pj, const double *V, el_ham **out) {
+  if (!ctx || !basis || !out || !omega_re || !delta) return EL_EINVAL;
+  *out = nullptr;
+  if (n_pairs < 0 || (n_pairs > 0 && (!pi || !pj || !V))) return fail(ctx, EL_EINVAL, "bad pair list");
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int n = basis->n;
+  el_ham *h = new el_ham();
+  h->basis = basis;
+  h->n = n;
+  memset(h->om_re, 0, sizeof h->om_re);
+  memset(h->om_im, 0, sizeof h->om_im);
+  memset(h->delta, 0, sizeof h->delta);
+  h->Vbits.assign((size_t)n * n, 0.0);
+  for (int p = 0; p < n_pairs; ++p) {
+    const int i = pi[p], j = pj[p];
+    if (i < 0 || j < 0 || i >= n || j >= n || i == j || !std::isfinite(V[p])) {
+      delete h;
+      return fail(ctx, EL_EINVAL, "pair %d: bad sites (%d, %d) or non-finite V", p, i, j);
+    }
+    const int qi = n - 1 - i, qj = n - 1 - j;
+    h->Vbits[(size_t)qi * n + qj] += V[p];
+    if (qi != qj) h->Vbits[(size_t)qj * n + qi] += V[p];
+  }
+  int rc = el_ham_set_drive(ctx, h, omega_re, omega_im, delta);
+  if (rc) { delete h; return rc; }
+  cudaError_t e = cudaMalloc(&h->d_diagV64, (size_t)basis->dim * sizeof(double));
+  if (e != cudaSuccess) { delete h; return el::fail(ctx, EL_ENOMEM, "cannot allocate diagonal (%s)", cudaGetErrorString(e)); }
+  rc = el::launch_diag_v(ctx, h);
+  if (rc) { el_ham_destroy(h); return rc; }
+  *out = h;
+  return EL_OK;
+}
+
+int el_ham_set_drive(el_ctx *ctx, el_ham *h, const double *omega_re,
+                     const double *omega_im, const double *delta) {
+  if (!ctx || !h || !omega_re || !delta) return EL_EINVAL;
+  const int n = h->n;
+  bool cplx = false;
+  for (int i = 0; i < n; ++i) {
+    const double ore = omega_re[i], oim = omega_im ? omega_im[i] : 0.0, d = delta[i];
+    if (!std::isfinite(ore) || !std::isfinite(oim) || !std::isfinite(d))
+      return fail(ctx, EL_EINVAL, "Om/delta must be finite");
+    const int q = n - 1 - i;
+    h->om_re[q] = ore;
+    h->om_im[q] = oim;
+    h->delta[q] = d;
+    if (oim != 0.0) cplx = true;
+  }
+  h->complex_drive = cplx;
+  return EL_OK;
+}
+
+int el_ham_diag(el_ctx *ctx, el_ham *h, int dtype, void *out) {
+  if (!ctx || !h || !out) return EL_EINVAL;
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  return el::launch_full_diag(ctx, h, dtype, out);
+}
+
+int el_ham_destroy(el_ham *h) {
+  if (!h) return EL_OK;
+  if (h->basis) cudaSetDevice(h->basis->device);
+  if (h->d_diagV64) cudaFree(h->d_diagV64);
+  if (h->d_diagV32) cudaFree(h->d_diagV32);
+  delete h;
+  return EL_OK;
+}
+
+int el_hv(el_ctx *ctx, el_ham *h, int dtype, int nvec, const void *x, void *y) {
+  if (!ctx || !h || !x || !y) return EL_EINVAL;
+  if (x == y) return el::fail(ctx, EL_EINVAL, "el_hv: x and y must not alias");
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  ApplyArgs A;
+  memset(&A, 0, sizeof A);
+  A.dtype = dtype;
+  A.nvec = nvec;
+  A.x = x;
+  A.y = y;
+  A.a = 1.0;
+  return el::launch_apply(ctx, h, A);
+}
+
+int el_hv_host(el_ctx *ctx, el_ham *h, int dtype, int nvec, const void *x_host, void *y_host) {
+  if (!ctx || !h || !x_host || !y_host) return EL_EINVAL;
+  const int es = el::dtype_size(dtype);
+  if (!es) return el::fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const size_t bytes = (size_t)h->basis->dim * nvec * es;
+  void *dx = nullptr, *dy = nullptr;
+  EL_CUDA_TRY(ctx, cudaMalloc(&dx, bytes));
+  cudaError_t e = cudaMalloc(&dy, bytes);
+  int rc = EL_OK;
+  if (e != cudaSuccess) { cudaFree(dx); return el::cuda_fail(ctx, e, "cudaMalloc"); }
+  e = cudaMemcpyAsync(dx, x_host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    rc = el_hv(ctx, h, dtype, nvec, dx, dy);
+    if (rc == EL_OK) {
+      e = cudaMemcpyAsync(y_host, dy, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+  }
+  cudaFree(dx);
+  cudaFree(dy);
+  if (rc) return rc;
+  if (e != cudaSuccess) return el::cuda_fail(ctx, e, "el_hv_host");
+  return EL_OK;
+}
+
+int el_observables(el_ctx *ctx, el_ham *h, int dtype, const void *psi,
+                   double *n_site_host, double *norm_host) {
+  if (!ctx || !h || !psi) return EL_EINVAL;
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int n = h->n;
+  int rc = el::launch_observables(ctx, h, dtype, psi, ctx->d_scalars);
+  if (rc) return rc;
+  EL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, (n + 1) * sizeof(double),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (n_site_host)
+    for (int i = 0; i < n; ++i) n_site_host[i] = ctx->h_scalars[n - 1 - i];
+  if (norm_host) *norm_host = ctx->h_scalars[n];
+  return EL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,193 @@
+/*
+ * energy_level_b200.h -- C ABI of the B200 matrix-free many-body ED library.
+ *
+ * The library applies and solves the Rydberg Hamiltonian
+ *
+ *     H = sum_i [ delta_i n_i + (Omega_i/2) sigma^x_i ] + sum_{i<j} V_ij n_i n_j
+ *
+ * (energies in cyclic MHz, times in ns, phase = 2*pi*1e-3 * E * t) on the full
+ * 2^N basis or on a constrained sector (blockade independent sets, fixed
+ * excitation number).  Basis identity follows the reference engine: site 0 is
+ * the most significant bit of a configuration code, bit = 1 means |r>, sector
+ * states are listed in ascending code order.
+ *
+ * Conventions of every entry point:
+ *   - the return value is a status code (EL_OK = 0); el_last_error() gives text;
+ *   - no C++ exception crosses the ABI and no kernel traps;
+ *   - vectors are caller-owned DEVICE pointers unless a name ends in _host;
+ *     a block of `nvec` vectors is stored row-major, [dim][nvec];
+ *   - handles and internal workspace are owned by the library;
+ *   - all work is queued on the context's stream (el_ctx_set_stream);
+ *   - a cancel flag (el_ctx_set_cancel) is polled between launches and turns
+ *     into EL_ECANCEL.
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths inside the energy-level project, src/core/manybody/...).
+ */
+#ifndef ENERGY_LEVEL_B200_H
+#define ENERGY_LEVEL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define EL_OK        0
+#define EL_EINVAL    1  /* bad argument (maps to ValueError)                    */
+#define EL_ENOMEM    2  /* allocation or memory budget (maps to MemoryError)    */
+#define EL_ENOTCONV  3  /* iteration cap reached before tolerance               */
+#define EL_ECANCEL   4  /* cancel flag observed (maps to RuntimeError 用户取消) */
+#define EL_ECUDA     5  /* CUDA runtime error (maps to RuntimeError)            */
+
+/* arithmetic types of state vectors */
+#define EL_F32   0
+#define EL_F64   1
+#define EL_C64   2
+#define EL_C128  3
+
+/* basis kinds accepted by el_basis_build */
+#define EL_BASIS_FULL      0  /* all 2^N codes                                 */
+#define EL_BASIS_BLOCKADE  1  /* independent sets of the edge list             */
+#define EL_BASIS_CHARGE    2  /* codes with popcount == k                      */
+
+/* internal layouts reported by el_basis_info */
+#define EL_LAYOUT_FULL   0  /* rank(code) = code                                */
+#define EL_LAYOUT_CHAIN  1  /* nearest-neighbour path: Zeckendorf ranking       */
+#define EL_LAYOUT_RING   2  /* nearest-neighbour cycle: two-branch Zeckendorf   */
+#define EL_LAYOUT_TABLE  3  /* general constraint: prefix/suffix class tables   */
+
+/* KPM moment modes */
+#define EL_KPM_DIRECT    0  /* mu_n from <z, T_n z>, the reference recurrence   */
+#define EL_KPM_DOUBLING  1  /* mu_2n = 2<T_n z,T_n z>-mu_0, mu_2n+1 likewise    */
+
+typedef struct el_ctx el_ctx;
+typedef struct el_basis el_basis;
+typedef struct el_ham el_ham;
+
+/* ---- library and context ------------------------------------------------ */
+
+/* Library version, major*10000 + minor*100 + patch. */
+int el_version(void);
+
+/* Create a context bound to CUDA device `device`; `stream` is a cudaStream_t
+ * (NULL = legacy default stream).  Replaces the implicit torch device setup of
+ * matrix_free.py:177-185 (torch_lanczos_ground_state) and kpm.py:48. */
+int el_ctx_create(int device, void *stream, el_ctx **out);
+int el_ctx_destroy(el_ctx *ctx);
+int el_ctx_set_stream(el_ctx *ctx, void *stream);
+/* Host flag polled between launches; nonzero -> EL_ECANCEL.  Mirrors the
+ * progress_arr[1] cancel convention of runtime.py:12-14 (check_cancel). */
+int el_ctx_set_cancel(el_ctx *ctx, const volatile int32_t *flag);
+/* Text of the last error on this context (empty string when none). */
+const char *el_last_error(const el_ctx *ctx);
+/* Number of kernels this context has launched since creation. */
+int64_t el_ctx_launches(const el_ctx *ctx);
+
+/* ---- basis ---------------------------------------------------------------- */
+
+/* Build a basis of `n` sites (1 <= n <= 63).  kind = EL_BASIS_FULL (n <= 34),
+ * EL_BASIS_BLOCKADE with `n_edges` pairs in `edges` (host, 2*n_edges int32,
+ * validated like basis.py:12-21 validate_edges), or EL_BASIS_CHARGE with
+ * excitation number k.  `max_states` <= 0 means no cap; otherwise a larger
+ * sector fails with EL_EINVAL like basis.py:38-39.
+ * Replaces basis.py:24-47 independent_states, matrix_free.py:12-38
+ * number_sector_basis and hamiltonian_plan.py:129-148 build_plan (states). */
+int el_basis_build(el_ctx *ctx, int n, const int32_t *edges, int n_edges,
+                   int kind, int k, int64_t max_states, el_basis **out);
+/* Dimension and internal layout (EL_LAYOUT_*). */
+int el_basis_info(const el_basis *basis, int64_t *dim, int *layout);
+/* Write the ascending code list (device uint64[dim]).  Bit-exact with the
+ * reference's state lists (basis.py:24-47, matrix_free.py:12-38). */
+int el_basis_codes(el_ctx *ctx, el_basis *basis, uint64_t *codes);
+/* rank[i] = index of codes[i] in the basis or -1 (device arrays).  Replaces
+ * the position table / searchsorted of channels.py:177-192. */
+int el_basis_rank(el_ctx *ctx, el_basis *basis, const uint64_t *codes,
+                  int64_t count, int64_t *ranks);
+int el_basis_destroy(el_basis *basis);
+
+/* ---- Hamiltonian ---------------------------------------------------------- */
+
+/* Create H on `basis`.  omega_re/omega_im/delta are per-site host arrays of
+ * length n (omega_im may be NULL); pairs (pi[p], pj[p], V[p]) are the I1
+ * density-density couplings.  Channel semantics follow channels.py:58-132
+ * (diagonal delta n + V n n; sigma^x amplitude Omega/2 for g->r and
+ * conj(Omega)/2 for r->g).  Replaces channels.py:91-132 channel_spec and the
+ * diagonal of channels.py:58-77. */
+int el_ham_create(el_ctx *ctx, el_basis *basis, const double *omega_re,
+                  const double *omega_im, const double *delta, int n_pairs,
+                  const int32_t *pi, const int32_t *pj, const double *V,
+                  el_ham **out);
+/* Replace the drive (per-site Omega and delta), keeping basis and V.  Used per
+ * piecewise-constant segment, replacing the per-segment CSR rebuild of
+ * engine_ed.py:141-144. */
+int el_ham_set_drive(el_ctx *ctx, el_ham *ham, const double *omega_re,
+                     const double *omega_im, const double *delta);
+/* Full diagonal d(s) = sum delta_i n_i + sum V_ij n_i n_j into a device array
+ * of type dtype (EL_F32 or EL_F64).  Replaces channels.py:58-77. */
+int el_ham_diag(el_ctx *ctx, el_ham *ham, int dtype, void *out);
+int el_ham_destroy(el_ham *ham);
+
+/* ---- apply ------------------------------------------------------------------ */
+
+/* y = H x for a block of nvec vectors (nvec in 1,2,4,8,16,32 or a multiple of
+ * 32).  Device pointers.  Replaces channels.py:210-221 ChannelKernel.matvec and
+ * the index_select/index_add_ action of matrix_free.py:200-204. */
+int el_hv(el_ctx *ctx, el_ham *ham, int dtype, int nvec, const void *x,
+          void *y);
+/* Same product with HOST buffers: copies in, applies, copies out.  The
+ * reference-facing form of matrix_free.py:51-62 hamiltonian_linear_operator. */
+int el_hv_host(el_ctx *ctx, el_ham *ham, int dtype, int nvec,
+               const void *x_host, void *y_host);
+
+/* ---- spectral bounds and KPM --------------------------------------------- */
+
+/* Extremal eigenvalues by FP64 Lanczos from a seeded start vector.  Replaces
+ * kpm.py:82-97 _bounds (ARPACK eigsh SA/LA). */
+int el_bounds(el_ctx *ctx, el_ham *ham, int max_iter, double tol,
+              uint64_t seed, double *emin, double *emax);
+/* Chebyshev moments mu[0..num] of Htil = (H - c)/r from nvec Rademacher
+ * probes processed `chunk` at a time (chunk in 1,2,4,8,16,32 or multiple of
+ * 32).  probes_host: NULL = counter-based probes from `seed`, else int8
+ * [nvec][dim] of +-1.  dtype EL_F32 or EL_F64 (vectors); moments are always
+ * accumulated in FP64.  mu[n] = sum_probes <z, T_n z> / (nvec * dim).
+ * Replaces kpm.py:26-75 kpm_moments_gpu and kpm.py:115-151 kpm_moments. */
+int el_kpm_moments(el_ctx *ctx, el_ham *ham, int dtype, int num, int nvec,
+                   int chunk, uint64_t seed, const int8_t *probes_host,
+                   int mode, double c, double r, double *mu_host);
+
+/* ---- Lanczos ground state ------------------------------------------------- */
+
+/* Lowest `nev` (1 or 2) eigenpairs by three-term Lanczos with FP64 alpha/beta,
+ * partial (omega-recurrence) or full reorthogonalisation (`reorth` 1 or 2;
+ * 0 = none), host tridiagonal eigensolve, explicit restarts.  Vectors in
+ * dtype (EL_F32/EL_F64 for real H, EL_C64/EL_C128 for complex Omega).
+ * v0: device start vector or NULL (seeded Gaussian).  evals/residuals: host
+ * [nev]; residual = ||H x - theta x|| of the returned Ritz vector.
+ * vec_out: device [dim] ground Ritz vector or NULL.
+ * Replaces matrix_free.py:118-286 torch_lanczos_ground_state and
+ * equilibrium.py:35-96 ground_state (eigsh 'SA'). */
+int el_lanczos_ground(el_ctx *ctx, el_ham *ham, int dtype, const void *v0,
+                      uint64_t seed, int max_iter, int max_restarts,
+                      double tol, int nev, int reorth, double *evals,
+                      double *residuals, int *iters, int *converged,
+                      void *vec_out);
+
+/* ---- time evolution ------------------------------------------------------- */
+
+/* psi <- exp(-i 2pi 1e-3 H tau_ns) psi by a Chebyshev expansion truncated at
+ * `tol` (dtype EL_C64 or EL_C128).  *n_terms returns the number of terms.
+ * Replaces the expm_multiply step of engine_ed.py:125 and engine_ed.py:145. */
+int el_cheb_step(el_ctx *ctx, el_ham *ham, int dtype, void *psi,
+                 double tau_ns, double tol, int *n_terms);
+/* Site occupations <n_i> (host double[n]) and squared norm of psi.  Replaces
+ * the bits @ |psi|^2 reduction of engine_ed.py:259-263 (_reduce). */
+int el_observables(el_ctx *ctx, el_ham *ham, int dtype, const void *psi,
+                   double *n_site_host, double *norm_host);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ENERGY_LEVEL_B200_H */

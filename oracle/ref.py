@@ -1,0 +1,270 @@
+"""numpy restatement of the reference's ED algorithms -- TEST INFRASTRUCTURE ONLY.
+
+Used by tests, ``__graft_entry__.smoke()`` and the CPU baseline of
+``bench.py`` as the checker; never imported by the product package.
+Conventions (reference src/core/manybody/basis.py:1-9, channels.py:12-14):
+site 0 is the most significant bit of a code, bit 1 means |r>, H[t, s] =
+<t|H|s>, energies in cyclic MHz, CONV = 2 pi 1e-3 (evolve_util.py:12).
+Pinned by tests/golden (fixtures written by the reference itself).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+CONV = 2 * np.pi * 1e-3
+
+
+# ------------------------------------------------------------------ basis
+
+def basis_bits(n, states):
+    """(n, dim) int8 bits, row i = site i (basis.py:6-9)."""
+    states = np.asarray(states, dtype=np.int64)
+    return np.asarray([((states >> (int(n) - 1 - i)) & 1) for i in range(int(n))], dtype=np.int8)
+
+
+def validate_edges(n, edges):
+    """Sorted unique (i<j) edges; errors as basis.py:12-21."""
+    out = set()
+    for e in edges or []:
+        if len(e) != 2 or any(isinstance(i, (bool, np.bool_)) or int(i) != i for i in e):
+            raise ValueError('blockade edge must be two integers')
+        i, j = map(int, e)
+        if not 0 <= i < n or not 0 <= j < n or i == j:
+            raise ValueError('blockade edge out of range or self loop: %r' % (e,))
+        out.add(tuple(sorted((i, j))))
+    return sorted(out)
+
+
+def independent_states(n, edges, max_states=1 << 20):
+    """Ascending codes of the independent sets (basis.py:24-47).
+
+    The reference walks a DFS that tries 'site empty' before 'site occupied';
+    with site 0 as the most significant bit its leaves come out in ascending
+    code order, which is what this site-by-site numpy expansion plus a sort
+    produces."""
+    n = int(n)
+    edges = validate_edges(n, edges)
+    earlier = [0] * n   # code bits of already placed neighbours of site i
+    for i, j in edges:
+        a, b = min(i, j), max(i, j)
+        earlier[b] |= 1 << (n - 1 - a)
+    codes = np.zeros(1, np.int64)
+    for i in range(n):
+        bit = np.int64(1) << (n - 1 - i)
+        ok = (codes & np.int64(earlier[i])) == 0
+        codes = np.concatenate((codes, codes[ok] | bit))
+    codes.sort()
+    if max_states and codes.size > int(max_states):
+        raise ValueError('restricted basis dimension exceeds max_states=%d' % max_states)
+    return codes
+
+
+def number_sector_basis(n, k):
+    """Ascending codes with popcount k (matrix_free.py:12-38)."""
+    n, k = int(n), int(k)
+    if not 0 <= n <= 63 or not 0 <= k <= n:
+        raise ValueError('charge_sector out of range')
+    codes = np.zeros(1, np.int64)
+    counts = np.zeros(1, np.int8)
+    for i in range(n):
+        new = codes | (np.int64(1) << i)
+        cnew = counts + 1
+        keep = cnew <= k
+        codes = np.concatenate((codes, new[keep]))
+        counts = np.concatenate((counts, cnew[keep]))
+    out = codes[counts == k]
+    out.sort()
+    return out
+
+
+def fib(i):
+    a, b = 0, 1
+    for _ in range(i):
+        a, b = b, a + b
+    return a
+
+
+# ------------------------------------------------------------ Hamiltonian
+
+def diagonal(n, codes, delta, pairs):
+    """d(s) = sum delta_i n_i + sum V_ij n_i n_j (channels.py:58-77, real case)."""
+    bits = basis_bits(n, codes).astype(np.float64)
+    d = np.zeros(bits.shape[1])
+    for i in range(n):
+        d += float(delta[i]) * bits[i]
+    for i, j, V in pairs:
+        d += float(V) * bits[int(i)] * bits[int(j)]
+    return d
+
+
+def hv(n, codes, omega, delta, pairs, x):
+    """y = H x on the full (codes=None) or restricted basis.
+
+    Follows ChannelKernel.matvec (channels.py:210-221) with the channel list of
+    channel_spec (channels.py:114-118): a source with site i in |g> feeds the
+    target code^mask with Omega_i/2, a source in |r> with conj(Omega_i)/2;
+    targets outside a restricted basis are dropped (channels.py:177-192)."""
+    n = int(n)
+    full = codes is None
+    codes = np.arange(1 << n, dtype=np.int64) if full else np.asarray(codes, np.int64)
+    x = np.asarray(x)
+    vec = x.ndim == 1
+    X = x.reshape(len(codes), -1)
+    d = diagonal(n, codes, delta, pairs)
+    cplx = np.iscomplexobj(X) or np.any(np.asarray(omega).imag != 0)
+    Y = (d[:, None] * X).astype(complex if cplx else X.dtype)
+    if not full:
+        order = np.argsort(codes)
+        sc = codes[order]
+    om = np.asarray(omega, complex)
+    for i in range(n):
+        if om[i] == 0:
+            continue
+        mask = np.int64(1) << (n - 1 - i)
+        bit = (codes >> (n - 1 - i)) & 1
+        targets = codes ^ mask
+        if full:
+            loc = targets
+            ok = np.ones(len(codes), bool)
+        else:
+            pos = np.searchsorted(sc, targets)
+            ok = pos < len(sc)
+            ok[ok] &= sc[pos[ok]] == targets[ok]
+            loc = np.zeros(len(codes), np.int64)
+            loc[ok] = order[pos[ok]]
+        amp = np.where(bit == 0, om[i] / 2.0, np.conj(om[i]) / 2.0)
+        if not cplx:
+            amp = amp.real
+        src = np.flatnonzero(ok)
+        np.add.at(Y, loc[src], amp[src, None] * X[src])
+    return Y.reshape(x.shape) if vec else Y
+
+
+def dense_h(n, codes, omega, delta, pairs):
+    """Dense H by applying hv to unit vectors (small systems only)."""
+    dim = (1 << n) if codes is None else len(codes)
+    cplx = np.any(np.asarray(omega).imag != 0)
+    E = np.eye(dim, dtype=complex if cplx else float)
+    return hv(n, codes, omega, delta, pairs, E)
+
+
+# ------------------------------------------------------------------- KPM
+
+def kpm_bounds(H):
+    """emin, emax, c, r (kpm.py:82-97; dense eigvalsh replaces eigsh here)."""
+    w = np.linalg.eigvalsh(H)
+    emin, emax = float(w[0]), float(w[-1])
+    c = 0.5 * (emin + emax)
+    r = 0.5 * (emax - emin) * (1.0 + 1e-3) + 1e-12
+    return emin, emax, c, r
+
+
+def kpm_moments(apply_h, dim, num, probes, c, r):
+    """Hutchinson moments (kpm.py:133-151): T0 z = z, T1 z = Htil z,
+    T_n z = 2 Htil T_{n-1} z - T_{n-2} z, acc[n] += Re <T_n z, z>,
+    mu = acc / (nvec * D)."""
+    probes = np.asarray(probes, dtype=np.float64)
+    acc = np.zeros(num + 1)
+    def htil(v):
+        return (apply_h(v) - c * v) / r
+    for z in probes:
+        tp = z.copy()
+        tc = htil(z)
+        acc[0] += tp @ z
+        if num >= 1:
+            acc[1] += tc @ z
+        for k in range(2, num + 1):
+            tn = 2 * htil(tc) - tp
+            acc[k] += tn @ z
+            tp, tc = tc, tn
+    return acc / (len(probes) * dim)
+
+
+def kpm_moments_exact(H, num, c, r):
+    """Exact moments mu_n = mean T_n(lambda) (kpm.py:122-132)."""
+    lam = (np.linalg.eigvalsh(H) - c) / r
+    mu = np.zeros(num + 1)
+    t0 = np.ones_like(lam)
+    t1 = lam.copy()
+    mu[0] = t0.mean()
+    if num >= 1:
+        mu[1] = t1.mean()
+    for k in range(2, num + 1):
+        t2 = 2 * lam * t1 - t0
+        mu[k] = t2.mean()
+        t0, t1 = t1, t2
+    return mu
+
+
+def jackson_kernel(num):
+    """Jackson damping factors (kpm.py:109-112)."""
+    k = np.arange(num + 1)
+    return ((num - k + 1) * np.cos(np.pi * k / (num + 1))
+            + np.sin(np.pi * k / (num + 1)) / np.tan(np.pi / (num + 1))) / (num + 1)
+
+
+def dos_from_moments(mu, c, r, energies, num, use_jackson=True):
+    """Jackson-damped Chebyshev DOS (kpm.py:182-189)."""
+    x = (np.asarray(energies, float) - c) / r
+    xn = np.clip(x, -1 + 1e-9, 1 - 1e-9)
+    G = jackson_kernel(num) if use_jackson else np.ones(num + 1)
+    series = mu[0] * np.ones_like(xn)
+    if num >= 1:
+        t0 = np.ones_like(xn)
+        t1 = xn.copy()
+        series += 2 * G[1] * mu[1] * t1
+        for k in range(2, num + 1):
+            t2 = 2 * xn * t1 - t0
+            series += 2 * G[k] * mu[k] * t2
+            t0, t1 = t1, t2
+    return np.maximum(series / (np.pi * np.sqrt(1 - xn ** 2)) / r, 0.0)
+
+
+# ------------------------------------------------------------ evolution
+
+def segment_intervals(a, b, segments):
+    """Split [a, b] at drive boundaries (runtime.py:56-60)."""
+    bounds = [float(a)] + sorted({float(s['t0']) for s in segments or []
+                                  if a < float(s['t0']) < b}) + [float(b)]
+    return list(zip(bounds[:-1], bounds[1:]))
+
+
+def segment_drive(t, segments, n):
+    """Latest segment with t0 <= t, 'left' rule (runtime.py:90-114)."""
+    ordered = sorted(segments, key=lambda s: float(s['t0']))
+    idx = 0
+    for k, s in enumerate(ordered):
+        if float(s['t0']) <= t:
+            idx = k
+    s = ordered[idx]
+    om = np.asarray(s.get('Om', np.zeros(n)), float).reshape(-1)
+    ph = np.asarray(s.get('phase', np.zeros(n)), float).reshape(-1)
+    de = np.asarray(s.get('delta', np.zeros(n)), float).reshape(-1)
+    return om * np.exp(1j * ph), de
+
+
+def evolve_segments(n, codes, pairs, segments, psi0, t_grid):
+    """Piecewise-constant exact propagation (engine_ed.py:130-147): for each
+    output interval and each drive piece, psi <- expm_multiply(-i CONV dt H)."""
+    import scipy.sparse as sp
+    from scipy.sparse.linalg import expm_multiply
+    psi = np.asarray(psi0, complex).copy()
+    t = np.asarray(t_grid, float)
+    out = [psi.copy()]
+    cache = {}
+    for k in range(1, len(t)):
+        for a, b in segment_intervals(t[k - 1], t[k], segments):
+            om, de = segment_drive(0.5 * (a + b), segments, n)
+            key = (tuple(om), tuple(de))
+            if key not in cache:
+                cache[key] = sp.csr_matrix(dense_h(n, codes, om, de, pairs))
+            psi = expm_multiply((-1j * CONV * (b - a)) * cache[key], psi)
+        out.append(psi.copy())
+    return out
+
+
+def site_occupations(n, codes, psi):
+    """<n_i> = bits @ |psi|^2 (engine_ed.py:259-263)."""
+    codes = np.arange(1 << n) if codes is None else codes
+    p = np.abs(np.asarray(psi)) ** 2
+    return basis_bits(n, codes).astype(float) @ p

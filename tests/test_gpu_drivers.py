@@ -1,0 +1,108 @@
+"""GPU parity of the Krylov, KPM and Chebyshev drivers against the oracle."""
+import numpy as np
+import pytest
+
+from oracle import ref
+from energy_level_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+
+def _chain_model(n, seed=3):
+    rng = np.random.default_rng(seed)
+    om = rng.uniform(0.5, 2.0, n)
+    de = rng.uniform(-2, 2, n)
+    pairs = configs.pairs_from_positions(configs.chain_positions(n, jitter=rng.uniform(-0.4, 0.4, n)))
+    return om, de, pairs
+
+
+@pytest.mark.parametrize("kind", ["full", "chain", "ring"])
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-9), ("float32", 2e-5), ("complex128", 1e-9)])
+def test_lanczos_ground_matches_dense(ctx, kind, dtype, tol):
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import solvers
+    n = 10
+    om, de, pairs = _chain_model(n)
+    edges = {"full": None, "chain": configs.chain_edges(n), "ring": configs.ring_edges(n)}[kind]
+    b = Basis(ctx, n, kind="full" if kind == "full" else "blockade", edges=edges)
+    h = Hamiltonian(ctx, b, om, de, pairs)
+    codes = None if kind == "full" else ref.independent_states(n, edges, None)
+    w = np.linalg.eigvalsh(ref.dense_h(n, codes, om, de, pairs))
+    r = solvers.lanczos_ground(h, dtype=dtype, tol=tol, nev=2)
+    assert r["converged"]
+    scale = max(1.0, abs(w[0]))
+    etol = 1e-9 if dtype != "float32" else 1e-6
+    assert abs(r["evals"][0] - w[0]) <= etol * scale
+    assert abs(r["evals"][1] - w[1]) <= 10 * etol * scale
+
+
+def test_chain12_ground_energy(ctx):
+    """Workload chain12 (open chain N=12, full basis, FP64, tol 1e-12)."""
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import solvers
+    cfg = configs.chain12()
+    b = Basis(ctx, cfg["n"], kind="full")
+    pairs = [(p["i"], p["j"], p["V"]) for p in cfg["calib"]["pairs"]]
+    h = Hamiltonian(ctx, b, cfg["Om"], cfg["delta"], pairs)
+    r = solvers.lanczos_ground(h, dtype="float64", tol=1e-12, nev=2, max_iter=400)
+    assert r["converged"]
+    # reference eigsh / dense eigh value (energies in cyclic MHz)
+    assert abs(r["evals"][0] - (-10.2963231346414)) < 1e-9
+    assert abs((r["evals"][1] - r["evals"][0]) - 0.840389) < 1e-5
+
+
+@pytest.mark.parametrize("mode", ["direct", "doubling"])
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-10), ("float32", 2e-4)])
+def test_kpm_moments_match_oracle(ctx, mode, dtype, tol):
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import solvers
+    n = 8
+    om, de, pairs = _chain_model(n, 5)
+    b = Basis(ctx, n, kind="full")
+    h = Hamiltonian(ctx, b, om, de, pairs)
+    H = ref.dense_h(n, None, om, de, pairs)
+    emin, emax, c, r = ref.kpm_bounds(H)
+    rng = np.random.default_rng(3)
+    nvec, num = 6, 64
+    z = rng.choice(np.array([-1.0, 1.0]), size=(nvec, 1 << n))
+    want = ref.kpm_moments(lambda v: H @ v, 1 << n, num, z, c, r)
+    got = solvers.kpm_moments(h, num, nvec, c, r, dtype=dtype, chunk=4, probes=z, mode=mode)
+    assert np.abs(got - want).max() < tol
+
+
+def test_bounds_match_dense(ctx):
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import solvers
+    n = 10
+    om, de, pairs = _chain_model(n, 6)
+    b = Basis(ctx, n, kind="full")
+    h = Hamiltonian(ctx, b, om, de, pairs)
+    w = np.linalg.eigvalsh(ref.dense_h(n, None, om, de, pairs))
+    lo, hi = solvers.bounds(h, max_iter=400, tol=1e-13)
+    assert abs(lo - w[0]) < 1e-8 and abs(hi - w[-1]) < 1e-8
+
+
+@pytest.mark.parametrize("dtype,tol", [("complex128", 1e-9), ("complex64", 2e-5)])
+def test_cheb_evolution_matches_expm(ctx, dtype, tol):
+    import torch
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import solvers
+    n = 10
+    edges = configs.chain_edges(n)
+    om, de, pairs = _chain_model(n, 7)
+    codes = ref.independent_states(n, edges, None)
+    b = Basis(ctx, n, kind="blockade", edges=edges)
+    h = Hamiltonian(ctx, b, om, de, pairs)
+    rng = np.random.default_rng(2)
+    psi0 = rng.normal(size=len(codes)) + 1j * rng.normal(size=len(codes))
+    psi0 /= np.linalg.norm(psi0)
+    import scipy.linalg as sla
+    H = ref.dense_h(n, codes, om, de, pairs)
+    want = sla.expm(-1j * ref.CONV * 37.0 * H) @ psi0
+    psi = torch.as_tensor(psi0, dtype=getattr(torch, dtype), device=ctx.device)
+    solvers.cheb_step(h, psi, 37.0, tol=1e-13 if dtype == "complex128" else 1e-7)
+    got = psi.cpu().numpy()
+    assert np.abs(got - want).max() < tol
+    ns, nrm = solvers.observables(h, psi)
+    assert abs(nrm - 1.0) < 10 * tol
+    assert np.allclose(ns, ref.site_occupations(n, codes, want), atol=10 * tol)
