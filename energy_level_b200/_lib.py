@@ -22,6 +22,7 @@ EL_F32, EL_F64, EL_C64, EL_C128 = range(4)
 EL_BASIS_FULL, EL_BASIS_BLOCKADE, EL_BASIS_CHARGE = range(3)
 EL_LAYOUT_FULL, EL_LAYOUT_CHAIN, EL_LAYOUT_RING, EL_LAYOUT_TABLE = range(4)
 EL_KPM_DIRECT, EL_KPM_DOUBLING = range(2)
+EL_KPM_GENERIC_KERNEL = 0x100
 
 DTYPES = {"float32": EL_F32, "float64": EL_F64, "complex64": EL_C64, "complex128": EL_C128}
 
@@ -41,6 +42,7 @@ PROTOTYPES = {
     "el_ctx_set_cancel": (C.c_int, [_vp, _vp]),
     "el_last_error": (C.c_char_p, [_vp]),
     "el_ctx_launches": (_i64, [_vp]),
+    "el_ctx_bytes": (C.c_int, [_vp, C.POINTER(_i64), C.POINTER(_i64)]),
     "el_basis_build": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_vp)]),
     "el_basis_info": (C.c_int, [_vp, C.POINTER(_i64), _ip]),
     "el_basis_codes": (C.c_int, [_vp, _vp, _vp]),

@@ -56,6 +56,14 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.el_ctx_launches(self.handle))
 
+    @property
+    def copied_bytes(self):
+        """(host->device, device->host) bytes copied by the library so far."""
+        a = C.c_int64()
+        b = C.c_int64()
+        check(self.lib.el_ctx_bytes(self.handle, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
     def call(self, name, *args):
         self.sync_stream()
         rc = getattr(self.lib, name)(self.handle, *args)

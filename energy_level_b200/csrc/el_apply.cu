@@ -545,8 +545,7 @@ int launch_diag_v(el_ctx *ctx, el_ham *h) {
   const int n = h->n;
   double *d_V = nullptr;
   EL_CUDA_TRY(ctx, cudaMalloc(&d_V, (size_t)n * n * sizeof(double)));
-  cudaError_t e = cudaMemcpyAsync(d_V, h->Vbits.data(), (size_t)n * n * sizeof(double),
-                                  cudaMemcpyHostToDevice, ctx->stream);
+  cudaError_t e = el::copy(ctx, d_V, h->Vbits.data(), (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     k_diag_v<<<grid_for(B.dim, 256), 256, (size_t)n * n * sizeof(double), ctx->stream>>>(
         B, n, d_V, h->d_diagV64, nullptr);
@@ -595,8 +594,7 @@ int gershgorin(el_ctx *ctx, el_ham *h, double *lo, double *hi) {
   if (rc) return rc;
   k_gershgorin<<<grid, 256, 0, ctx->stream>>>(B, H, ctx->d_partials, ctx->d_counter, ctx->d_scalars);
   EL_LAUNCH_CHECK(ctx);
-  EL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, 2 * sizeof(double),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
+  EL_CUDA_TRY(ctx, el::copy(ctx, ctx->h_scalars, ctx->d_scalars, 2 * sizeof(double), cudaMemcpyDeviceToHost));
   EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   *lo = ctx->h_scalars[0];
   *hi = ctx->h_scalars[1];
@@ -839,11 +837,11 @@ int el_hv_host(el_ctx *ctx, el_ham *h, int dtype, int nvec, const void *x_host, 
   cudaError_t e = cudaMalloc(&dy, bytes);
   int rc = EL_OK;
   if (e != cudaSuccess) { cudaFree(dx); return el::cuda_fail(ctx, e, "cudaMalloc"); }
-  e = cudaMemcpyAsync(dx, x_host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  e = el::copy(ctx, dx, x_host, bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     rc = el_hv(ctx, h, dtype, nvec, dx, dy);
     if (rc == EL_OK) {
-      e = cudaMemcpyAsync(y_host, dy, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+      e = el::copy(ctx, y_host, dy, bytes, cudaMemcpyDeviceToHost);
       if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     }
   }
@@ -861,8 +859,7 @@ int el_observables(el_ctx *ctx, el_ham *h, int dtype, const void *psi,
   const int n = h->n;
   int rc = el::launch_observables(ctx, h, dtype, psi, ctx->d_scalars);
   if (rc) return rc;
-  EL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, (n + 1) * sizeof(double),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
+  EL_CUDA_TRY(ctx, el::copy(ctx, ctx->h_scalars, ctx->d_scalars, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost));
   EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (n_site_host)
     for (int i = 0; i < n; ++i) n_site_host[i] = ctx->h_scalars[n - 1 - i];

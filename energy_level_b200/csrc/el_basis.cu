@@ -156,9 +156,9 @@ int upload_tables(el_ctx *ctx, el_basis *b) {
   EL_CUDA_TRY(ctx, cudaMalloc(&b->d_pre_off, npre * sizeof(int64_t)));
   EL_CUDA_TRY(ctx, cudaMalloc(&b->d_pre_cls, npre * sizeof(int32_t)));
   EL_CUDA_TRY(ctx, cudaMalloc(&b->d_suf_rank, b->h_suf_rank.size() * sizeof(int32_t)));
-  EL_CUDA_TRY(ctx, cudaMemcpy(b->d_pre_off, b->h_pre_off.data(), npre * sizeof(int64_t), cudaMemcpyHostToDevice));
-  EL_CUDA_TRY(ctx, cudaMemcpy(b->d_pre_cls, b->h_pre_cls.data(), npre * sizeof(int32_t), cudaMemcpyHostToDevice));
-  EL_CUDA_TRY(ctx, cudaMemcpy(b->d_suf_rank, b->h_suf_rank.data(), b->h_suf_rank.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  EL_CUDA_TRY(ctx, el::copy(ctx, b->d_pre_off, b->h_pre_off.data(), npre * sizeof(int64_t), cudaMemcpyHostToDevice));
+  EL_CUDA_TRY(ctx, el::copy(ctx, b->d_pre_cls, b->h_pre_cls.data(), npre * sizeof(int32_t), cudaMemcpyHostToDevice));
+  EL_CUDA_TRY(ctx, el::copy(ctx, b->d_suf_rank, b->h_suf_rank.data(), b->h_suf_rank.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   // groups for the code expansion
   std::vector<uint64_t> gp;
   std::vector<int64_t> go;
@@ -176,11 +176,11 @@ int upload_tables(el_ctx *ctx, el_basis *b) {
     if ((e = cudaMalloc(&d_gc, gc.size() * 4)) != cudaSuccess) break;
     if ((e = cudaMalloc(&d_co, b->h_cls_off.size() * 8)) != cudaSuccess) break;
     if ((e = cudaMalloc(&d_sl, std::max<size_t>(1, b->h_suf_list.size()) * 4)) != cudaSuccess) break;
-    cudaMemcpy(d_gp, gp.data(), gp.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_go, go.data(), go.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_gc, gc.data(), gc.size() * 4, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_co, b->h_cls_off.data(), b->h_cls_off.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_sl, b->h_suf_list.data(), b->h_suf_list.size() * 4, cudaMemcpyHostToDevice);
+    el::copy(ctx, d_gp, gp.data(), gp.size() * 8, cudaMemcpyHostToDevice);
+    el::copy(ctx, d_go, go.data(), go.size() * 8, cudaMemcpyHostToDevice);
+    el::copy(ctx, d_gc, gc.data(), gc.size() * 4, cudaMemcpyHostToDevice);
+    el::copy(ctx, d_co, b->h_cls_off.data(), b->h_cls_off.size() * 8, cudaMemcpyHostToDevice);
+    el::copy(ctx, d_sl, b->h_suf_list.data(), b->h_suf_list.size() * 4, cudaMemcpyHostToDevice);
     const int64_t ng = (int64_t)gp.size();
     int grid = el::grid_for(ng * 32, 256);
     k_codes_table<<<grid, 256, 0, ctx->stream>>>(ng, d_gp, d_go, d_gc, d_co, d_sl, b->L, b->d_codes);
@@ -295,8 +295,7 @@ int el_basis_codes(el_ctx *ctx, el_basis *b, uint64_t *codes) {
   if (!ctx || !b || !codes) return EL_EINVAL;
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   if (b->layout == EL_LAYOUT_TABLE) {
-    EL_CUDA_TRY(ctx, cudaMemcpyAsync(codes, b->d_codes, (size_t)b->dim * 8,
-                                     cudaMemcpyDeviceToDevice, ctx->stream));
+    EL_CUDA_TRY(ctx, el::copy(ctx, codes, b->d_codes, (size_t)b->dim * 8, cudaMemcpyDeviceToDevice));
     return EL_OK;
   }
   BasisDev B = el::basis_dev(b);

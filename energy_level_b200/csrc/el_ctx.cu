@@ -153,4 +153,11 @@ const char *el_last_error(const el_ctx *ctx) {
 
 int64_t el_ctx_launches(const el_ctx *ctx) { return ctx ? ctx->launches : -1; }
 
+int el_ctx_bytes(const el_ctx *ctx, int64_t *h2d, int64_t *d2h) {
+  if (!ctx) return EL_EINVAL;
+  if (h2d) *h2d = ctx->h2d_bytes;
+  if (d2h) *d2h = ctx->d2h_bytes;
+  return EL_OK;
+}
+
 }  // extern "C"

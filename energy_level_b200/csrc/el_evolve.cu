@@ -91,7 +91,7 @@ extern "C" int el_cheb_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
   char *buf = (char *)el::workspace(ctx, 5, 4 * vb);
   if (!buf) return EL_ENOMEM;
   void *t0 = buf, *t1 = buf + vb, *t2 = buf + 2 * vb, *acc = buf + 3 * vb;
-  EL_CUDA_TRY(ctx, cudaMemcpyAsync(t0, psi, vb, cudaMemcpyDeviceToDevice, ctx->stream));
+  EL_CUDA_TRY(ctx, el::copy(ctx, t0, psi, vb, cudaMemcpyDeviceToDevice));
   double cre, cim;
   coef(0, &cre, &cim);
   rc = el::launch_axpby(ctx, dtype, dim, cre, cim, t0, 0, 0, acc, nullptr);
@@ -114,7 +114,7 @@ extern "C" int el_cheb_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
     if (rc) return rc;
     void *t = xm1; xm1 = xc; xc = y; y = t;
   }
-  EL_CUDA_TRY(ctx, cudaMemcpyAsync(psi, acc, vb, cudaMemcpyDeviceToDevice, ctx->stream));
+  EL_CUDA_TRY(ctx, el::copy(ctx, psi, acc, vb, cudaMemcpyDeviceToDevice));
   if (n_terms) *n_terms = M + 1;
   return EL_OK;
 }

@@ -31,6 +31,8 @@ struct el_ctx {
   std::string err;
   const volatile int32_t *cancel = nullptr;
   int64_t launches = 0;
+  int64_t h2d_bytes = 0;   // host->device bytes copied by the library
+  int64_t d2h_bytes = 0;   // device->host bytes copied by the library
   // deterministic reduction scratch: per-block partials + completion counter
   double *d_partials = nullptr;
   size_t partial_cap = 0;  // doubles
@@ -108,6 +110,14 @@ int grid_for(int64_t work, int block);
 // Cached device workspace `slot` of at least `bytes` bytes (nullptr on failure,
 // with the error recorded on ctx).
 void *workspace(el_ctx *ctx, int slot, size_t bytes);
+
+// Asynchronous copy on the context stream, counting host<->device bytes.
+inline cudaError_t copy(el_ctx *ctx, void *dst, const void *src, size_t bytes,
+                        cudaMemcpyKind kind) {
+  if (kind == cudaMemcpyHostToDevice) ctx->h2d_bytes += (int64_t)bytes;
+  else if (kind == cudaMemcpyDeviceToHost) ctx->d2h_bytes += (int64_t)bytes;
+  return cudaMemcpyAsync(dst, src, bytes, kind, ctx->stream);
+}
 
 #define EL_CUDA_TRY(ctx, expr)                                   \
   do {                                                           \
@@ -307,4 +317,8 @@ int launch_scale(el_ctx *ctx, int dtype, int64_t len, const double *scale_dev,
                  int invert_sqrt, void *x);
 int launch_observables(el_ctx *ctx, el_ham *h, int dtype, const void *psi,
                        double *out_dev);
+// tiled full-basis KPM recurrence (el_kpm_full.cu)
+bool kpm_full_eligible(const el_ham *h, int dtype, int chunk, int mode);
+int kpm_full(el_ctx *ctx, el_ham *h, int dtype, int num, int nvec, int chunk, uint64_t seed,
+             const int8_t *probes_host, double c, double r, double *mu_host);
 }  // namespace el

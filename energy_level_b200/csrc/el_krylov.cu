@@ -27,8 +27,7 @@ using el::fail;
 bool is_cplx(int dtype) { return dtype == EL_C64 || dtype == EL_C128; }
 
 int sync_read(el_ctx *ctx, const double *dev, int count, double *host) {
-  EL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_scalars, dev, count * sizeof(double),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
+  EL_CUDA_TRY(ctx, el::copy(ctx, ctx->h_scalars, dev, count * sizeof(double), cudaMemcpyDeviceToHost));
   EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   for (int i = 0; i < count; ++i) host[i] = ctx->h_scalars[i];
   return EL_OK;
@@ -132,8 +131,12 @@ extern "C" int el_kpm_moments(el_ctx *ctx, el_ham *h, int dtype, int num, int nv
   if (num < 1 || nvec < 1) return fail(ctx, EL_EINVAL, "num and nvec must be positive integers");
   if (chunk < 1 || chunk > 256 || (chunk & (chunk - 1))) return fail(ctx, EL_EINVAL, "chunk must be a power of two <= 256");
   if (!(r > 0) || !std::isfinite(r) || !std::isfinite(c)) return fail(ctx, EL_EINVAL, "bad scaling c, r");
+  const bool force_generic = (mode & EL_KPM_GENERIC_KERNEL) != 0;
+  mode &= ~EL_KPM_GENERIC_KERNEL;
   if (mode != EL_KPM_DIRECT && mode != EL_KPM_DOUBLING) return fail(ctx, EL_EINVAL, "unknown KPM mode");
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (!force_generic && el::kpm_full_eligible(h, dtype, chunk, mode))
+    return el::kpm_full(ctx, h, dtype, num, nvec, chunk, seed, probes_host, c, r, mu_host);
   const int64_t dim = h->basis->dim;
   const int es = el::dtype_size(dtype);
   const size_t vb = (size_t)dim * chunk * es;
@@ -159,14 +162,13 @@ extern "C" int el_kpm_moments(el_ctx *ctx, el_ham *h, int dtype, int num, int nv
     // t0 = z (probes beyond b are zero vectors and contribute nothing)
     if (probes_host) {
       EL_CUDA_TRY(ctx, cudaMemsetAsync(d_probe8, 0, (size_t)dim * chunk, ctx->stream));
-      EL_CUDA_TRY(ctx, cudaMemcpyAsync(d_probe8, probes_host + (size_t)done * dim, (size_t)dim * b,
-                                       cudaMemcpyHostToDevice, ctx->stream));
+      EL_CUDA_TRY(ctx, el::copy(ctx, d_probe8, probes_host + (size_t)done * dim, (size_t)dim * b, cudaMemcpyHostToDevice));
       rc = el::launch_probe_copy(ctx, dtype, dim, chunk, d_probe8, t0);
     } else {
       rc = el::launch_fill_rademacher(ctx, dtype, dim, chunk, seed, done, b, t0);
     }
     if (rc) return rc;
-    if (direct) EL_CUDA_TRY(ctx, cudaMemcpyAsync(zp, t0, vb, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (direct) EL_CUDA_TRY(ctx, el::copy(ctx, zp, t0, vb, cudaMemcpyDeviceToDevice));
     // first step: t1 = Htil t0 ; dots <t0,t0>, <t0,t1>
     ApplyArgs A;
     memset(&A, 0, sizeof A);
@@ -189,8 +191,7 @@ extern "C" int el_kpm_moments(el_ctx *ctx, el_ham *h, int dtype, int num, int nv
       if (rc) return rc;
       void *t = xm1; xm1 = x; x = y; y = t;
     }
-    EL_CUDA_TRY(ctx, cudaMemcpyAsync(hd.data(), d_dots, hd.size() * sizeof(double),
-                                     cudaMemcpyDeviceToHost, ctx->stream));
+    EL_CUDA_TRY(ctx, el::copy(ctx, hd.data(), d_dots, hd.size() * sizeof(double), cudaMemcpyDeviceToHost));
     EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     for (int v = 0; v < b; ++v) {
       const double *d0 = &hd[(size_t)v * 4];
@@ -248,7 +249,7 @@ extern "C" int el_lanczos_ground(el_ctx *ctx, el_ham *h, int dtype, const void *
   int rc;
   // start vector
   if (v0) {
-    EL_CUDA_TRY(ctx, cudaMemcpyAsync(Vj(0), v0, vb, cudaMemcpyDeviceToDevice, ctx->stream));
+    EL_CUDA_TRY(ctx, el::copy(ctx, Vj(0), v0, vb, cudaMemcpyDeviceToDevice));
   } else {
     rc = el::launch_fill_gauss(ctx, dtype, dim, seed, Vj(0));
     if (rc) return rc;
@@ -371,8 +372,7 @@ extern "C" int el_lanczos_ground(el_ctx *ctx, el_ham *h, int dtype, const void *
       el::tridiag_vec(al.data(), be.data(), mm, theta[q], svec[q]);
       std::vector<double> coef(2 * mm, 0.0);
       for (int k = 0; k < mm; ++k) coef[2 * k] = svec[q][k];
-      EL_CUDA_TRY(ctx, cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(double),
-                                       cudaMemcpyHostToDevice, ctx->stream));
+      EL_CUDA_TRY(ctx, el::copy(ctx, d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice));
       void *dst = (q == 0) ? xr : rv;
       rc = el::launch_gemv_n(ctx, dtype, dim, mm, Vb, dim, d_coef, dst);
       if (rc) return rc;
@@ -413,7 +413,7 @@ extern "C" int el_lanczos_ground(el_ctx *ctx, el_ham *h, int dtype, const void *
       rc = el::launch_axpby(ctx, dtype, dim, 0.5, 0, rv, 1, 0, xr, nullptr);
       if (rc) return rc;
     }
-    EL_CUDA_TRY(ctx, cudaMemcpyAsync(Vj(0), xr, vb, cudaMemcpyDeviceToDevice, ctx->stream));
+    EL_CUDA_TRY(ctx, el::copy(ctx, Vj(0), xr, vb, cudaMemcpyDeviceToDevice));
     if (nev == 2 && nq == 2) {
       // recompute the ground Ritz vector is unnecessary: it is rebuilt next pass
     }
@@ -422,7 +422,7 @@ extern "C" int el_lanczos_ground(el_ctx *ctx, el_ham *h, int dtype, const void *
   if (iters) *iters = total_steps;
   if (converged) *converged = conv ? 1 : 0;
   if (vec_out) {
-    EL_CUDA_TRY(ctx, cudaMemcpyAsync(vec_out, xr, vb, cudaMemcpyDeviceToDevice, ctx->stream));
+    EL_CUDA_TRY(ctx, el::copy(ctx, vec_out, xr, vb, cudaMemcpyDeviceToDevice));
     EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   }
   return EL_OK;

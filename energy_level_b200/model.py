@@ -1,0 +1,139 @@
+"""calib / plan -> native basis and Hamiltonian, with the reference's checks.
+
+Accepts the reference engine's inputs unchanged: a ``calib`` dict
+(atoms + pairs with V/J/A), per-site ``Om``/``delta``/``gamma`` arrays,
+``terms`` and an optional HamiltonianPlan or ``basis_indices``.
+The B200 path implements the I1 model (Omega, delta, V); J/A exchange
+channels and non-Hermitian gamma are refused with ConfigConflict, never
+silently dropped (backends.py:9-18 semantics).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .core import Basis, Context, Hamiltonian, default_context
+
+
+class ConfigConflict(ValueError):
+    """A configuration key is refused by the selected backend; ``keys`` lists
+    the offending ``manybody.*`` keys (same contract as backends.py:9-18)."""
+
+    def __init__(self, message, *, keys=()):
+        super().__init__(message)
+        self.keys = tuple(keys)
+
+
+def active_terms(calib):
+    """Channels present in a calib (couplings.py:26-40 semantics)."""
+    given = (calib or {}).get('terms')
+    if given is not None:
+        return list(given)
+    pairs = (calib or {}).get('pairs') or []
+    out = []
+    for name, key in (('I1', 'V'), ('I2', 'J'), ('I3', 'A')):
+        if any(abs(complex(p.get(key) or 0.0)) > 0.0 for p in pairs):
+            out.append(name)
+    return out
+
+
+def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None):
+    """Validate and flatten a calib to (n, Om complex[n], delta[n], pairs)."""
+    atoms = (calib or {}).get('atoms') or []
+    n = len(atoms)
+    if n == 0:
+        raise ValueError('通道声明需要至少一个原子')
+    Om = np.zeros(n, complex) if Om is None else np.asarray(Om, complex).reshape(-1)
+    delta = np.zeros(n) if delta is None else np.asarray(delta, float).reshape(-1)
+    gamma = np.zeros(n) if gamma is None else np.asarray(gamma, float).reshape(-1)
+    if any(x.shape != (n,) or not np.isfinite(x).all() for x in (Om, delta, gamma)):
+        raise ValueError('Om/delta/gamma 须为有限、长度为 N 的数组')
+    if np.any(gamma != 0):
+        raise ConfigConflict('b200 backends need a Hermitian H (gamma = 0)', keys=('manybody.gamma_mhz',))
+    use = set(active_terms(calib) if terms is None else terms)
+    pairs = []
+    for p in (calib.get('pairs') or []):
+        i, j = int(p['i']), int(p['j'])
+        if not (0 <= i < n and 0 <= j < n) or i == j:
+            raise ValueError('pair (%d, %d) out of range' % (i, j))
+        for key, term in (('J', 'I2'), ('A', 'I3')):
+            if term in use and abs(complex(p.get(key) or 0.0)) > 0.0:
+                raise ConfigConflict('b200 backends implement the I1 model only (%s channel %s != 0)'
+                                     % (term, key), keys=('manybody.calib',))
+        if 'I1' in use:
+            V = complex(p.get('V') or 0.0)
+            if V.imag != 0:
+                raise ValueError('V must be real')
+            if V.real != 0:
+                pairs.append((i, j, float(V.real)))
+    return n, Om, delta, pairs
+
+
+def _is_chain_or_ring(n, edges):
+    es = sorted({tuple(sorted((int(a), int(b)))) for a, b in edges})
+    chain = [(i, i + 1) for i in range(n - 1)]
+    return es == chain or es == sorted(chain + [(0, n - 1)])
+
+
+def basis_for(ctx: Context, n, plan=None, basis_indices=None, constraint=None, max_states=None):
+    """Native basis for the reference's basis descriptions.
+
+    plan: HamiltonianPlan dict (hamiltonian_plan.py:129-148) -> its blockade
+    edges when projected; basis_indices: an explicit code list, accepted when
+    it is a blockade sector of its plan, a fixed-excitation sector or the full
+    basis (checked code by code); returns (Basis, permutation or None) where the
+    permutation maps the caller's order to ascending order."""
+    if plan is not None and plan.get('projected'):
+        edges = plan.get('blockade_edges') or []
+        b = Basis(ctx, n, kind='blockade', edges=edges, max_states=max_states)
+        if plan.get('states') is not None and len(plan['states']) != b.dim:
+            raise ValueError('plan states do not match its blockade edges')
+        return b, None
+    if constraint is not None:
+        kind = constraint.get('kind')
+        if kind == 'blockade':
+            return Basis(ctx, n, kind='blockade', edges=constraint.get('edges') or [],
+                         max_states=max_states), None
+        if kind == 'charge':
+            return Basis(ctx, n, kind='charge', k=int(constraint['k'])), None
+    if basis_indices is None:
+        return Basis(ctx, n, kind='full'), None
+    codes = np.asarray(basis_indices, np.int64).reshape(-1)
+    if codes.size == 0 or np.any(codes < 0) or np.any(codes >= (1 << n)):
+        raise ValueError('basis_indices 须为非空有效位编码')
+    order = np.argsort(codes, kind='stable')
+    srt = codes[order]
+    if np.any(np.diff(srt) == 0):
+        raise ValueError('basis_indices 不能重复')
+    perm = None if np.array_equal(order, np.arange(codes.size)) else order
+    pc = np.array([int(c).bit_count() for c in srt])
+    if codes.size == (1 << n):
+        return Basis(ctx, n, kind='full'), perm
+    if np.all(pc == pc[0]):
+        b = Basis(ctx, n, kind='charge', k=int(pc[0]))
+        if b.dim == codes.size and np.array_equal(b.codes().cpu().numpy(), srt):
+            return b, perm
+    # a blockade sector: the graph of pairs never jointly excited
+    bits = np.array([[(int(c) >> (n - 1 - i)) & 1 for i in range(n)] for c in srt], dtype=np.int64)
+    co = bits.T @ bits
+    edges = [[i, j] for i in range(n) for j in range(i + 1, n) if co[i, j] == 0]
+    b = Basis(ctx, n, kind='blockade', edges=edges)
+    if b.dim == codes.size and np.array_equal(b.codes().cpu().numpy(), srt):
+        return b, perm
+    raise ValueError('basis_indices is not a full, fixed-excitation or blockade basis; '
+                     'the b200 backends need one of those')
+
+
+def build(calib, Om=None, delta=None, gamma=None, terms=None, plan=None, basis_indices=None,
+          constraint=None, device=0, ctx=None, max_states=None):
+    """(ctx, basis, hamiltonian, permutation) for a reference-style model."""
+    n, Om, delta, pairs = model_arrays(calib, Om, delta, gamma, terms)
+    dev = device
+    if isinstance(dev, str):
+        if dev.startswith('cpu'):
+            raise RuntimeError('CUDA 不可用')
+        dev = int(dev.split(':')[1]) if ':' in dev else 0
+    ctx = ctx or default_context(int(dev))
+    b, perm = basis_for(ctx, n, plan=plan, basis_indices=basis_indices, constraint=constraint,
+                        max_states=max_states)
+    h = Hamiltonian(ctx, b, Om, delta, pairs)
+    return ctx, b, h, perm

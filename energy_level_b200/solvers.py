@@ -38,11 +38,12 @@ def kpm_scale(emin, emax):
 
 
 def kpm_moments(ham: Hamiltonian, num, nvec, c, r, dtype="float32", chunk=32, seed=0,
-                probes=None, mode="doubling"):
+                probes=None, mode="doubling", generic=False):
     """mu[0..num] of Htil = (H - c)/r from nvec Rademacher probes.
 
     probes: None (counter-based, from seed) or an int8/float array [nvec, dim]
-    of +-1 entries (e.g. the reference's own numpy draws)."""
+    of +-1 entries (e.g. the reference's own numpy draws).  generic=True
+    forces the row-parallel kernel where the tiled full-basis one applies."""
     if dtype not in ("float32", "float64"):
         raise ValueError('dtype 必须为 float32/float64')
     mu = np.zeros(int(num) + 1)
@@ -55,6 +56,8 @@ def kpm_moments(ham: Hamiltonian, num, nvec, c, r, dtype="float32", chunk=32, se
             raise ValueError('probes must be +-1')
         pb = np.ascontiguousarray(p, dtype=np.int8)
     md = {"direct": _lib.EL_KPM_DIRECT, "doubling": _lib.EL_KPM_DOUBLING}[mode]
+    if generic:
+        md |= _lib.EL_KPM_GENERIC_KERNEL
     ham.ctx.call('el_kpm_moments', ham.handle, C.c_int(_lib.DTYPES[dtype]), C.c_int(int(num)),
                  C.c_int(int(nvec)), C.c_int(int(chunk)), C.c_uint64(int(seed)),
                  C.c_void_p(pb.ctypes.data) if pb is not None else None, C.c_int(md),

@@ -61,6 +61,8 @@ extern "C" {
 /* KPM moment modes */
 #define EL_KPM_DIRECT    0  /* mu_n from <z, T_n z>, the reference recurrence   */
 #define EL_KPM_DOUBLING  1  /* mu_2n = 2<T_n z,T_n z>-mu_0, mu_2n+1 likewise    */
+#define EL_KPM_GENERIC_KERNEL 0x100 /* flag: use the row-parallel kernel even
+                                       where the tiled full-basis one applies */
 
 typedef struct el_ctx el_ctx;
 typedef struct el_basis el_basis;
@@ -84,6 +86,9 @@ int el_ctx_set_cancel(el_ctx *ctx, const volatile int32_t *flag);
 const char *el_last_error(const el_ctx *ctx);
 /* Number of kernels this context has launched since creation. */
 int64_t el_ctx_launches(const el_ctx *ctx);
+/* Host->device and device->host bytes this context has copied since creation
+ * (inputs, parameters, scalars and results; device-to-device copies excluded). */
+int el_ctx_bytes(const el_ctx *ctx, int64_t *h2d, int64_t *d2h);
 
 /* ---- basis ---------------------------------------------------------------- */
 
@@ -152,6 +157,9 @@ int el_bounds(el_ctx *ctx, el_ham *ham, int max_iter, double tol,
  * 32).  probes_host: NULL = counter-based probes from `seed`, else int8
  * [nvec][dim] of +-1.  dtype EL_F32 or EL_F64 (vectors); moments are always
  * accumulated in FP64.  mu[n] = sum_probes <z, T_n z> / (nvec * dim).
+ * On the full basis (6 <= N <= 25) EL_KPM_DOUBLING runs the tiled kernel
+ * (two reads and two writes per element and step) unless the
+ * EL_KPM_GENERIC_KERNEL flag is or-ed into `mode`.
  * Replaces kpm.py:26-75 kpm_moments_gpu and kpm.py:115-151 kpm_moments. */
 int el_kpm_moments(el_ctx *ctx, el_ham *ham, int dtype, int num, int nvec,
                    int chunk, uint64_t seed, const int8_t *probes_host,

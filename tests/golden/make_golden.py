@@ -1,0 +1,168 @@
+"""Generate golden fixtures by running the energy-level reference itself.
+
+Run in a checkout where the reference tree is importable:
+
+    python tests/golden/make_golden.py /path/to/energy-level
+
+It writes small .npz files next to this script.  The GPU tests, the CPU
+oracle tests and smoke() compare against these files; nothing at test time
+imports the reference.  Every call below is a public function of the
+reference's src/core/manybody package (file:line given per fixture).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def main(ref_root: str) -> None:
+    sys.path.insert(0, ref_root)
+    from src.core.manybody import basis as rbasis                       # basis.py
+    from src.core.manybody import matrix_free as rmf                    # matrix_free.py
+    from src.core.manybody import assemble as rasm                      # assemble.py
+    from src.core.manybody import kpm as rkpm                           # kpm.py
+    from src.core.manybody import equilibrium as req                    # equilibrium.py
+    from src.core.manybody import engine_ed as red                      # engine_ed.py
+    from src.core.manybody import hamiltonian_plan as rplan             # hamiltonian_plan.py
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from energy_level_b200 import configs
+
+    # -- basis codes: independent_states (basis.py:24-47), number_sector_basis
+    #    (matrix_free.py:12-38), independent_set_count (basis.py:50-76)
+    graphs = {
+        "chain10": (10, configs.chain_edges(10)),
+        "ring11": (11, configs.ring_edges(11)),
+        "ring20": (20, configs.ring_edges(20)),
+        "square3x3": (9, [[0, 1], [1, 2], [3, 4], [4, 5], [6, 7], [7, 8], [0, 3], [3, 6],
+                          [1, 4], [4, 7], [2, 5], [5, 8]]),
+        "nnn_chain12": (12, configs.chain_edges(12) + [[i, i + 2] for i in range(10)]),
+        "chain22": (22, configs.chain_edges(22)),
+    }
+    out = {}
+    for name, (n, edges) in graphs.items():
+        codes = np.asarray(rbasis.independent_states(n, edges, max_states=1 << 22), np.int64)
+        out["codes_" + name] = codes
+        out["edges_" + name] = np.asarray(edges, np.int64)
+        out["n_" + name] = np.int64(n)
+        out["count_" + name] = np.int64(rbasis.independent_set_count(n, edges))
+    for n, k in [(10, 4), (12, 6), (6, 0), (6, 6)]:
+        out["charge_%d_%d" % (n, k)] = np.asarray(rmf.number_sector_basis(n, k), np.int64)
+    np.savez_compressed(os.path.join(HERE, "basis.npz"), **out)
+
+    # -- H x: hamiltonian_linear_operator (matrix_free.py:51-62) on the full
+    #    basis and on restricted bases; build_H_sparse diagonal (assemble.py:277)
+    out = {}
+    rng = np.random.default_rng(20261203)
+    cases = {
+        "full7": (7, None),
+        "chain10": (10, configs.chain_edges(10)),
+        "ring9": (9, configs.ring_edges(9)),
+        "square3x3": (9, graphs["square3x3"][1]),
+    }
+    for name, (n, edges) in cases.items():
+        pos = configs.chain_positions(n, a=5.5, jitter=rng.uniform(-0.4, 0.4, n))
+        calib = configs.calib_from_positions(pos)
+        om = rng.uniform(0.5, 2.5, n)
+        de = rng.uniform(-3.0, 3.0, n)
+        basis = None if edges is None else rbasis.independent_states(n, edges)
+        op = rmf.hamiltonian_linear_operator(calib, Om=om, delta=de, terms=["I1"],
+                                             basis_indices=basis)
+        dim = op.shape[0]
+        x = rng.normal(size=dim) + 1j * rng.normal(size=dim)
+        out["x_" + name] = x
+        out["y_" + name] = op @ x
+        out["om_" + name] = om
+        out["de_" + name] = de
+        out["pairs_" + name] = np.asarray([[p["i"], p["j"], p["V"]] for p in calib["pairs"]])
+        out["n_" + name] = np.int64(n)
+        out["edges_" + name] = np.asarray(edges if edges else np.zeros((0, 2)), np.int64)
+        H = rasm.build_H_sparse(calib, om, de, ["I1"], None, basis_indices=basis)
+        out["diag_" + name] = np.asarray(H.diagonal()).real
+    # complex Omega (phase) on a restricted basis: conj direction of channels.py:114-118
+    n = 8
+    pos = configs.chain_positions(n)
+    calib = configs.calib_from_positions(pos)
+    omc = rng.uniform(0.5, 2.0, n) * np.exp(1j * rng.uniform(0, 2 * np.pi, n))
+    de = rng.uniform(-2, 2, n)
+    basis = rbasis.independent_states(n, configs.chain_edges(n))
+    op = rmf.hamiltonian_linear_operator(calib, Om=omc, delta=de, terms=["I1"], basis_indices=basis)
+    x = rng.normal(size=len(basis)) + 1j * rng.normal(size=len(basis))
+    out.update(x_cplx8=x, y_cplx8=op @ x, om_cplx8=omc, de_cplx8=de, n_cplx8=np.int64(n),
+               pairs_cplx8=np.asarray([[p["i"], p["j"], p["V"]] for p in calib["pairs"]]),
+               edges_cplx8=np.asarray(configs.chain_edges(n), np.int64))
+    np.savez_compressed(os.path.join(HERE, "hv.npz"), **out)
+
+    # -- KPM: kpm_moments (kpm.py:115-151) with its own numpy probe stream,
+    #    exact moments, _bounds, jackson_kernel, _dos_from_moments
+    n = 7
+    pos = configs.chain_positions(n, a=5.5, jitter=rng.uniform(-0.4, 0.4, n))
+    calib = configs.calib_from_positions(pos)
+    om = rng.uniform(0.5, 2.0, n)
+    de = rng.uniform(-3, 3, n)
+    H = rasm.build_H_sparse(calib, om, de, ["I1"], None)
+    num, nvec, seed = 48, 4, 3
+    mu, c, r = rkpm.kpm_moments(H, num=num, nvec=nvec, seed=seed)
+    probe_rng = np.random.default_rng(seed)
+    z = np.stack([probe_rng.choice(np.array([-1.0, 1.0]), size=H.shape[0]) for _ in range(nvec)])
+    mu_exact, _, _ = rkpm.kpm_moments(H, num=num, exact=True)
+    emin, emax, c2, r2 = rkpm._bounds(H)
+    energies = np.linspace(emin, emax, 64)
+    rho = rkpm._dos_from_moments(mu, c, r, energies, num)
+    np.savez_compressed(os.path.join(HERE, "kpm.npz"), n=np.int64(n), om=om, de=de,
+                        pairs=np.asarray([[p["i"], p["j"], p["V"]] for p in calib["pairs"]]),
+                        num=np.int64(num), nvec=np.int64(nvec), seed=np.int64(seed), mu=mu, c=c, r=r,
+                        probes=z, mu_exact=mu_exact, emin=emin, emax=emax,
+                        jackson=rkpm.jackson_kernel(num), energies=energies, rho=rho)
+
+    # -- ground states: ground_state (equilibrium.py:35-96) with eigsh on the
+    #    matrix-free operator for the chain12 workload; blockade sector by
+    #    dense eigh of the projected plan (hamiltonian_plan.py:129-156)
+    cfg = configs.chain12()
+    op = rmf.hamiltonian_linear_operator(cfg["calib"], Om=cfg["Om"], delta=cfg["delta"], terms=["I1"])
+    v0 = np.random.default_rng(0).standard_normal(op.shape[0])
+    gs = req.ground_state(op, dense_max=0, k=2, v0=v0)
+    plan = rplan.build_plan(cfg["calib"], Om=cfg["Om"], delta=cfg["delta"], terms=["I1"],
+                            constraint={"kind": "blockade", "edges": configs.chain_edges(12)})
+    gsb = req.ground_state(rplan.compile_sparse(plan), dense_max=4096, k=2)
+    cfgr = configs.ring20()
+    ring_pairs = np.asarray([[p["i"], p["j"], p["V"]] for p in cfgr["calib"]["pairs"]])
+    plan_r = rplan.build_plan(cfgr["calib"], Om=np.full(20, 2.0), delta=np.full(20, 1.0),
+                              terms=["I1"], constraint={"kind": "blockade", "edges": configs.ring_edges(20)})
+    gsr = req.ground_state(rplan.compile_sparse(plan_r), dense_max=0, k=2,
+                           v0=np.random.default_rng(1).standard_normal(plan_r["dim"]))
+    np.savez_compressed(os.path.join(HERE, "ground.npz"),
+                        chain12_E0=gs["E0"], chain12_gap=gs["gap"], chain12_evals=gs["evals"],
+                        chain12b_E0=gsb["E0"], chain12b_gap=gsb["gap"],
+                        ring20_E0=gsr["E0"], ring20_gap=gsr["gap"], ring20_pairs=ring_pairs)
+
+    # -- evolution: evolve_manybody (engine_ed.py:153-372) with piecewise-
+    #    constant segments on a projected blockade plan (segment path,
+    #    engine_ed.py:130-147), record_psi for the final state
+    n = 9
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+    steps, total = 12, 240.0
+    segments = [{"t0": k * total / steps, "Om": np.full(n, 2.0 + 0.3 * np.sin(k)),
+                 "delta": np.full(n, 6.0 - 12.0 * k / steps)} for k in range(steps)]
+    plan = rplan.build_plan(calib, Om=np.full(n, 2.0), delta=np.zeros(n), terms=["I1"],
+                            constraint={"kind": "blockade", "edges": configs.chain_edges(n)})
+    t_grid = np.linspace(0.0, total, 5)
+    res = red.evolve_manybody(calib, psi0="g" * n, t_grid=t_grid, segments=segments, plan=plan,
+                              terms=["I1"], record_psi=True, want_corr=False, want_entropy=False,
+                              want_observables=False)
+    np.savez_compressed(os.path.join(HERE, "evolve.npz"), n=np.int64(n), t_grid=t_grid,
+                        seg_t0=np.asarray([s["t0"] for s in segments]),
+                        seg_om=np.asarray([s["Om"] for s in segments]),
+                        seg_de=np.asarray([s["delta"] for s in segments]),
+                        pairs=np.asarray([[p["i"], p["j"], p["V"]] for p in calib["pairs"]]),
+                        pops_atom=res["pops_atom"], norms=res["norms"], psi_final=res["psi_amp"],
+                        basis_states=np.asarray(res["basis_states"], np.int64))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

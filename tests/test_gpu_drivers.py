@@ -106,3 +106,30 @@ def test_cheb_evolution_matches_expm(ctx, dtype, tol):
     ns, nrm = solvers.observables(h, psi)
     assert abs(nrm - 1.0) < 10 * tol
     assert np.allclose(ns, ref.site_occupations(n, codes, want), atol=10 * tol)
+
+
+@pytest.mark.parametrize("n", [8, 13, 14, 17])
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-10), ("float32", 2e-4)])
+def test_tiled_kpm_matches_oracle(ctx, n, dtype, tol):
+    """Tiled full-basis KPM (doubling) vs the C oracle's direct recurrence on
+    identical probes; n >= 14 exercises the two-group pass alternation."""
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import solvers
+    from oracle import build as ob
+    rng = np.random.default_rng(n)
+    om = rng.uniform(0.5, 2.0, n)
+    de = rng.uniform(-3, 3, n)
+    pos = [[6.0 * (i % 5), 6.0 * (i // 5), 0.0] for i in range(n)]
+    pairs = configs.pairs_from_positions(pos)
+    b = Basis(ctx, n, kind="full")
+    h = Hamiltonian(ctx, b, om, de, pairs)
+    lo, hi = solvers.bounds(h, max_iter=400, tol=1e-13)
+    c, r = solvers.kpm_scale(lo, hi)
+    nvec, num = 8, 41
+    z = rng.choice(np.array([-1, 1], dtype=np.int8), size=(nvec, 1 << n))
+    want = ob.kpm_full(n, om, ob.diag_full(n, de, pairs), c, r, num, z)
+    got = solvers.kpm_moments(h, num, nvec, c, r, dtype=dtype, chunk=8, probes=z, mode="doubling")
+    gen = solvers.kpm_moments(h, num, nvec, c, r, dtype=dtype, chunk=8, probes=z, mode="doubling",
+                              generic=True)
+    assert np.abs(got - want).max() < tol
+    assert np.abs(gen - want).max() < tol

@@ -1,0 +1,137 @@
+"""Pin the CPU oracle to golden vectors written by the reference itself
+(tests/golden/make_golden.py).  CPU only."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import ref
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(GOLD, name + ".npz"), allow_pickle=False)
+
+
+def pairs_of(arr):
+    return [(int(i), int(j), float(v)) for i, j, v in np.asarray(arr)]
+
+
+@pytest.mark.parametrize("name", ["chain10", "ring11", "ring20", "square3x3", "nnn_chain12", "chain22"])
+def test_independent_states_bit_exact(name):
+    g = load("basis")
+    n = int(g["n_" + name])
+    edges = g["edges_" + name].tolist()
+    codes = ref.independent_states(n, edges, max_states=None)
+    assert np.array_equal(codes, g["codes_" + name])
+    assert len(codes) == int(g["count_" + name])
+
+
+def test_fibonacci_and_lucas_dimensions():
+    g = load("basis")
+    assert len(g["codes_chain22"]) == ref.fib(24)
+    assert len(g["codes_ring20"]) == ref.fib(21) + ref.fib(19) == 15127
+    assert len(g["codes_chain10"]) == ref.fib(12)
+
+
+@pytest.mark.parametrize("n,k", [(10, 4), (12, 6), (6, 0), (6, 6)])
+def test_number_sector_bit_exact(n, k):
+    g = load("basis")
+    assert np.array_equal(ref.number_sector_basis(n, k), g["charge_%d_%d" % (n, k)])
+
+
+def test_max_states_cap():
+    with pytest.raises(ValueError):
+        ref.independent_states(20, [[i, i + 1] for i in range(19)], max_states=100)
+
+
+@pytest.mark.parametrize("name", ["full7", "chain10", "ring9", "square3x3", "cplx8"])
+def test_hv_matches_reference(name):
+    g = load("hv")
+    n = int(g["n_" + name])
+    edges = g["edges_" + name].tolist()
+    codes = None if not edges else ref.independent_states(n, edges, None)
+    y = ref.hv(n, codes, g["om_" + name], g["de_" + name], pairs_of(g["pairs_" + name]), g["x_" + name])
+    assert np.max(np.abs(y - g["y_" + name])) < 1e-12 * max(1.0, np.abs(g["y_" + name]).max())
+
+
+@pytest.mark.parametrize("name", ["full7", "chain10", "ring9", "square3x3"])
+def test_diagonal_matches_reference(name):
+    g = load("hv")
+    n = int(g["n_" + name])
+    edges = g["edges_" + name].tolist()
+    codes = np.arange(1 << n) if not edges else ref.independent_states(n, edges, None)
+    d = ref.diagonal(n, codes, g["de_" + name], pairs_of(g["pairs_" + name]))
+    assert np.max(np.abs(d - g["diag_" + name])) < 1e-12
+
+
+def test_kpm_matches_reference():
+    g = load("kpm")
+    n = int(g["n"])
+    H = ref.dense_h(n, None, g["om"], g["de"], pairs_of(g["pairs"]))
+    emin, emax, c, r = ref.kpm_bounds(H)
+    assert abs(emin - float(g["emin"])) < 1e-9 and abs(emax - float(g["emax"])) < 1e-9
+    assert abs(c - float(g["c"])) < 1e-9 and abs(r - float(g["r"])) < 1e-9
+    num = int(g["num"])
+    mu = ref.kpm_moments(lambda v: H @ v, H.shape[0], num, g["probes"], float(g["c"]), float(g["r"]))
+    assert np.max(np.abs(mu - g["mu"])) < 1e-12
+    mu_ex = ref.kpm_moments_exact(H, num, float(g["c"]), float(g["r"]))
+    assert np.max(np.abs(mu_ex - g["mu_exact"])) < 1e-12
+    assert np.max(np.abs(ref.jackson_kernel(num) - g["jackson"])) < 1e-15
+    rho = ref.dos_from_moments(g["mu"], float(g["c"]), float(g["r"]), g["energies"], num)
+    assert np.max(np.abs(rho - g["rho"])) < 1e-12
+
+
+def test_kpm_doubling_identity_matches_direct():
+    """mu_2n = 2<T_n z, T_n z> - mu_0 and mu_2n+1 = 2<T_n+1 z, T_n z> - mu_1
+    reproduce the direct recurrence (the identity the GPU doubling mode uses)."""
+    g = load("kpm")
+    n = int(g["n"])
+    H = ref.dense_h(n, None, g["om"], g["de"], pairs_of(g["pairs"]))
+    c, r = float(g["c"]), float(g["r"])
+    Ht = (H - c * np.eye(H.shape[0])) / r
+    num = int(g["num"])
+    acc = np.zeros(num + 1)
+    for z in g["probes"]:
+        ts = [z, Ht @ z]
+        while len(ts) < num // 2 + 2:
+            ts.append(2 * Ht @ ts[-1] - ts[-2])
+        m0, m1 = z @ z, ts[1] @ z
+        acc[0] += m0
+        acc[1] += m1
+        for k in range(1, num // 2 + 1):
+            if 2 * k <= num:
+                acc[2 * k] += 2 * ts[k] @ ts[k] - m0
+            if 2 * k + 1 <= num:
+                acc[2 * k + 1] += 2 * ts[k + 1] @ ts[k] - m1
+    mu = acc / (len(g["probes"]) * H.shape[0])
+    assert np.max(np.abs(mu - g["mu"])) < 1e-11
+
+
+def test_ground_state_chain12_matches_reference():
+    g = load("ground")
+    from energy_level_b200 import configs
+    cfg = configs.chain12()
+    pairs = [(p["i"], p["j"], p["V"]) for p in cfg["calib"]["pairs"]]
+    codes = ref.independent_states(12, configs.chain_edges(12), None)
+    w = np.linalg.eigvalsh(ref.dense_h(12, codes, cfg["Om"], cfg["delta"], pairs))
+    assert abs(w[0] - float(g["chain12b_E0"])) < 1e-9
+    assert abs((w[1] - w[0]) - float(g["chain12b_gap"])) < 1e-9
+    # full basis value quoted by the reference (eigsh on the matrix-free operator)
+    assert abs(float(g["chain12_E0"]) - (-10.2963231346414)) < 1e-9
+
+
+def test_evolution_matches_reference():
+    g = load("evolve")
+    n = int(g["n"])
+    from energy_level_b200 import configs
+    segs = [{"t0": float(t), "Om": om, "delta": de} for t, om, de in zip(g["seg_t0"], g["seg_om"], g["seg_de"])]
+    codes = ref.independent_states(n, configs.chain_edges(n), None)
+    assert np.array_equal(codes, g["basis_states"])
+    psi0 = np.zeros(len(codes), complex)
+    psi0[0] = 1.0
+    states = ref.evolve_segments(n, codes, pairs_of(g["pairs"]), segs, psi0, g["t_grid"])
+    assert np.max(np.abs(states[-1] - g["psi_final"])) < 1e-10
+    pops = np.array([ref.site_occupations(n, codes, s) for s in states])
+    assert np.max(np.abs(pops - g["pops_atom"])) < 1e-10
