@@ -317,6 +317,10 @@ int launch_scale(el_ctx *ctx, int dtype, int64_t len, const double *scale_dev,
                  int invert_sqrt, void *x);
 int launch_observables(el_ctx *ctx, el_ham *h, int dtype, const void *psi,
                        double *out_dev);
+// TMA-fed tiled full-basis KPM recurrence (el_kpm_tma.cu), 20 <= N <= 25
+bool kpm_tma_eligible(const el_ham *h, int dtype, int chunk);
+int kpm_tma(el_ctx *ctx, el_ham *h, int dtype, int num, int nvec, int chunk, uint64_t seed,
+            const int8_t *probes_host, double c, double r, double *mu_host);
 // tiled full-basis KPM recurrence (el_kpm_full.cu)
 bool kpm_full_eligible(const el_ham *h, int dtype, int chunk, int mode);
 int kpm_full(el_ctx *ctx, el_ham *h, int dtype, int num, int nvec, int chunk, uint64_t seed,

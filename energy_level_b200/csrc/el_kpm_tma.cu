@@ -1,0 +1,575 @@
+// TMA-fed tiled KPM recurrence on the full 2^N basis (14 <= N <= 25).
+//
+// Same two-group pass scheme as el_kpm_full.cu (see its header): the
+// sigma^x part of H splits by row bit into X_A (row bits [0, a)) and X_B
+// (row bits [a, N)); a pass over the tiles of one group completes
+//   t_m     = p_m + s_m X_G t_{m-1}
+// and starts
+//   p_{m+1} = 2(D-c)/r t_m + (2/r) X_G t_m - t_{m-1},
+// reading two vectors and writing two per Chebyshev step.
+//
+// Here every byte of tile traffic moves by TMA, not through the LSU pipe:
+//   - vectors are [pair group][row] arrays of 8-byte cells (two FP32 probes
+//     or one FP64 probe), so an A tile (2^a consecutive rows) is one 64 KB box
+//     and a B tile (row bit 0 plus row bits a..N-1) is 2^(N-a) row pairs of
+//     16 bytes, 2^a rows apart, fetched as boxes of 256 pairs;
+//   - the t_{m-1} tile of the next work item is prefetched into a second
+//     buffer while the current one is processed;
+//   - t_m and p_{m+1} are written into shared memory and stored by TMA.
+// Shared memory per CTA: three 2^13-cell buffers (S_cur, S_next, S2) = 192 KB.
+// Waits on the TMA transaction barriers are bounded; on timeout the kernel
+// records an error flag (read by the host) and finishes without hanging.
+#include "el_internal.cuh"
+
+#include <algorithm>
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+namespace {
+
+using el::fail;
+
+template <typename T> struct Cell8;
+template <> struct Cell8<float> { typedef float2 U; static constexpr int PU = 2; };
+template <> struct Cell8<double> { typedef double U; static constexpr int PU = 1; };
+
+__device__ __forceinline__ float2 z8(float2) { return make_float2(0.f, 0.f); }
+__device__ __forceinline__ double z8(double) { return 0.0; }
+__device__ __forceinline__ float2 fma8(float s, float2 x, float2 y) { return make_float2(fmaf(s, x.x, y.x), fmaf(s, x.y, y.y)); }
+__device__ __forceinline__ double fma8(double s, double x, double y) { return fma(s, x, y); }
+__device__ __forceinline__ float2 add8(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double add8(double a, double b) { return a + b; }
+__device__ __forceinline__ float2 sub8(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double sub8(double a, double b) { return a - b; }
+__device__ __forceinline__ float2 scl8(float s, float2 x) { return make_float2(s * x.x, s * x.y); }
+__device__ __forceinline__ double scl8(double s, double x) { return s * x; }
+__device__ __forceinline__ float get8(float2 v, int i) { return i ? v.y : v.x; }
+__device__ __forceinline__ double get8(double v, int) { return v; }
+
+
+enum { KIND_A = 0, KIND_B = 1 };
+enum { MODE_STEP = 0, MODE_PROLOGUE = 1, MODE_LAST = 2 };
+constexpr int NT = 1024;
+
+template <typename T>
+struct TmaArgs {
+  int n, a, mode, ng, log_tiles, hb, nbox;
+  int64_t dim, tiles, items;
+  T s_m, two_r, pro_alpha, pro_beta;
+  T amp[16];
+  const T *d2;
+  double *partials;
+  unsigned int *counter;
+  double *dots;
+  int *err;
+};
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after a fixed number of polls and flags the error.
+__device__ __forceinline__ void mbar_wait(uint64_t *bar, unsigned parity, int *err) {
+  for (int it = 0; it < (1 << 20); ++it)
+    if (mbar_try(bar, parity)) return;
+  atomicExch(err, 1);
+}
+__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, int c0, int c1, int c2, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+      ::"r"(smem_u32(dst)), "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tma_store3(const CUtensorMap *m, int c0, int c1, int c2, const void *src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];"
+               ::"l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src)) : "memory");
+}
+__device__ __forceinline__ void tma_store4(const CUtensorMap *m, int c0, int c1, int c2, int c3, const void *src) {
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
+               ::"l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src)) : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Tile <-> tensor-map coordinates.  A: 3-D map {256-byte chunk, chunk index,
+// group}; B: 4-D map {16-byte row pair, tile, h, group}.
+template <int KIND, typename T>
+__device__ __forceinline__ void tile_load(const TmaArgs<T> &A, void *dst, const CUtensorMap *m,
+                                          uint32_t tile, int g, uint64_t *bar) {
+  if (KIND == KIND_A) {
+    tma_load3(dst, m, 0, (int)(tile << (A.a - 5)), g, bar);
+  } else {
+    for (int k = 0; k < A.nbox; ++k)
+      tma_load4((char *)dst + (size_t)k * A.hb * 16, m, 0, (int)tile, k * A.hb, g, bar);
+  }
+}
+template <int KIND, typename T>
+__device__ __forceinline__ void tile_store(const TmaArgs<T> &A, const CUtensorMap *m, uint32_t tile,
+                                           int g, const void *src) {
+  if (KIND == KIND_A) {
+    tma_store3(m, 0, (int)(tile << (A.a - 5)), g, src);
+  } else {
+    for (int k = 0; k < A.nbox; ++k)
+      tma_store4(m, 0, (int)tile, k * A.hb, g, (const char *)src + (size_t)k * A.hb * 16);
+  }
+}
+
+template <int KIND>
+__device__ __forceinline__ uint32_t row_of(int a, uint32_t tile, int l) {
+  if (KIND == KIND_A) return (tile << a) + (uint32_t)l;
+  return (uint32_t)(l & 1) + ((uint32_t)(l >> 1) << a) + (tile << 1);
+}
+
+// h[j] += sum_{k in [K0, KMAX)} amp_k * S[(tid ^ 2^k) + NT*j] for the R cells
+// of this thread.  Bit-outer order: one address per bit, R independent FMA
+// chains per bit.
+template <typename T, int R, int K0, int KMAX>
+__device__ __forceinline__ void gather_all(const typename Cell8<T>::U *S, int tid,
+                                           const TmaArgs<T> &A, typename Cell8<T>::U (&h)[R]) {
+#pragma unroll
+  for (int k = K0; k < KMAX; ++k) {
+    const typename Cell8<T>::U *base = S + (tid ^ (1 << k));
+    const T a = A.amp[k];
+#pragma unroll
+    for (int j = 0; j < R; ++j) h[j] = fma8(a, base[NT * j], h[j]);
+  }
+}
+
+template <typename T, int TB, int KIND>
+__global__ void __launch_bounds__(NT, 1)
+k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
+          const __grid_constant__ CUtensorMap mapQ) {
+  typedef typename Cell8<T>::U U;
+  constexpr int PU = Cell8<T>::PU;
+  constexpr int R = (1 << TB) / NT;          // cells per thread (TB >= 10)
+  constexpr int LOGNT = 10;
+  constexpr int NWARP = NT / 32;
+  constexpr int K0 = (KIND == KIND_B) ? 1 : 0;
+  constexpr unsigned TILE_BYTES = (1u << TB) * 8u;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  U *const Sb0 = reinterpret_cast<U *>(smem_raw);
+  U *const Sb1 = reinterpret_cast<U *>(smem_raw + TILE_BYTES);
+  U *const S2 = reinterpret_cast<U *>(smem_raw + 2 * TILE_BYTES);
+  __shared__ __align__(8) uint64_t bar[3];   // S buffers 0/1, S2
+  __shared__ double wred[NWARP][2 * PU];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ndots = A.ng * PU * 2;
+  double *dacc = A.partials + (size_t)blockIdx.x * ndots;
+  for (int i = tid; i < ndots; i += NT) dacc[i] = 0.0;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
+    fence_async_smem();
+  }
+  __syncthreads();
+  unsigned par[3] = {0u, 0u, 0u};
+  const T *__restrict__ d2 = A.d2;
+  int cur = 0;
+  int64_t item = blockIdx.x;
+  // per-thread FP64 sums of <t,t> and <t,t_prev> for the current probe group
+  double acc_tt[PU], acc_tq[PU];
+#pragma unroll
+  for (int q = 0; q < PU; ++q) { acc_tt[q] = 0.0; acc_tq[q] = 0.0; }
+  int gacc = (int)(item >> A.log_tiles);
+  if (tid == 0 && item < A.items) {
+    const uint32_t tile = (uint32_t)(item & (A.tiles - 1));
+    mbar_expect(&bar[0], TILE_BYTES);
+    tile_load<KIND>(A, Sb0, &mapQ, tile, gacc, &bar[0]);
+  }
+  for (; item < A.items; item += gridDim.x) {
+    const int g = (int)(item >> A.log_tiles);
+    const uint32_t tile = (uint32_t)(item & (A.tiles - 1));
+    const int64_t nxt = item + gridDim.x;
+    if (g != gacc) {   // uniform across the CTA: flush the previous group's sums
+#pragma unroll
+      for (int q = 0; q < PU; ++q) {
+        double x = acc_tt[q], y = acc_tq[q];
+        for (int o = 16; o > 0; o >>= 1) {
+          x += __shfl_xor_sync(0xffffffffu, x, o);
+          y += __shfl_xor_sync(0xffffffffu, y, o);
+        }
+        if (lane == 0) { wred[warp][2 * q] = x; wred[warp][2 * q + 1] = y; }
+        acc_tt[q] = 0.0; acc_tq[q] = 0.0;
+      }
+      __syncthreads();
+      if (tid < 2 * PU) {
+        double sum = 0.0;
+#pragma unroll
+        for (int w = 0; w < NWARP; ++w) sum += wred[w][tid];
+        dacc[gacc * PU * 2 + tid] += sum;
+      }
+      gacc = g;
+    }
+    U *S = cur ? Sb1 : Sb0;
+    U *Sn = cur ? Sb0 : Sb1;
+    if (tid == 0) {
+      // the previous item's S2 store (the older of its two groups) has read
+      // its source; the S store may still be reading Sn
+      bulk_wait_read<1>();
+      if (A.mode != MODE_PROLOGUE) {
+        mbar_expect(&bar[2], TILE_BYTES);
+        tile_load<KIND>(A, S2, &mapP, tile, g, &bar[2]);
+      }
+    }
+    __syncthreads();   // nobody writes S2 before that store is done
+    if (cur) { mbar_wait(&bar[1], par[1], A.err); par[1] ^= 1u; }
+    else { mbar_wait(&bar[0], par[0], A.err); par[0] ^= 1u; }
+
+    U own[R], hx[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) { own[j] = S[tid + NT * j]; hx[j] = z8(U{}); }
+    // X_G t_{m-1} (or X_G t_0 in the prologue): shared bits, then the upper
+    // tile bits, whose partners are this thread's own cells
+    gather_all<T, R, K0, LOGNT>(S, tid, A, hx);
+#pragma unroll
+    for (int b = 0; (1 << b) < R; ++b)
+#pragma unroll
+      for (int j = 0; j < R; ++j) hx[j] = fma8(A.amp[LOGNT + b], own[j ^ (1 << b)], hx[j]);
+    if (tid == 0 && nxt < A.items) {
+      // prefetch the next t_{m-1} tile once the previous S store has read Sn
+      bulk_wait_read<0>();
+      const int gn = (int)(nxt >> A.log_tiles);
+      const uint32_t tn = (uint32_t)(nxt & (A.tiles - 1));
+      uint64_t *bn = cur ? &bar[0] : &bar[1];
+      mbar_expect(bn, TILE_BYTES);
+      tile_load<KIND>(A, Sn, &mapQ, tn, gn, bn);
+    }
+    // per-tile products: two interleaved FP32 partial sums per quantity,
+    // widened to FP64 once per tile
+    T pt[PU][2], pq[PU][2];
+#pragma unroll
+    for (int q = 0; q < PU; ++q) { pt[q][0] = pt[q][1] = pq[q][0] = pq[q][1] = (T)0; }
+    if (A.mode == MODE_PROLOGUE) {
+      // p_1 = (D-c)/r t_0 + pro_beta X_G t_0 -> S2 -> P
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const int l = tid + NT * j;
+        const uint32_t row = row_of<KIND>(A.a, tile, l);
+        S2[l] = fma8(A.pro_beta, hx[j], scl8(A.pro_alpha * d2[row], own[j]));
+#pragma unroll
+        for (int q = 0; q < PU; ++q) pt[q][j & 1] = fma(get8(own[j], q), get8(own[j], q), pt[q][j & 1]);
+      }
+      fence_async_smem();
+      __syncthreads();
+      if (tid == 0) { tile_store<KIND>(A, &mapP, tile, g, S2); bulk_commit(); }
+    } else {
+      mbar_wait(&bar[2], par[2], A.err);
+      par[2] ^= 1u;
+      // t_m = p_m + s_m X_G t_{m-1}
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const int l = tid + NT * j;
+        const U t = fma8(A.s_m, hx[j], S2[l]);
+        if (A.mode != MODE_LAST) S2[l] = t;
+        hx[j] = t;
+#pragma unroll
+        for (int q = 0; q < PU; ++q) {
+          pt[q][j & 1] = fma(get8(t, q), get8(t, q), pt[q][j & 1]);
+          pq[q][j & 1] = fma(get8(t, q), get8(own[j], q), pq[q][j & 1]);
+        }
+      }
+      if (A.mode != MODE_LAST) {
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) { tile_store<KIND>(A, &mapP, tile, g, S2); bulk_commit(); }
+        // p_{m+1} = d2 t_m + (2/r) X_G t_m - t_{m-1}  (t_m in hx[], t_{m-1} in own[])
+        U h2[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) h2[j] = z8(U{});
+        gather_all<T, R, K0, LOGNT>(S2, tid, A, h2);
+#pragma unroll
+        for (int b = 0; (1 << b) < R; ++b)
+#pragma unroll
+          for (int j = 0; j < R; ++j) h2[j] = fma8(A.amp[LOGNT + b], hx[j ^ (1 << b)], h2[j]);
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const int l = tid + NT * j;
+          const uint32_t row = row_of<KIND>(A.a, tile, l);
+          S[l] = sub8(fma8(A.two_r, h2[j], scl8(d2[row], hx[j])), S[l]);   // S[l] = t_{m-1}
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) { tile_store<KIND>(A, &mapQ, tile, g, S); bulk_commit(); }
+      }
+    }
+    // per-tile products: FP32 tree sums over the R cells, widened to FP64
+#pragma unroll
+    for (int q = 0; q < PU; ++q) {
+      acc_tt[q] += (double)pt[q][0] + (double)pt[q][1];
+      acc_tq[q] += (double)pq[q][0] + (double)pq[q][1];
+    }
+    cur ^= 1;
+  }
+  // flush the last group
+#pragma unroll
+  for (int q = 0; q < PU; ++q) {
+    double x = acc_tt[q], y = acc_tq[q];
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_xor_sync(0xffffffffu, x, o);
+      y += __shfl_xor_sync(0xffffffffu, y, o);
+    }
+    if (lane == 0) { wred[warp][2 * q] = x; wred[warp][2 * q + 1] = y; }
+  }
+  __syncthreads();
+  if (tid < 2 * PU && blockIdx.x < A.items) {
+    double sum = 0.0;
+#pragma unroll
+    for (int w = 0; w < NWARP; ++w) sum += wred[w][tid];
+    dacc[gacc * PU * 2 + tid] += sum;
+  }
+  if (tid == 0) bulk_wait_all();
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(A.counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int i = tid; i < ndots; i += NT) {
+    double sum = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) sum += __ldcg(&A.partials[(size_t)b * ndots + i]);
+    A.dots[i] = sum;
+  }
+  if (tid == 0) *A.counter = 0u;
+}
+
+// probes -> 8-byte cells [pair group][row]; probe p = g*PU + lane
+template <typename T>
+__global__ void k_cells8(int64_t dim, int ng, uint64_t seed, int64_t probe0, int nvalid,
+                         const int8_t *probes, T *out) {
+  constexpr int PU = Cell8<T>::PU;
+  const int64_t total = dim * ng * PU;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = (int)(t % PU);
+    const int64_t cell = t / PU;
+    const int64_t row = cell % dim;
+    const int g = (int)(cell / dim);
+    const int p = g * PU + lane;
+    T v = 0;
+    if (p < nvalid)
+      v = probes ? (T)probes[(int64_t)p * dim + row]
+                 : (T)el::rademacher(seed, (uint64_t)(probe0 + p), (uint64_t)row);
+    out[t] = v;
+  }
+}
+
+template <typename T>
+__global__ void k_d2_8(int n, int64_t dim, const double *diagV, const double *delta_bits, double c,
+                       double r, T *out) {
+  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < dim;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    double d = diagV[row];
+    for (int k = 0; k < n; ++k) if ((row >> k) & 1) d += delta_bits[k];
+    out[row] = (T)(2.0 * (d - c) / r);
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// A map: {chunk elems (256 B), chunks, groups}; B map: {pair elems (16 B), 2^(a-1), 2^(n-a), groups}
+template <typename T>
+int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap *mA, CUtensorMap *mB) {
+  auto enc = encode_fn();
+  if (!enc) return fail(ctx, EL_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const uint64_t dim = 1ull << n;
+  const uint64_t e256 = 256 / sizeof(T), e16 = 16 / sizeof(T);
+  {
+    cuuint64_t gdim[3] = {e256, dim * 8 / 256, (cuuint64_t)ng};
+    cuuint64_t gstr[2] = {256, dim * 8};
+    cuuint32_t box[3] = {(cuuint32_t)e256, (cuuint32_t)(1u << (a - 5)), 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(mA, dt, 3, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(ctx, EL_ECUDA, "tensor map A encode failed (%d)", (int)r);
+  }
+  {
+    cuuint64_t gdim[4] = {e16, 1ull << (a - 1), 1ull << (n - a), (cuuint64_t)ng};
+    cuuint64_t gstr[3] = {16, (1ull << a) * 8, dim * 8};
+    cuuint32_t box[4] = {(cuuint32_t)e16, 1, (cuuint32_t)hb, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = enc(mB, dt, 4, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(ctx, EL_ECUDA, "tensor map B encode failed (%d)", (int)r);
+  }
+  return EL_OK;
+}
+
+template <typename T>
+int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
+            const int8_t *probes_host, int num, double c, double r, std::vector<double> &acc) {
+  constexpr int PU = Cell8<T>::PU;
+  const int n = h->n;
+  const int64_t dim = h->basis->dim;
+  const int ng = chunk / PU;
+  const size_t vb = (size_t)dim * chunk * sizeof(T);
+  char *buf = (char *)el::workspace(ctx, 6, 2 * vb + (size_t)dim * sizeof(T) + 64);
+  if (!buf) return EL_ENOMEM;
+  void *P = buf, *Q = buf + vb;
+  T *d2 = reinterpret_cast<T *>(buf + 2 * vb);
+  int *d_err = reinterpret_cast<int *>(buf + 2 * vb + (size_t)dim * sizeof(T));
+  const int M = (num + 1) / 2;
+  double *d_dots = (double *)el::workspace(ctx, 7, (size_t)(M + 1) * chunk * 2 * sizeof(double));
+  if (!d_dots) return EL_ENOMEM;
+  int8_t *d_probe8 = nullptr;
+  if (probes_host) {
+    d_probe8 = (int8_t *)el::workspace(ctx, 2, (size_t)dim * chunk);
+    if (!d_probe8) return EL_ENOMEM;
+  }
+  EL_CUDA_TRY(ctx, cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
+  {
+    double *d_delta = (double *)el::workspace(ctx, 8, 64 * sizeof(double));
+    if (!d_delta) return EL_ENOMEM;
+    EL_CUDA_TRY(ctx, el::copy(ctx, d_delta, h->delta, 64 * sizeof(double), cudaMemcpyHostToDevice));
+    k_d2_8<T><<<el::grid_for(dim, 256), 256, 0, ctx->stream>>>(n, dim, h->d_diagV64, d_delta, c, r, d2);
+    EL_LAUNCH_CHECK(ctx);
+  }
+  const int a = std::min(13, std::max((n + 2) / 2, n - 12));
+  const int TBA = a, TBB = n - a + 1;
+  const int hb = (int)std::min<int64_t>(256, (int64_t)1 << (n - a));
+  CUtensorMap mA[2], mB[2];   // [P buffer, Q buffer]
+  int rc = make_maps<T>(ctx, P, n, a, ng, hb, &mA[0], &mB[0]);
+  if (rc) return rc;
+  rc = make_maps<T>(ctx, Q, n, a, ng, hb, &mA[1], &mB[1]);
+  if (rc) return rc;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  auto launch = [&](int kind, int mode, double s_m, int pbuf, double *dots) -> int {
+    TmaArgs<T> A;
+    memset(&A, 0, sizeof A);
+    const int TB = kind == KIND_B ? TBB : TBA;
+    A.n = n; A.a = a; A.mode = mode; A.ng = ng; A.dim = dim; A.hb = hb;
+    A.nbox = (int)(((int64_t)1 << (n - a)) / hb);
+    A.tiles = kind == KIND_A ? (dim >> a) : ((int64_t)1 << (a - 1));
+    A.items = A.tiles * ng;
+    A.log_tiles = 0;
+    while (((int64_t)1 << A.log_tiles) < A.tiles) ++A.log_tiles;
+    A.s_m = (T)s_m; A.two_r = (T)(2.0 / r); A.pro_alpha = (T)0.5; A.pro_beta = (T)(1.0 / r);
+    for (int k = 0; k < TB && k < 16; ++k) {
+      int rowbit = (kind == KIND_A) ? k : (k >= 1 ? a + k - 1 : -1);
+      A.amp[k] = (T)((rowbit >= 0) ? 0.5 * h->om_re[rowbit] : 0.0);
+    }
+    A.d2 = d2; A.dots = dots; A.err = d_err; A.counter = ctx->d_counter;
+    const int grid = (int)std::min<int64_t>(A.items, sms);
+    int e = el::ensure_partials(ctx, (size_t)grid * ng * PU * 2);
+    if (e) return e;
+    A.partials = ctx->d_partials;
+    const CUtensorMap &mp = kind == KIND_A ? mA[pbuf] : mB[pbuf];
+    const CUtensorMap &mq = kind == KIND_A ? mA[pbuf ^ 1] : mB[pbuf ^ 1];
+    const size_t smem = (size_t)3 * ((size_t)1 << TB) * 8;
+    bool ok = false;
+#define EL_TCASE(TBV, KV)                                                                     \
+  if (TB == TBV && kind == KV) {                                                              \
+    cudaFuncSetAttribute(k_kpm_tma<T, TBV, KV>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                         (int)smem);                                                          \
+    k_kpm_tma<T, TBV, KV><<<grid, NT, smem, ctx->stream>>>(A, mp, mq);                        \
+    ok = true;                                                                                \
+  }
+    EL_TCASE(10, KIND_A) EL_TCASE(11, KIND_A) EL_TCASE(12, KIND_A) EL_TCASE(13, KIND_A)
+    EL_TCASE(10, KIND_B) EL_TCASE(11, KIND_B) EL_TCASE(12, KIND_B) EL_TCASE(13, KIND_B)
+#undef EL_TCASE
+    if (!ok) return fail(ctx, EL_EINVAL, "TMA pass with %d tile bits not instantiated", TB);
+    EL_LAUNCH_CHECK(ctx);
+    return EL_OK;
+  };
+  std::vector<double> hd((size_t)(M + 1) * chunk * 2);
+  for (int done = 0; done < nvalid_total; done += chunk) {
+    const int b = std::min(chunk, nvalid_total - done);
+    if (probes_host)
+      EL_CUDA_TRY(ctx, el::copy(ctx, d_probe8, probes_host + (size_t)done * dim, (size_t)dim * b,
+                                cudaMemcpyHostToDevice));
+    // t_0 -> Q (buffer 1); the prologue writes p_1 into P (buffer 0)
+    k_cells8<T><<<el::grid_for(dim * chunk, 256), 256, 0, ctx->stream>>>(
+        dim, ng, seed, done, b, d_probe8, reinterpret_cast<T *>(Q));
+    EL_LAUNCH_CHECK(ctx);
+    int pbuf = 0;   // index of the buffer holding P this pass
+    rc = launch(KIND_B, MODE_PROLOGUE, 0.0, pbuf, d_dots);
+    if (rc) return rc;
+    for (int m = 1; m <= M; ++m) {
+      if ((m & 63) == 0 && el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
+      const int kind = (m & 1) ? KIND_A : KIND_B;
+      rc = launch(kind, m == M ? MODE_LAST : MODE_STEP, m == 1 ? 1.0 / r : 2.0 / r, pbuf,
+                  d_dots + (size_t)m * chunk * 2);
+      if (rc) return rc;
+      pbuf ^= 1;
+    }
+    EL_CUDA_TRY(ctx, el::copy(ctx, hd.data(), d_dots, hd.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    int herr = 0;
+    EL_CUDA_TRY(ctx, el::copy(ctx, &herr, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (herr) return fail(ctx, EL_ECUDA, "TMA transaction wait timed out in the KPM pass");
+    for (int p = 0; p < b; ++p) {
+      const double mu0 = hd[(size_t)p * 2];
+      const double mu1 = hd[((size_t)chunk + p) * 2 + 1];
+      acc[0] += mu0;
+      if (num >= 1) acc[1] += mu1;
+      for (int m = 1; m <= M; ++m) {
+        const double tt = hd[((size_t)m * chunk + p) * 2];
+        const double tq = hd[((size_t)m * chunk + p) * 2 + 1];
+        if (2 * m <= num) acc[2 * m] += 2.0 * tt - mu0;
+        if (m >= 2 && 2 * m - 1 <= num) acc[2 * m - 1] += 2.0 * tq - mu1;
+      }
+    }
+  }
+  return EL_OK;
+}
+
+}  // namespace
+
+namespace el {
+
+bool kpm_tma_eligible(const el_ham *h, int dtype, int chunk) {
+  if (h->basis->layout != EL_LAYOUT_FULL || h->complex_drive) return false;
+  if (h->n < 20 || h->n > 25) return false;
+  const int pu = (dtype == EL_F32) ? 2 : 1;
+  if (dtype != EL_F32 && dtype != EL_F64) return false;
+  return chunk % pu == 0 && chunk / pu <= 128;
+}
+
+int kpm_tma(el_ctx *ctx, el_ham *h, int dtype, int num, int nvec, int chunk, uint64_t seed,
+            const int8_t *probes_host, double c, double r, double *mu_host) {
+  std::vector<double> acc(num + 1, 0.0);
+  int rc = (dtype == EL_F32)
+               ? run_tma<float>(ctx, h, nvec, chunk, seed, probes_host, num, c, r, acc)
+               : run_tma<double>(ctx, h, nvec, chunk, seed, probes_host, num, c, r, acc);
+  if (rc) return rc;
+  const double norm = 1.0 / ((double)nvec * (double)h->basis->dim);
+  for (int k = 0; k <= num; ++k) mu_host[k] = acc[k] * norm;
+  return EL_OK;
+}
+
+}  // namespace el

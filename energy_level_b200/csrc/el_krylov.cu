@@ -135,6 +135,8 @@ extern "C" int el_kpm_moments(el_ctx *ctx, el_ham *h, int dtype, int num, int nv
   mode &= ~EL_KPM_GENERIC_KERNEL;
   if (mode != EL_KPM_DIRECT && mode != EL_KPM_DOUBLING) return fail(ctx, EL_EINVAL, "unknown KPM mode");
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (!force_generic && mode == EL_KPM_DOUBLING && el::kpm_tma_eligible(h, dtype, chunk))
+    return el::kpm_tma(ctx, h, dtype, num, nvec, chunk, seed, probes_host, c, r, mu_host);
   if (!force_generic && el::kpm_full_eligible(h, dtype, chunk, mode))
     return el::kpm_full(ctx, h, dtype, num, nvec, chunk, seed, probes_host, c, r, mu_host);
   const int64_t dim = h->basis->dim;

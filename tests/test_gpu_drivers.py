@@ -133,3 +133,32 @@ def test_tiled_kpm_matches_oracle(ctx, n, dtype, tol):
                               generic=True)
     assert np.abs(got - want).max() < tol
     assert np.abs(gen - want).max() < tol
+
+
+@pytest.mark.parametrize("n", [20, 22])
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-10), ("float32", 2e-4)])
+def test_tma_kpm_matches_generic_kernel(ctx, n, dtype, tol):
+    """TMA-fed tiled KPM (20 <= N <= 25) vs the row-parallel kernel on the same
+    probes, and the FP64 result vs the C oracle's direct recurrence."""
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import solvers
+    rng = np.random.default_rng(n)
+    om = rng.uniform(0.5, 2.0, n)
+    de = rng.uniform(-3, 3, n)
+    pos = [[6.0 * (i % 5), 6.0 * (i // 5), 0.0] for i in range(n)]
+    pairs = configs.pairs_from_positions(pos)
+    b = Basis(ctx, n, kind="full")
+    h = Hamiltonian(ctx, b, om, de, pairs)
+    lo, hi = solvers.bounds(h, max_iter=400, tol=1e-12)
+    c, r = solvers.kpm_scale(lo, hi)
+    nvec, num = 8, 21
+    z = rng.choice(np.array([-1, 1], dtype=np.int8), size=(nvec, 1 << n))
+    got = solvers.kpm_moments(h, num, nvec, c, r, dtype=dtype, chunk=8, probes=z, mode="doubling")
+    gen = solvers.kpm_moments(h, num, nvec, c, r, dtype="float64", chunk=8, probes=z, mode="direct",
+                              generic=True)
+    assert np.abs(got - gen).max() < tol
+    if n == 20 and dtype == "float64":
+        from oracle import build as ob
+        want = ob.kpm_full(n, om, ob.diag_full(n, de, pairs), c, r, num, z[:2])
+        got2 = solvers.kpm_moments(h, num, 2, c, r, dtype="float64", chunk=2, probes=z[:2])
+        assert np.abs(got2 - want).max() < 1e-10
