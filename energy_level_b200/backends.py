@@ -1,0 +1,201 @@
+"""Backend names, capabilities and routing for the drop-in boundary.
+
+The reference dispatches equilibrium work by name through EQ_BACKENDS
+(backends.py:112-118) and eq_route.solve_equilibrium (eq_route.py:340-490),
+and time evolution through TIME_BACKENDS -> runspec._ENGINE_TABLE
+(backends.py:48-110, 177-179; runspec.py:660-697).  This module declares the
+B200 backends in the same shapes:
+
+    EQ_BACKENDS   'b200-lanczos': ('gs',)   'b200-kpm': ('thermal', 'dos')
+    TIME_BACKENDS 'b200-cheb': TimeBackend(segments, projected, return_state)
+
+``solve_equilibrium`` accepts the reference's ``system`` dict and keyword
+arguments for these names and returns the same result keys as
+eq_route._solve_ground / _solve_thermal / _solve_dos.  ``install_into``
+registers the names into a reference backends module.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .model import ConfigConflict
+
+
+@dataclass(frozen=True)
+class TimeBackend:
+    module: str
+    function: str
+    aliases: tuple = ()
+    options: tuple = ()
+    segments: bool = False
+    projected: bool = False
+    gamma: bool = False
+    return_state: bool = False
+    charge: bool = False
+    order: bool = False
+    pauli: str = ''
+    native_state: str = ''
+    algorithm: str = ''
+
+
+EQ_BACKENDS = {
+    'b200-lanczos': ('gs',),
+    'b200-kpm': ('thermal', 'dos'),
+}
+
+TIME_BACKENDS = {
+    'b200-cheb': TimeBackend('energy_level_b200.engine', 'evolve_manybody',
+                             aliases=('b200', 'b200-ed', 'chebyshev-gpu'),
+                             options=(('memory_budget_mb', 'memory_budget_mb'), ('dtype', 'dtype'),
+                                      ('device', 'device')),
+                             segments=True, projected=True, gamma=False, return_state=True,
+                             algorithm='chebyshev'),
+}
+
+
+def normalize_equilibrium_backend(name, want):
+    name = str(name or '').lower()
+    name = {'kpm-b200': 'b200-kpm', 'lanczos-b200': 'b200-lanczos'}.get(name, name)
+    if name not in EQ_BACKENDS:
+        raise ValueError('未知 b200 平衡态后端 %r' % name)
+    if want not in EQ_BACKENDS[name]:
+        raise ValueError('平衡态后端 %r 不支持 want=%r' % (name, want))
+    return name
+
+
+def normalize_time_backend(name):
+    name = str(name or '').lower()
+    if name in TIME_BACKENDS:
+        return name
+    for canon, b in TIME_BACKENDS.items():
+        if name in b.aliases:
+            return canon
+    raise ValueError('未知多体 solver=%r；合法：%s' % (name, list(TIME_BACKENDS)))
+
+
+def validate_time_capabilities(name, *, segments=None, plan=None, gamma=None, return_state=False,
+                               charge_sector=None, psi0=None, pauli_strings=None, **_):
+    """Refuse what b200-cheb does not implement, with ConfigConflict keys
+    (backends.py:182-230 semantics)."""
+    b = TIME_BACKENDS[normalize_time_backend(name)]
+    if pauli_strings:
+        raise ConfigConflict('%s 不提供 Pauli 串观测' % name, keys=('manybody.pauli_strings',))
+    if segments and not b.segments:
+        raise ConfigConflict('%s 尚不支持 drive_segments' % name, keys=('manybody.drive_segments',))
+    if plan and plan.get('projected') and not b.projected:
+        raise ConfigConflict('%s 尚不支持 projected HamiltonianPlan' % name, keys=('manybody.constraint',))
+    if gamma is not None and np.any(np.asarray(gamma) != 0):
+        raise ConfigConflict('%s 仅支持 gamma=0' % name, keys=('manybody.gamma_mhz',))
+    if charge_sector is not None:
+        raise ConfigConflict('%s 尚不支持实时 charge_sector' % name, keys=('manybody.charge_sector',))
+    if isinstance(psi0, str) and psi0 == 'ground':
+        raise ValueError('%s 尚不支持 ground 初态；请先准备兼容初态' % name)
+
+
+def engine_entries():
+    """{(name, 'many'): (module, function)} like backends.py:177-179."""
+    return {(name, 'many'): (b.module, b.function) for name, b in TIME_BACKENDS.items()}
+
+
+def solve_equilibrium(system, want='gs', *, backend='b200-lanczos', betas=None, k=2, v0=None,
+                      seed=0, num=400, nvec=200, dtype=None, memory_budget_mb=None,
+                      return_state=False, sector=None, progress_arr=None, **unused):
+    """eq_route.solve_equilibrium for the b200 names (same result keys)."""
+    from . import kpm as bkpm
+    from .matrix_free import b200_lanczos_ground_state
+    if progress_arr is not None and float(progress_arr[1]) != 0:
+        raise RuntimeError('用户取消')
+    backend = normalize_equilibrium_backend(backend, want)
+    system = dict(system)
+    plan = system.get('plan') or {}
+    for key in ('Om', 'delta', 'gamma', 'terms'):
+        if system.get(key) is None and key in plan:
+            system[key] = plan[key]
+    if system.get('H') is not None or system.get('H_builder') is not None:
+        raise ValueError('%s 需要物理 calib；不能忽略显式 H/H_builder' % backend)
+    if 'calib' not in system:
+        raise ValueError("%s 后端需要 system['calib']" % backend)
+    n_sites = len(system['calib']['atoms'])
+    base = dict(want=want, backend=backend, n_sites=n_sites)
+    if want == 'gs':
+        constraint = None
+        if sector is not None or system.get('charge_sector') is not None:
+            kq = int(sector if sector is not None else system['charge_sector'])
+            if np.any(np.asarray(system.get('Om') if system.get('Om') is not None else 0) != 0):
+                raise ValueError('固定 charge_sector 要求 Omega=0')
+            constraint = {'kind': 'charge', 'k': kq}
+        from . import model, solvers
+        if constraint is not None:
+            ctx, basis, ham, _ = model.build(system['calib'], system.get('Om'), system.get('delta'),
+                                             system.get('gamma'), system.get('terms'),
+                                             constraint=constraint, device=system.get('device', 'cuda'))
+            r = solvers.lanczos_ground(ham, dtype=dtype or 'float64', seed=seed,
+                                       max_iter=min(300, basis.dim), tol=1e-9, nev=min(k, basis.dim),
+                                       return_vec=True)
+            vec = r['vec'].cpu().numpy()
+            codes = basis.codes().cpu().numpy()
+            bits = np.asarray([((codes >> (n_sites - 1 - i)) & 1) for i in range(n_sites)], float)
+            out = dict(base, sector=int(constraint['k']), charge_sector=int(constraint['k']),
+                       dim_sub=basis.dim, sector_idx=codes, E0=float(r['evals'][0]),
+                       gap=float(r['evals'][1] - r['evals'][0]) if len(r['evals']) > 1 else 0.0,
+                       evals=np.asarray(r['evals']), n_atom=bits @ (np.abs(vec) ** 2))
+            if return_state:
+                out['vec'] = vec.astype(np.complex128)
+            return out
+        r = b200_lanczos_ground_state(system['calib'], system.get('Om'), system.get('delta'),
+                                      system.get('gamma'), system.get('terms'),
+                                      m=system.get('krylov_dim', 300), seed=seed,
+                                      dtype=dtype or 'float64', device=system.get('device', 'cuda'),
+                                      return_state=True, memory_budget_mb=memory_budget_mb,
+                                      plan=plan if plan.get('projected') else None, nev=k)
+        vec = r.pop('vec')
+        if plan.get('projected'):
+            codes = np.asarray(r.pop('basis_states'), np.int64)
+        else:
+            codes = np.arange(1 << n_sites, dtype=np.int64)
+        bits = np.asarray([((codes >> (n_sites - 1 - i)) & 1) for i in range(n_sites)], float)
+        p = np.abs(vec) ** 2
+        obs = dict(n_atom=bits @ p)
+        if len(codes) <= (1 << 18):
+            ni = obs['n_atom']
+            obs['corr'] = (bits * p) @ bits.T - np.outer(ni, ni)
+        out = dict(base, **r, **obs)
+        out['backend'] = backend
+        if return_state:
+            out['vec'] = vec
+        return out
+    if want == 'thermal':
+        betas = np.atleast_1d(np.asarray([1.0] if betas is None else betas, float))
+        if betas.ndim != 1 or not len(betas) or not np.isfinite(betas).all() or np.any(betas <= 0):
+            raise ValueError('betas 须为非空、有限的正数数组')
+        th = bkpm.kpm_thermal_b200(system, betas, num=num, nvec=nvec, seed=seed,
+                                   dtype=dtype or 'float32', memory_budget_mb=memory_budget_mb,
+                                   device=system.get('device', 'cuda'), chunk=system.get('kpm_chunk', 32))
+        return dict(base, betas=th['betas'], E=th['E'], C=th['C'], F=th['F'])
+    if want == 'dos':
+        r = bkpm.kpm_dos_b200(system, num=num, nvec=nvec, seed=seed, dtype=dtype or 'float32',
+                              memory_budget_mb=memory_budget_mb, device=system.get('device', 'cuda'),
+                              chunk=system.get('kpm_chunk', 32))
+        return dict(base, energies=r['energies'], rho=r['rho'])
+    raise ValueError('want 需为 gs/thermal/dos，实=%r' % want)
+
+
+def install_into(reference_backends, shim_module='b200_shim'):
+    """Register the b200 names into a reference backends module in place:
+    EQ_BACKENDS gains 'b200-lanczos'/'b200-kpm', TIME_BACKENDS gains
+    'b200-cheb' (constructed with the module's own TimeBackend class).  The
+    reference resolves time engines as '.manybody.<module>' (backends.py:177),
+    so the entry names a shim module in that package that re-exports
+    energy_level_b200.engine.evolve_manybody."""
+    eq = reference_backends.EQ_BACKENDS
+    for name, wants in EQ_BACKENDS.items():
+        eq[name] = tuple(wants)
+    tb = reference_backends.TIME_BACKENDS
+    cls = getattr(reference_backends, 'TimeBackend', TimeBackend)
+    for name, b in TIME_BACKENDS.items():
+        tb[name] = cls(shim_module, b.function, aliases=b.aliases, options=b.options,
+                       segments=b.segments, projected=b.projected, gamma=b.gamma,
+                       return_state=b.return_state)
+    return reference_backends

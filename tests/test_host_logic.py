@@ -1,0 +1,128 @@
+"""CPU tests of the host layer: backend declarations and routing rules,
+model validation, state grammar, segment resolution, KPM post-processing."""
+import os
+import types
+
+import numpy as np
+import pytest
+
+from energy_level_b200 import backends, configs, engine, kpm as bkpm, model
+from energy_level_b200.state import state_vector
+from oracle import ref
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_backend_names_and_capabilities():
+    assert backends.normalize_equilibrium_backend("b200-lanczos", "gs") == "b200-lanczos"
+    assert backends.normalize_equilibrium_backend("kpm-b200", "dos") == "b200-kpm"
+    with pytest.raises(ValueError):
+        backends.normalize_equilibrium_backend("b200-kpm", "gs")
+    assert backends.normalize_time_backend("chebyshev-gpu") == "b200-cheb"
+    b = backends.TIME_BACKENDS["b200-cheb"]
+    assert b.segments and b.projected and b.return_state and not b.gamma
+    assert backends.engine_entries()[("b200-cheb", "many")] == ("energy_level_b200.engine", "evolve_manybody")
+
+
+def test_capability_refusals_are_config_conflicts():
+    with pytest.raises(model.ConfigConflict) as e:
+        backends.validate_time_capabilities("b200-cheb", gamma=[0.1, 0.0])
+    assert e.value.keys == ("manybody.gamma_mhz",)
+    with pytest.raises(model.ConfigConflict):
+        backends.validate_time_capabilities("b200-cheb", pauli_strings=[{"label": "x"}])
+    with pytest.raises(ValueError):
+        backends.validate_time_capabilities("b200-cheb", psi0="ground")
+    backends.validate_time_capabilities("b200-cheb", segments=[{"t0": 0}], plan={"projected": True})
+
+
+def test_install_into_reference_shaped_module():
+    from dataclasses import dataclass
+
+    @dataclass(frozen=True)
+    class TimeBackend:
+        module: str
+        function: str
+        aliases: tuple = ()
+        options: tuple = ()
+        segments: bool = False
+        projected: bool = False
+        gamma: bool = False
+        return_state: bool = False
+
+    fake = types.SimpleNamespace(EQ_BACKENDS={"ed": ("gs",)}, TIME_BACKENDS={}, TimeBackend=TimeBackend)
+    backends.install_into(fake)
+    assert fake.EQ_BACKENDS["b200-kpm"] == ("thermal", "dos")
+    assert fake.TIME_BACKENDS["b200-cheb"].module == "b200_shim"
+    assert fake.TIME_BACKENDS["b200-cheb"].projected
+
+
+def test_model_refuses_unimplemented_channels():
+    calib = configs.calib_from_positions(configs.chain_positions(4))
+    n, om, de, pairs = model.model_arrays(calib, np.ones(4), np.zeros(4))
+    assert n == 4 and len(pairs) == 6
+    bad = dict(calib, terms=["I1", "I2"])
+    bad["pairs"] = [dict(p, J=0.3) for p in calib["pairs"]]
+    with pytest.raises(model.ConfigConflict):
+        model.model_arrays(bad, np.ones(4), np.zeros(4))
+    with pytest.raises(model.ConfigConflict):
+        model.model_arrays(calib, np.ones(4), np.zeros(4), gamma=np.full(4, 0.1))
+    with pytest.raises(ValueError):
+        model.model_arrays(calib, np.ones(3), np.zeros(4))
+    with pytest.raises(ValueError):
+        model.model_arrays({"atoms": [], "pairs": []})
+
+
+def test_state_grammar_full_and_projected():
+    n = 6
+    codes = ref.independent_states(n, configs.chain_edges(n), None)
+    v = state_vector("rgrgrg", n, codes)
+    assert np.count_nonzero(v) == 1 and v[np.searchsorted(codes, 0b101010)] == 1
+    full = state_vector(None, n)
+    assert full[0] == 1 and np.linalg.norm(full) == pytest.approx(1.0)
+    with pytest.raises(ValueError):
+        state_vector("rrgggg", n, codes)     # weight outside the blockade basis
+    sup = state_vector(("sup", [("gggggg", 1.0), ("rggggg", 1.0)]), n, codes)
+    assert np.allclose(np.abs(sup[sup != 0]), 1 / np.sqrt(2))
+    prod = state_vector([[1, 1]] * 2 + ["g"] * 4, 4 + 2)
+    assert np.count_nonzero(prod) == 4
+
+
+def test_segment_rules_match_oracle():
+    n = 3
+    segs = [{"t0": 0.0, "Om": [1, 1, 1], "delta": [0, 0, 0]},
+            {"t0": 5.0, "Om": [2, 2, 2], "delta": [1, 1, 1], "phase": [0.5, 0, 0]}]
+    assert engine.segment_intervals(0.0, 10.0, segs) == ref.segment_intervals(0.0, 10.0, segs)
+    om, de = engine.segment_drive(7.0, segs, n)
+    om2, de2 = ref.segment_drive(7.0, segs, n)
+    assert np.allclose(om, om2) and np.allclose(de, de2)
+    om3, de3 = engine.segment_drive(2.0, segs, n, interp="midpoint")
+    assert np.allclose(om3, 0.5 * (np.ones(3) + 2.0 * np.exp(1j * np.array([0.5, 0.0, 0.0]))))
+    assert np.allclose(de3, 0.5)
+    with pytest.raises(ValueError):
+        engine.time_grid([0.0])
+    with pytest.raises(RuntimeError, match="用户取消"):
+        engine.check_cancel(np.array([0.0, 1.0]))
+
+
+def test_kpm_postprocessing_matches_reference_golden():
+    g = np.load(os.path.join(GOLD, "kpm.npz"))
+    num = int(g["num"])
+    assert np.max(np.abs(bkpm.jackson_kernel(num) - g["jackson"])) < 1e-15
+    rho = bkpm.dos_from_moments(g["mu"], float(g["c"]), float(g["r"]), g["energies"], num)
+    assert np.max(np.abs(rho - g["rho"])) < 1e-12
+    c, r = bkpm.kpm_scale(float(g["emin"]), float(g["emax"]))
+    assert abs(c - float(g["c"])) < 1e-12 and abs(r - float(g["r"])) < 1e-12
+
+
+def test_kpm_thermal_from_exact_moments_matches_spectrum():
+    g = np.load(os.path.join(GOLD, "kpm.npz"))
+    n = int(g["n"])
+    H = ref.dense_h(n, None, g["om"], g["de"], [(int(i), int(j), v) for i, j, v in g["pairs"]])
+    w = np.linalg.eigvalsh(H)
+    c, r = float(g["c"]), float(g["r"])
+    mu = ref.kpm_moments_exact(H, 512, c, r)
+    th = bkpm.thermal_from_moments(len(w), [0.1, 0.5], (mu, c, r), 512)
+    for i, b in enumerate([0.1, 0.5]):
+        p = np.exp(-b * (w - w.min()))
+        E = float(p @ w / p.sum())
+        assert abs(th["E"][i] - E) < 1e-5
