@@ -59,6 +59,11 @@ PROTOTYPES = {
                                  C.c_int, C.c_double, C.c_double, _dp]),
     "el_lanczos_ground": (C.c_int, [_vp, _vp, C.c_int, _vp, _u64, C.c_int, C.c_int, C.c_double,
                                     C.c_int, C.c_int, _dp, _dp, _ip, _ip, _vp]),
+    "el_batch_create": (C.c_int, [_vp, C.c_int, _vp, _vp, _dp, _dp, _vp, _vp, _vp, _dp, C.c_int, C.c_int,
+                                  C.c_double, C.POINTER(_vp)]),
+    "el_batch_run": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _u64]),
+    "el_batch_results": (C.c_int, [_vp, _vp, _dp, _dp, _dp, _vp, _vp]),
+    "el_batch_destroy": (C.c_int, [_vp]),
     "el_cheb_step": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, _ip]),
     "el_observables": (C.c_int, [_vp, _vp, C.c_int, _vp, _dp, _dp]),
 }

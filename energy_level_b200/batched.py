@@ -1,0 +1,144 @@
+"""Batched ground states: hundreds of independent instances, one launch.
+
+``BatchedGroundStates`` describes the batch once on the device
+(el_batch_create), runs it as ONE persistent kernel (el_batch_run: CTAs pull
+instances from an atomic queue, largest sector first) and reads the results
+(el_batch_results).  ``autotune`` picks threads per CTA and CTAs per SM by
+timing the candidates on the batch itself (CUDA events), ``capture`` records
+the run in a CUDA graph for repeated solves.  The per-instance result keys
+follow the reference's ground-state dicts (E0, gap, residuals, converged;
+matrix_free.py:273-276) as arrays over the batch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .core import _torch, default_context
+from .model import model_arrays
+
+_TUNED = {}
+
+
+def _layout(n, edges):
+    if not edges:
+        return _lib.EL_LAYOUT_FULL
+    es = sorted({tuple(sorted((int(a), int(b)))) for a, b in edges})
+    chain = [(i, i + 1) for i in range(n - 1)]
+    if es == chain:
+        return _lib.EL_LAYOUT_CHAIN
+    if n >= 3 and es == sorted(chain + [(0, n - 1)]):
+        return _lib.EL_LAYOUT_RING
+    raise ValueError('batched solves support nearest-neighbour chain/ring blockade sectors '
+                     'or full bases')
+
+
+class BatchedGroundStates:
+    def __init__(self, instances, dtype='float32', max_iter=200, tol=None, device=0, ctx=None):
+        if dtype not in ('float32', 'float64'):
+            raise ValueError('dtype 必须为 float32/float64')
+        self.ctx = ctx or default_context(device)
+        ns, lays, om, de, poff, pi, pj, V = [], [], [], [], [0], [], [], []
+        for inst in instances:
+            n, o, d, pairs = model_arrays(inst['calib'], inst.get('Om'), inst.get('delta'),
+                                          inst.get('gamma'), inst.get('terms'))
+            if np.any(o.imag != 0):
+                raise ValueError('batched solves need real Omega')
+            ns.append(n)
+            lays.append(_layout(n, inst.get('edges')))
+            om.extend(o.real.tolist())
+            de.extend(d.tolist())
+            for i, j, v in pairs:
+                pi.append(i); pj.append(j); V.append(v)
+            poff.append(len(V))
+        self.count = len(ns)
+        self.n_sites = np.asarray(ns)
+        self.dtype = dtype
+        self.tol = float(tol if tol is not None else (1e-5 if dtype == 'float32' else 1e-10))
+        arr = lambda x, t: np.ascontiguousarray(np.asarray(x, dtype=t))
+        self._keep = [arr(ns, np.int32), arr(lays, np.int32), arr(om, np.float64), arr(de, np.float64),
+                      arr(poff, np.int32), arr(pi if pi else [0], np.int32), arr(pj if pj else [0], np.int32),
+                      arr(V if V else [0.0], np.float64)]
+        k = self._keep
+        h = C.c_void_p()
+        self.ctx.call('el_batch_create', C.c_int(self.count), C.c_void_p(k[0].ctypes.data),
+                      C.c_void_p(k[1].ctypes.data), _lib.dptr(k[2]), _lib.dptr(k[3]),
+                      C.c_void_p(k[4].ctypes.data), C.c_void_p(k[5].ctypes.data),
+                      C.c_void_p(k[6].ctypes.data), _lib.dptr(k[7]), C.c_int(_lib.DTYPES[dtype]),
+                      C.c_int(int(max_iter)), C.c_double(self.tol), C.byref(h))
+        self.handle = h
+        self.config = (512, 1)
+        self.signature = (self.count, tuple(np.bincount(self.n_sites).tolist()), dtype, int(max_iter))
+
+    def run(self, threads=None, ctas_per_sm=None, seed=0):
+        t, c = self.config
+        self.ctx.call('el_batch_run', self.handle, C.c_int(int(threads or t)),
+                      C.c_int(int(ctas_per_sm or c)), C.c_uint64(int(seed)))
+
+    def results(self):
+        e0 = np.zeros(self.count)
+        gap = np.zeros(self.count)
+        res = np.zeros(self.count)
+        it = np.zeros(self.count, np.int32)
+        cv = np.zeros(self.count, np.int32)
+        self.ctx.call('el_batch_results', self.handle, _lib.dptr(e0), _lib.dptr(gap), _lib.dptr(res),
+                      C.c_void_p(it.ctypes.data), C.c_void_p(cv.ctypes.data))
+        return dict(E0=e0, gap=gap, residuals=res, iters=it, converged=cv.astype(bool),
+                    backend='b200-batch-lanczos', dtype=self.dtype, tolerance=self.tol)
+
+    def autotune(self, candidates=((256, 1), (256, 2), (512, 1), (512, 2), (1024, 1)), reps=1):
+        """Time each (threads, ctas_per_sm) on this batch; keep the fastest."""
+        torch = _torch()
+        if self.signature in _TUNED:
+            self.config = _TUNED[self.signature][0]
+            return _TUNED[self.signature]
+        timings = {}
+        stream = torch.cuda.current_stream()
+        for cand in candidates:
+            self.run(*cand)            # sizes the workspace, warms the code path
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            for _ in range(reps):
+                self.run(*cand)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            timings[cand] = ev0.elapsed_time(ev1) / reps
+        best = min(timings, key=timings.get)
+        self.config = best
+        _TUNED[self.signature] = (best, timings)
+        return best, timings
+
+    def capture(self, seed=0):
+        """CUDA graph of one batched solve with the current configuration."""
+        torch = _torch()
+        self.run(seed=seed)            # workspace sized outside capture
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.run(seed=seed)
+        return g
+
+    def close(self):
+        if getattr(self, 'handle', None):
+            self.ctx.lib.el_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batched_ground_states(instances, dtype='float32', max_iter=200, tol=None, device=0, tune=False):
+    b = BatchedGroundStates(instances, dtype=dtype, max_iter=max_iter, tol=tol, device=device)
+    if tune:
+        b.autotune()
+    b.run()
+    out = b.results()
+    out['config'] = b.config
+    b.close()
+    return out

@@ -1,0 +1,595 @@
+// Batched Lanczos ground states: many independent Hamiltonians with uneven
+// sector dimensions in ONE persistent launch.
+//
+// Every CTA pulls instances from an atomic queue (the host orders them by
+// decreasing dimension, so the longest solves start first) and runs the whole
+// three-term Lanczos recurrence of one instance on its own slice of the
+// workspace:
+//   w = H v_j - beta_j v_{j-1};  alpha_j = <v_j, w>;  w -= alpha_j v_j
+// Vectors are FP32 (or FP64); alpha/beta, the omega recurrence of partial
+// reorthogonalisation (Simon 1984) and the tridiagonal eigensolve are FP64.
+// The two lowest Ritz values come from a warp-parallel Sturm multisection;
+// the residual estimate beta_{j+1} |s_j| of the lowest pair from inverse
+// iteration on one thread.  Convergence: residual estimate of both pairs
+// <= tol * max(1, |theta|).  H follows channels.py:58-132 (diagonal
+// delta n + V n n, sigma^x with Omega/2) on nearest-neighbour chain / ring
+// blockade sectors (Zeckendorf ranking) or full bases; this is the batched
+// counterpart of the reference's dense batched_ground_state
+// (equilibrium.py:251-311) and of per-instance eigsh calls (eq_route.py:540).
+#include "el_internal.cuh"
+
+#include <algorithm>
+#include <numeric>
+
+namespace {
+
+using el::fail;
+
+constexpr int MAXIT = 384;      // Krylov steps per instance (workspace rows)
+constexpr int MAXN = 40;        // sites per instance
+
+struct Inst {
+  int n, layout, pad0, pad1;
+  int64_t dim, off;             // rows and offset into the concatenated diagonal
+  double om[MAXN];              // Omega/2 per bit position
+};
+
+struct BatchArgs {
+  int count, max_iter, use_fp64, pad;
+  double tol, eps;
+  const Inst *inst;             // [count], processing order
+  const double *diag;           // concatenated diagonal (FP64)
+  void *ws;                     // per-CTA workspace: (max_iter + 2) * dim_max values
+  int64_t dim_max;
+  unsigned int *queue;
+  uint64_t seed;
+  double *e0, *e1, *res, *gap;  // outputs in processing order
+  int *iters, *conv;
+};
+
+
+template <int NT>
+__device__ double block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < NT / 32; ++w) s += red[w];   // same order on every thread
+  return s;
+}
+
+// Sturm count of eigenvalues of T (a[0..m-1], b[0..m-2]) below x.
+__device__ int sturm(const double *a, const double *b, int m, double x) {
+  int cnt = 0;
+  double q = a[0] - x;
+  if (q < 0) ++cnt;
+  for (int i = 1; i < m; ++i) {
+    if (fabs(q) < 1e-300) q = (q < 0 ? -1e-300 : 1e-300);
+    q = a[i] - x - b[i - 1] * b[i - 1] / q;
+    if (q < 0) ++cnt;
+  }
+  return cnt;
+}
+
+// k-th smallest eigenvalue by 32-way multisection within one warp.
+__device__ double warp_eig(const double *a, const double *b, int m, int k, double lo, double hi) {
+  const int lane = threadIdx.x & 31;
+  for (int round = 0; round < 14; ++round) {
+    const double x = lo + (hi - lo) * (lane + 1) / 33.0;
+    const int c = sturm(a, b, m, x);
+    const unsigned below = __ballot_sync(0xffffffffu, c > k);   // points above the eigenvalue
+    const int first = below ? (__ffs(below) - 1) : 32;
+    const double nlo = lo + (hi - lo) * first / 33.0;
+    const double nhi = lo + (hi - lo) * (first + 1) / 33.0;
+    lo = nlo;
+    hi = nhi;
+    if (hi - lo <= 1e-15 * fmax(1.0, fabs(hi))) break;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// Last component of the unit eigenvector of T for eigenvalue lam (inverse
+// iteration with a pivoted tridiagonal LU, one thread).
+__device__ double last_component(const double *a, const double *b, int m, double lam, double *work) {
+  if (m == 1) return 1.0;
+  double *d = work, *u1 = work + m, *u2 = work + 2 * m, *l = work + 3 * m, *x = work + 4 * m;
+  int *piv = (int *)(work + 5 * m);
+  double scale = 0.0;
+  for (int i = 0; i < m; ++i) scale = fmax(scale, fabs(a[i]) + (i < m - 1 ? fabs(b[i]) : 0.0));
+  const double eps = 2.2e-16 * fmax(scale, 1e-300);
+  double cd = a[0] - lam, cu1 = b[0], cu2 = 0.0;
+  for (int i = 0; i < m - 1; ++i) {
+    const double sub = b[i], nd = a[i + 1] - lam, nu1 = (i + 1 < m - 1) ? b[i + 1] : 0.0;
+    if (fabs(cd) >= fabs(sub)) {
+      piv[i] = 0;
+      double dv = fabs(cd) < eps ? (cd < 0 ? -eps : eps) : cd;
+      const double f = sub / dv;
+      l[i] = f; d[i] = dv; u1[i] = cu1; u2[i] = cu2;
+      cd = nd - f * cu1; cu1 = nu1 - f * cu2; cu2 = 0.0;
+    } else {
+      piv[i] = 1;
+      const double f = cd / sub;
+      l[i] = f; d[i] = sub; u1[i] = nd; u2[i] = nu1;
+      cd = cu1 - f * nd; cu1 = cu2 - f * nu1; cu2 = 0.0;
+    }
+  }
+  d[m - 1] = fabs(cd) < eps ? (cd < 0 ? -eps : eps) : cd;
+  for (int i = 0; i < m; ++i) x[i] = 1.0 + 0.01 * sin(1.0 + i);
+  for (int it = 0; it < 3; ++it) {
+    for (int i = 0; i < m - 1; ++i) {
+      if (piv[i]) { const double t = x[i]; x[i] = x[i + 1]; x[i + 1] = t; }
+      x[i + 1] -= l[i] * x[i];
+    }
+    for (int i = m - 1; i >= 0; --i) {
+      double s = x[i];
+      if (i + 1 < m) s -= u1[i] * x[i + 1];
+      if (i + 2 < m) s -= u2[i] * x[i + 2];
+      x[i] = s / d[i];
+    }
+    double nrm = 0.0;
+    for (int i = 0; i < m; ++i) nrm += x[i] * x[i];
+    nrm = sqrt(nrm);
+    if (!(nrm > 0) || !isfinite(nrm)) return 1.0;
+    for (int i = 0; i < m; ++i) x[i] /= nrm;
+  }
+  return fabs(x[m - 1]);
+}
+
+__device__ __forceinline__ uint64_t unrank_b(const Inst &I, const uint64_t *fib, int64_t row) {
+  if (I.layout == EL_LAYOUT_FULL) return (uint64_t)row;
+  uint64_t r = (uint64_t)row, c = 0;
+  const int n = I.n;
+  if (I.layout == EL_LAYOUT_CHAIN) {
+    for (int k = n - 1; k >= 0; --k) { const uint64_t w = fib[k + 2]; if (r >= w) { c |= 1ULL << k; r -= w; } }
+    return c;
+  }
+  if (r < fib[n + 1]) {
+    for (int k = n - 2; k >= 0; --k) { const uint64_t w = fib[k + 2]; if (r >= w) { c |= 1ULL << k; r -= w; } }
+    return c;
+  }
+  r -= fib[n + 1];
+  c = 1ULL << (n - 1);
+  for (int k = n - 3; k >= 1; --k) { const uint64_t w = fib[k + 1]; if (r >= w) { c |= 1ULL << k; r -= w; } }
+  return c;
+}
+
+__device__ __forceinline__ int64_t ring_rank(const uint64_t *fib, int n, uint64_t c) {
+  int64_t r = 0;
+  if ((c >> (n - 1)) & 1ULL) {
+    r = (int64_t)fib[n + 1];
+    uint64_t m = c & ~(1ULL << (n - 1));
+    while (m) { const int k = __ffsll((long long)m) - 1; r += (int64_t)fib[k + 1]; m &= m - 1; }
+  } else {
+    uint64_t m = c;
+    while (m) { const int k = __ffsll((long long)m) - 1; r += (int64_t)fib[k + 2]; m &= m - 1; }
+  }
+  return r;
+}
+
+__device__ __forceinline__ int64_t flip_b(const Inst &I, const uint64_t *fib, uint64_t code,
+                                          int64_t row, int k) {
+  const uint64_t bit = 1ULL << k;
+  const bool set = (code & bit) != 0;
+  if (I.layout == EL_LAYOUT_FULL) return row ^ (int64_t)bit;
+  const int n = I.n;
+  uint64_t adj = 0;
+  if (k + 1 < n) adj |= bit << 1;
+  if (k > 0) adj |= bit >> 1;
+  if (I.layout == EL_LAYOUT_RING) {
+    if (k == 0) adj |= 1ULL << (n - 1);
+    if (k == n - 1) adj |= 1ULL;
+  }
+  if (!set && (code & adj)) return -1;
+  if (I.layout == EL_LAYOUT_CHAIN) {
+    const int64_t w = (int64_t)fib[k + 2];
+    return set ? row - w : row + w;
+  }
+  if (k == n - 1) return ring_rank(fib, n, code ^ bit);
+  const bool top = (code >> (n - 1)) & 1ULL;
+  const int64_t w = (int64_t)(top ? fib[k + 1] : fib[k + 2]);
+  return set ? row - w : row + w;
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_lanczos_batch(const BatchArgs A) {
+  __shared__ Inst I;
+  __shared__ uint64_t fib[MAXN + 3];
+  __shared__ double red[NT / 32];
+  __shared__ double al[MAXIT], be[MAXIT];
+  __shared__ double wcur[MAXIT + 2], wprev[MAXIT + 2];
+  __shared__ double work[8 * MAXIT + 8];   // [0, MAXIT): omega row; [2 MAXIT, 8 MAXIT): inverse iteration
+  __shared__ int s_idx, s_flag, s_done, s_force;
+  __shared__ double s_th[2], s_res[2];
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    fib[0] = 0; fib[1] = 1;
+    for (int i = 2; i < MAXN + 3; ++i) fib[i] = fib[i - 1] + fib[i - 2];
+  }
+  T *Vb = reinterpret_cast<T *>(A.ws) + (size_t)blockIdx.x * (A.max_iter + 2) * A.dim_max;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_idx = (int)atomicAdd(A.queue, 1u);
+    __syncthreads();
+    const int idx = s_idx;
+    if (idx >= A.count) break;
+    if (tid == 0) I = A.inst[idx];
+    __syncthreads();
+    const int64_t dim = I.dim;
+    const double *D = A.diag + I.off;
+    const int m = (int)min((int64_t)A.max_iter, dim);
+    T *W = Vb + (size_t)(A.max_iter + 1) * A.dim_max;
+    // start vector: counter-based Gaussian, normalised
+    double nrm = 0.0;
+    for (int64_t r = tid; r < dim; r += NT) {
+      const uint64_t h1 = el::counter_hash(A.seed + idx, 0x77, (uint64_t)r);
+      const uint64_t h2 = el::counter_hash(A.seed + idx, 0x99, (uint64_t)r);
+      const double u1 = ((h1 >> 11) + 1.0) * (1.0 / 9007199254740993.0);
+      const double u2 = (h2 >> 11) * (1.0 / 9007199254740992.0);
+      const T v = (T)(sqrt(-2.0 * log(u1)) * cospi(2.0 * u2));
+      Vb[r] = v;
+      nrm += (double)v * (double)v;
+    }
+    nrm = block_sum<NT>(nrm, red);
+    {
+      const T sc = (T)(1.0 / sqrt(nrm));
+      for (int64_t r = tid; r < dim; r += NT) Vb[r] *= sc;
+    }
+    if (tid == 0) { wcur[0] = 1.0; s_force = 0; s_done = 0; s_th[0] = s_th[1] = 0.0; s_res[0] = s_res[1] = 1e300; }
+    __syncthreads();
+    double beta = 0.0, anorm = 0.0;
+    int j = 0, steps = 0;
+    for (j = 0; j < m; ++j) {
+      const T *v = Vb + (size_t)j * A.dim_max;
+      const T *vp = j ? Vb + (size_t)(j - 1) * A.dim_max : nullptr;
+      // w = H v - beta v_prev ; alpha = <v, w>
+      double pa = 0.0;
+      for (int64_t r = tid; r < dim; r += NT) {
+        const uint64_t code = unrank_b(I, fib, r);
+        double h = D[r] * (double)v[r];
+        for (int k = 0; k < I.n; ++k) {
+          const double amp = I.om[k];
+          if (amp == 0.0) continue;
+          const int64_t t = flip_b(I, fib, code, r, k);
+          if (t >= 0) h += amp * (double)v[t];
+        }
+        const T wv = (T)(h - (vp ? beta * (double)vp[r] : 0.0));
+        W[r] = wv;
+        pa += (double)v[r] * (double)wv;
+      }
+      const double alpha = block_sum<NT>(pa, red);
+      double pn = 0.0;
+      for (int64_t r = tid; r < dim; r += NT) {
+        const T wv = (T)((double)W[r] - alpha * (double)v[r]);
+        W[r] = wv;
+        pn += (double)wv * (double)wv;
+      }
+      double b2 = block_sum<NT>(pn, red);
+      anorm = fmax(anorm, fabs(alpha) + beta);
+      double bnext = sqrt(fmax(b2, 0.0));
+      // partial reorthogonalisation: omega recurrence on thread 0
+      if (tid == 0) {
+        al[j] = alpha;
+        int flag = s_force;
+        s_force = 0;
+        if (j > 0 && bnext > 0) {
+          double wmax = 0.0;
+          for (int k = 0; k < j; ++k) {
+            double t = be[k] * wcur[k + 1] + (al[k] - alpha) * wcur[k] - beta * (k < j - 0 ? wprev[k] : 0.0);
+            if (k > 0) t += be[k - 1] * wcur[k - 1];
+            t /= bnext;
+            t += (t >= 0 ? 1.0 : -1.0) * A.eps * anorm / bnext;
+            work[k] = t;
+            wmax = fmax(wmax, fabs(t));
+          }
+          if (wmax > sqrt(A.eps)) flag = 1;
+        }
+        s_flag = flag;
+      }
+      __syncthreads();
+      if (s_flag && j > 0) {
+        for (int pass = 0; pass < 2; ++pass) {
+          for (int k = 0; k <= j; ++k) {
+            const T *vk = Vb + (size_t)k * A.dim_max;
+            double pc = 0.0;
+            for (int64_t r = tid; r < dim; r += NT) pc += (double)vk[r] * (double)W[r];
+            const double cc = block_sum<NT>(pc, red);
+            for (int64_t r = tid; r < dim; r += NT) W[r] = (T)((double)W[r] - cc * (double)vk[r]);
+          }
+        }
+        double pn2 = 0.0;
+        for (int64_t r = tid; r < dim; r += NT) pn2 += (double)W[r] * (double)W[r];
+        b2 = block_sum<NT>(pn2, red);
+        bnext = sqrt(fmax(b2, 0.0));
+      }
+      if (tid == 0) {
+        // advance the omega recurrence (reset after a reorthogonalisation)
+        if (j == 0) {
+          wprev[0] = 1.0;
+          wcur[0] = A.eps; wcur[1] = 1.0;
+        } else {
+          for (int k = 0; k <= j - 1; ++k) wprev[k] = wcur[k];
+          wprev[j] = wcur[j];
+          if (s_flag) {
+            for (int k = 0; k <= j; ++k) wcur[k] = A.eps;
+            s_force = 1;   // Simon: also orthogonalise the next vector
+          } else {
+            for (int k = 0; k < j; ++k) wcur[k] = work[k];
+            wcur[j] = A.eps * sqrt((double)dim);
+          }
+          wcur[j + 1] = 1.0;
+        }
+        be[j] = bnext;
+      }
+      __syncthreads();   // al/be/omega rows visible to warp 0 and everyone
+      steps = j + 1;
+      const bool invariant = !(bnext > 1e-12 * fmax(1.0, anorm));
+      const bool check = invariant || (j + 1 == m) || ((steps >= 2) && (steps % 8 == 0));
+      if (check && tid < 32) {
+        const int mm = steps;
+        double lo = 1e300, hi = -1e300;
+        for (int i = 0; i < mm; ++i) {
+          const double rr = (i > 0 ? fabs(be[i - 1]) : 0.0) + (i + 1 < mm ? fabs(be[i]) : 0.0);
+          lo = fmin(lo, al[i] - rr);
+          hi = fmax(hi, al[i] + rr);
+        }
+        lo -= 1e-9 * fmax(1.0, fabs(lo));
+        hi += 1e-9 * fmax(1.0, fabs(hi));
+        const int ne = mm >= 2 ? 2 : 1;
+        for (int q = 0; q < ne; ++q) {
+          const double th = warp_eig(al, be, mm, q, lo, hi);
+          if (tid == 0) {
+            s_th[q] = th;
+            s_res[q] = bnext * last_component(al, be, mm, th, work + 2 * MAXIT);
+          }
+        }
+        if (tid == 0) {
+          bool ok = (ne == 2);
+          for (int q = 0; q < ne; ++q) ok = ok && (s_res[q] <= A.tol * fmax(1.0, fabs(s_th[q])));
+          s_done = (ok || invariant || j + 1 == m) ? 1 : 0;
+        }
+      }
+      __syncthreads();
+      if (s_done) break;
+      // v_{j+1} = w / beta
+      T *vn = Vb + (size_t)(j + 1) * A.dim_max;
+      const double inv = 1.0 / bnext;
+      for (int64_t r = tid; r < dim; r += NT) vn[r] = (T)((double)W[r] * inv);
+      beta = bnext;
+      __syncthreads();
+    }
+    if (tid == 0) {
+      A.e0[idx] = s_th[0];
+      A.e1[idx] = s_th[1];
+      A.gap[idx] = s_th[1] - s_th[0];
+      A.res[idx] = fmax(s_res[0], s_res[1]);
+      A.iters[idx] = steps;
+      A.conv[idx] = (s_res[0] <= A.tol * fmax(1.0, fabs(s_th[0])) &&
+                     s_res[1] <= A.tol * fmax(1.0, fabs(s_th[1]))) ? 1 : 0;
+    }
+  }
+}
+
+// diagonal of every instance: V part + delta part, concatenated
+__global__ void k_batch_diag(int count, const Inst *inst, const double *Vmats, const double *deltas,
+                             double *diag) {
+  __shared__ uint64_t fib[MAXN + 3];
+  if (threadIdx.x == 0) {
+    fib[0] = 0; fib[1] = 1;
+    for (int i = 2; i < MAXN + 3; ++i) fib[i] = fib[i - 1] + fib[i - 2];
+  }
+  __syncthreads();
+  for (int i = blockIdx.y; i < count; i += gridDim.y) {
+    const Inst &I = inst[i];
+    const double *V = Vmats + (size_t)i * MAXN * MAXN;
+    const double *dl = deltas + (size_t)i * MAXN;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < I.dim;
+         r += (int64_t)gridDim.x * blockDim.x) {
+      const uint64_t code = unrank_b(I, fib, r);
+      double s = 0.0;
+      uint64_t m = code;
+      while (m) {
+        const int k = __ffsll((long long)m) - 1;
+        m &= m - 1;
+        s += dl[k];
+        uint64_t m2 = m;
+        while (m2) {
+          const int k2 = __ffsll((long long)m2) - 1;
+          m2 &= m2 - 1;
+          s += V[k * MAXN + k2];
+        }
+      }
+      diag[I.off + r] = s;
+    }
+  }
+}
+
+uint64_t fibh(int i) { uint64_t a = 0, b = 1; for (int k = 0; k < i; ++k) { uint64_t t = a + b; a = b; b = t; } return a; }
+
+struct el_batch_impl {
+  int count = 0, dtype = 0, max_iter = 0;
+  double tol = 0;
+  int64_t total_rows = 0, dim_max = 0;
+  std::vector<int> order;           // processing position -> caller index
+  Inst *d_inst = nullptr;
+  double *d_diag = nullptr;
+  double *d_out = nullptr;          // 4 doubles per instance
+  int *d_iout = nullptr;            // 2 ints per instance
+  unsigned *d_queue = nullptr;
+  void *ws = nullptr;
+  size_t ws_bytes = 0;
+  int device = 0;
+};
+
+}  // namespace
+
+struct el_batch : el_batch_impl {};
+
+extern "C" {
+
+int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_t *layouts,
+                    const double *omega, const double *delta, const int32_t *pair_off,
+                    const int32_t *pi, const int32_t *pj, const double *V, int dtype,
+                    int max_iter, double tol, el_batch **out) {
+  if (!ctx || !out || count < 1 || !n_sites || !layouts || !omega || !delta || !pair_off) return EL_EINVAL;
+  *out = nullptr;
+  if (dtype != EL_F32 && dtype != EL_F64) return fail(ctx, EL_EINVAL, "batched Lanczos vectors must be EL_F32 or EL_F64");
+  if (max_iter < 2 || max_iter > MAXIT) return fail(ctx, EL_EINVAL, "max_iter must be in [2, %d]", MAXIT);
+  if (!(tol > 0) || !std::isfinite(tol)) return fail(ctx, EL_EINVAL, "tol must be positive");
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  std::vector<int64_t> dims(count);
+  for (int i = 0; i < count; ++i) {
+    const int n = n_sites[i];
+    if (n < 1 || n > MAXN) return fail(ctx, EL_EINVAL, "instance %d: n must be in [1, %d]", i, MAXN);
+    if (layouts[i] == EL_LAYOUT_CHAIN) dims[i] = (int64_t)fibh(n + 2);
+    else if (layouts[i] == EL_LAYOUT_RING) {
+      if (n < 3) return fail(ctx, EL_EINVAL, "instance %d: ring needs n >= 3", i);
+      dims[i] = (int64_t)(fibh(n + 1) + fibh(n - 1));
+    } else if (layouts[i] == EL_LAYOUT_FULL) {
+      if (n > 24) return fail(ctx, EL_EINVAL, "instance %d: full basis in a batch limited to n <= 24", i);
+      dims[i] = 1LL << n;
+    } else {
+      return fail(ctx, EL_EINVAL, "instance %d: layout must be chain, ring or full", i);
+    }
+  }
+  el_batch *b = new el_batch();
+  b->count = count; b->dtype = dtype; b->max_iter = max_iter; b->tol = tol; b->device = ctx->device;
+  b->order.resize(count);
+  std::iota(b->order.begin(), b->order.end(), 0);
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return dims[x] > dims[y]; });
+  std::vector<int> noff(count + 1, 0);
+  for (int i = 0; i < count; ++i) noff[i + 1] = noff[i] + n_sites[i];
+  std::vector<Inst> inst(count);
+  std::vector<double> Vm((size_t)count * MAXN * MAXN, 0.0), Dl((size_t)count * MAXN, 0.0);
+  int64_t off = 0;
+  int rc = EL_OK;
+  for (int p = 0; p < count && rc == EL_OK; ++p) {
+    const int i = b->order[p];
+    const int n = n_sites[i];
+    Inst &I = inst[p];
+    memset(&I, 0, sizeof I);
+    I.n = n; I.layout = layouts[i]; I.dim = dims[i]; I.off = off;
+    for (int s2 = 0; s2 < n; ++s2) {
+      const double o = omega[noff[i] + s2], dd = delta[noff[i] + s2];
+      if (!std::isfinite(o) || !std::isfinite(dd)) { rc = fail(ctx, EL_EINVAL, "instance %d: non-finite drive", i); break; }
+      I.om[n - 1 - s2] = 0.5 * o;
+      Dl[(size_t)p * MAXN + (n - 1 - s2)] = dd;
+    }
+    for (int q = pair_off[i]; q < pair_off[i + 1] && rc == EL_OK; ++q) {
+      const int a = pi[q], c = pj[q];
+      if (a < 0 || c < 0 || a >= n || c >= n || a == c || !std::isfinite(V[q])) {
+        rc = fail(ctx, EL_EINVAL, "instance %d: bad pair (%d, %d)", i, a, c);
+        break;
+      }
+      const int qa = n - 1 - a, qb = n - 1 - c;
+      Vm[(size_t)p * MAXN * MAXN + qa * MAXN + qb] += V[q];
+      Vm[(size_t)p * MAXN * MAXN + qb * MAXN + qa] += V[q];
+    }
+    off += dims[i];
+    b->dim_max = std::max(b->dim_max, dims[i]);
+  }
+  b->total_rows = off;
+  double *d_V = nullptr, *d_D = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (rc == EL_OK) do {
+    if ((e = cudaMalloc(&b->d_inst, sizeof(Inst) * count)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&b->d_diag, (size_t)off * 8)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&b->d_out, (size_t)count * 4 * 8)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&b->d_iout, (size_t)count * 2 * 4)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&b->d_queue, 64)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&d_V, Vm.size() * 8)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&d_D, Dl.size() * 8)) != cudaSuccess) break;
+    if ((e = el::copy(ctx, b->d_inst, inst.data(), sizeof(Inst) * count, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+    if ((e = el::copy(ctx, d_V, Vm.data(), Vm.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+    if ((e = el::copy(ctx, d_D, Dl.data(), Dl.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+    k_batch_diag<<<dim3(64, std::min(count, 1024)), 256, 0, ctx->stream>>>(count, b->d_inst, d_V, d_D, b->d_diag);
+    ctx->launches++;
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
+    e = cudaStreamSynchronize(ctx->stream);
+  } while (0);
+  if (d_V) cudaFree(d_V);
+  if (d_D) cudaFree(d_D);
+  if (rc == EL_OK && e != cudaSuccess) rc = el::cuda_fail(ctx, e, "el_batch_create");
+  if (rc != EL_OK) { el_batch_destroy(b); return rc; }
+  *out = b;
+  return EL_OK;
+}
+
+int el_batch_run(el_ctx *ctx, el_batch *b, int threads, int ctas_per_sm, uint64_t seed) {
+  if (!ctx || !b) return EL_EINVAL;
+  if (threads != 256 && threads != 512 && threads != 1024) return fail(ctx, EL_EINVAL, "threads must be 256, 512 or 1024");
+  if (ctas_per_sm < 1 || ctas_per_sm > 2) return fail(ctx, EL_EINVAL, "ctas_per_sm must be 1 or 2");
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const int grid = std::min(b->count, sms * ctas_per_sm);
+  const size_t es = b->dtype == EL_F32 ? 4 : 8;
+  const size_t need = (size_t)grid * (b->max_iter + 2) * b->dim_max * es;
+  if (need > b->ws_bytes) {
+    // grows only outside graph capture (a first run sizes it)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx->stream, &cs);
+    if (cs != cudaStreamCaptureStatusNone) return fail(ctx, EL_EINVAL, "run the batch once before capturing it");
+    EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (b->ws) cudaFree(b->ws);
+    b->ws = nullptr;
+    b->ws_bytes = 0;
+    cudaError_t e = cudaMalloc(&b->ws, need);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, EL_ENOMEM, "batched workspace of %zu bytes", need); }
+    b->ws_bytes = need;
+  }
+  EL_CUDA_TRY(ctx, cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned), ctx->stream));
+  BatchArgs A;
+  memset(&A, 0, sizeof A);
+  A.count = b->count; A.max_iter = b->max_iter; A.tol = b->tol; A.eps = b->dtype == EL_F32 ? 1.19e-7 : 2.22e-16;
+  A.inst = b->d_inst; A.diag = b->d_diag; A.ws = b->ws; A.dim_max = b->dim_max; A.queue = b->d_queue;
+  A.seed = seed;
+  A.e0 = b->d_out; A.e1 = b->d_out + b->count; A.res = b->d_out + 2 * b->count; A.gap = b->d_out + 3 * b->count;
+  A.iters = b->d_iout; A.conv = b->d_iout + b->count;
+#define EL_BCASE(TT, NTV) k_lanczos_batch<TT, NTV><<<grid, NTV, 0, ctx->stream>>>(A)
+  if (b->dtype == EL_F32) {
+    if (threads == 256) EL_BCASE(float, 256); else if (threads == 512) EL_BCASE(float, 512); else EL_BCASE(float, 1024);
+  } else {
+    if (threads == 256) EL_BCASE(double, 256); else if (threads == 512) EL_BCASE(double, 512); else EL_BCASE(double, 1024);
+  }
+#undef EL_BCASE
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+int el_batch_results(el_ctx *ctx, el_batch *b, double *e0, double *gap, double *residual,
+                     int32_t *iters, int32_t *converged) {
+  if (!ctx || !b || !e0 || !gap) return EL_EINVAL;
+  const int count = b->count;
+  std::vector<double> ho((size_t)count * 4);
+  std::vector<int> hi((size_t)count * 2);
+  EL_CUDA_TRY(ctx, el::copy(ctx, ho.data(), b->d_out, ho.size() * 8, cudaMemcpyDeviceToHost));
+  EL_CUDA_TRY(ctx, el::copy(ctx, hi.data(), b->d_iout, hi.size() * 4, cudaMemcpyDeviceToHost));
+  EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int p = 0; p < count; ++p) {
+    const int i = b->order[p];
+    e0[i] = ho[p];
+    gap[i] = ho[(size_t)3 * count + p];
+    if (residual) residual[i] = ho[(size_t)2 * count + p];
+    if (iters) iters[i] = hi[p];
+    if (converged) converged[i] = hi[(size_t)count + p];
+  }
+  return EL_OK;
+}
+
+int el_batch_destroy(el_batch *b) {
+  if (!b) return EL_OK;
+  cudaSetDevice(b->device);
+  if (b->d_inst) cudaFree(b->d_inst);
+  if (b->d_diag) cudaFree(b->d_diag);
+  if (b->d_out) cudaFree(b->d_out);
+  if (b->d_iout) cudaFree(b->d_iout);
+  if (b->d_queue) cudaFree(b->d_queue);
+  if (b->ws) cudaFree(b->ws);
+  delete b;
+  return EL_OK;
+}
+
+}  // extern "C"

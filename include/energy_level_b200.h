@@ -182,6 +182,35 @@ int el_lanczos_ground(el_ctx *ctx, el_ham *ham, int dtype, const void *v0,
                       double *residuals, int *iters, int *converged,
                       void *vec_out);
 
+/* ---- batched ground states ---------------------------------------------- */
+
+typedef struct el_batch el_batch;
+
+/* Describe `count` independent Hamiltonians: instance i has n_sites[i] sites
+ * (<= 40), basis layout layouts[i] (EL_LAYOUT_CHAIN or EL_LAYOUT_RING
+ * blockade sectors, or EL_LAYOUT_FULL up to 24 sites), per-site Omega and
+ * delta (host, concatenated over instances) and the I1 pairs
+ * pi/pj/V[pair_off[i] .. pair_off[i+1]).  Vectors in dtype (EL_F32/EL_F64),
+ * alpha/beta and the tridiagonal solve in FP64; at most max_iter (<= 384)
+ * Lanczos steps per instance; convergence when the residual estimates of the
+ * two lowest Ritz pairs are <= tol * max(1, |theta|).
+ * Replaces the per-instance eigsh calls of eq_route.py:540-728 and the dense
+ * batched_ground_state of equilibrium.py:251-311 for sector problems. */
+int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_t *layouts,
+                    const double *omega, const double *delta, const int32_t *pair_off,
+                    const int32_t *pi, const int32_t *pj, const double *V, int dtype,
+                    int max_iter, double tol, el_batch **out);
+/* Queue the whole batch as ONE persistent launch (CTAs pull instances from an
+ * atomic queue, largest first).  threads: 256/512/1024 per CTA; ctas_per_sm:
+ * 1 or 2.  Asynchronous and capturable in a CUDA graph once a first run has
+ * sized the workspace. */
+int el_batch_run(el_ctx *ctx, el_batch *batch, int threads, int ctas_per_sm, uint64_t seed);
+/* Copy results (caller order): ground energy, gap E1 - E0, max residual
+ * estimate, Lanczos steps, converged flag.  Synchronises the stream. */
+int el_batch_results(el_ctx *ctx, el_batch *batch, double *e0, double *gap, double *residual,
+                     int32_t *iters, int32_t *converged);
+int el_batch_destroy(el_batch *batch);
+
 /* ---- time evolution ------------------------------------------------------- */
 
 /* psi <- exp(-i 2pi 1e-3 H tau_ns) psi by a Chebyshev expansion truncated at

@@ -147,3 +147,42 @@ def test_solve_equilibrium_routes(ctx):
     t = solve_equilibrium({"calib": cfg["calib"], "Om": cfg["Om"], "delta": cfg["delta"]}, "thermal",
                           backend="b200-kpm", betas=[0.1], num=128, nvec=16)
     assert np.isfinite(t["E"]).all()
+
+
+def test_batched_ground_states_match_dense(ctx):
+    """Uneven chain/ring sectors in one persistent launch vs dense eigh."""
+    from energy_level_b200.batched import batched_ground_states
+    from oracle import ref
+    rng = np.random.default_rng(4)
+    insts, want = [], []
+    for k in range(24):
+        n = int(rng.integers(6, 13))
+        ring = (k % 3 == 0)
+        edges = configs.ring_edges(n) if ring else configs.chain_edges(n)
+        calib = configs.calib_from_positions(configs.chain_positions(n, jitter=rng.uniform(-0.3, 0.3, n)))
+        Delta = 2.0 * rng.uniform(0, 3)
+        insts.append(dict(calib=calib, Om=np.full(n, 2.0), delta=np.full(n, -Delta), edges=edges))
+        codes = ref.independent_states(n, edges, None)
+        pairs = [(p["i"], p["j"], p["V"]) for p in calib["pairs"]]
+        w = np.linalg.eigvalsh(ref.dense_h(n, codes, np.full(n, 2.0), np.full(n, -Delta), pairs))
+        want.append((w[0], w[1] - w[0]))
+    want = np.array(want)
+    r64 = batched_ground_states(insts, dtype="float64", tol=1e-10)
+    assert r64["converged"].all()
+    assert np.max(np.abs(r64["E0"] - want[:, 0])) < 1e-8
+    assert np.max(np.abs(r64["gap"] - want[:, 1])) < 1e-7
+    r32 = batched_ground_states(insts, dtype="float32", tune=True)
+    assert np.max(np.abs(r32["E0"] - want[:, 0]) / np.abs(want[:, 0])) < 1e-6
+
+
+def test_batched_graph_replay_is_deterministic(ctx):
+    from energy_level_b200.batched import BatchedGroundStates
+    insts = [c for c in configs.batch512(count=32)]
+    b = BatchedGroundStates(insts, dtype="float32")
+    b.run()
+    r1 = b.results()
+    g = b.capture()
+    g.replay()
+    r2 = b.results()
+    assert np.array_equal(r1["E0"], r2["E0"])
+    b.close()
