@@ -1,0 +1,340 @@
+// Adjoint pulse gradients through the Chebyshev propagator.
+//
+// Pulse: K piecewise-constant steps; step k lasts tau_k with
+//     H_k = sum_i [ -Delta_k b_i n_i + (Omega_k a_i / 2) sigma^x_i ] + sum V n n
+// (a_i, b_i: fixed site shapes, 1 by default; the reference's delta is
+// -Delta, channels.py:68-73).  Each step applies the truncated expansion
+//     U_k = sum_{m<=M} c_m T_m(Htil_k),  Htil_k = (H_k - b_k)/a_k
+// of el_cheb_step.  Objective: F = |<phi|psi_K>|^2 (fidelity with a target)
+// or F = <psi_K|O|psi_K> for a diagonal observable O.
+//
+// Discretise-then-differentiate: with lambda_K = dF/d(conj psi_K) / 2
+// (a phi for the fidelity, O psi_K for the observable) the gradient of the
+// computed map follows from reverse-mode differentiation of the Chebyshev
+// recurrence t_0 = psi, t_1 = Htil t_0, t_{m+1} = 2 Htil t_m - t_{m-1}:
+//     u_M = conj(c_M) lambda,  u_m = conj(c_m) lambda + s_{m+1} Htil u_{m+1} - u_{m+2}
+//     (s_1 = 1, s_m = 2 otherwise),   lambda_{k-1} = u_0,
+//     dF/dtheta_k = 2 sum_{m>=1} s_m Re <G_theta u_m, t_{m-1}> / a_k,
+// with G_Omega = sum a_i sigma^x_i / 2 and G_Delta = -sum b_i n_i.  a_k, b_k
+// are held fixed (the map depends on them only at the truncation level).
+// The forward pass keeps one state per step; the backward pass recomputes the
+// Chebyshev terms t_0..t_{M-1} of one step at a time from that checkpoint
+// (the recurrence is recomputed, never stored across steps).
+#include "el_internal.cuh"
+
+#include <algorithm>
+
+namespace {
+
+using el::fail;
+
+template <typename S>
+struct AdjArgs {
+  const S *diagV;
+  S delta[EL_MAX_SITES];   // current -Delta_k b_i per bit position
+  S ahalf[EL_MAX_SITES];   // a_i / 2 per bit position
+  S bsh[EL_MAX_SITES];     // b_i per bit position
+  S om;                    // Omega_k
+  S alpha, beta;           // y = clam lam + alpha H x + beta x - z
+  S cl_re, cl_im;
+  const S *x, *z, *lam, *t;
+  S *y;
+  double *partials;
+  unsigned int *counter;
+  double *out;             // [2]: Re<G_O x, t>, Re<G_D x, t>
+};
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_adjoint_step(BasisDev B, AdjArgs<S> P) {
+  __shared__ double red[2][256];
+  __shared__ bool last;
+  double gO = 0.0, gD = 0.0;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < B.dim;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t code = el::unrank_row(B, r);
+    const S xr = P.x[2 * r], xi = P.x[2 * r + 1];
+    S sre = 0, sim = 0, dsum = P.diagV[r], nb = 0;
+    for (int k = 0; k < B.n; ++k) {
+      if ((code >> k) & 1ULL) { dsum += P.delta[k]; nb += P.bsh[k]; }
+      const S amp = P.ahalf[k];
+      if (amp == S(0)) continue;
+      const int64_t tg = el::flip_target(B, code, r, k);
+      if (tg < 0) continue;
+      sre += amp * P.x[2 * tg];
+      sim += amp * P.x[2 * tg + 1];
+    }
+    // H x = dsum x + Omega S
+    const S hre = dsum * xr + P.om * sre, him = dsum * xi + P.om * sim;
+    S yre = P.alpha * hre + P.beta * xr, yim = P.alpha * him + P.beta * xi;
+    if (P.z) { yre -= P.z[2 * r]; yim -= P.z[2 * r + 1]; }
+    if (P.lam) {
+      const S lr = P.lam[2 * r], li = P.lam[2 * r + 1];
+      yre += P.cl_re * lr - P.cl_im * li;
+      yim += P.cl_re * li + P.cl_im * lr;
+    }
+    P.y[2 * r] = yre;
+    P.y[2 * r + 1] = yim;
+    if (P.t) {
+      const double tr = P.t[2 * r], ti = P.t[2 * r + 1];
+      gO += (double)sre * tr + (double)sim * ti;               // Re(conj(G_O x) t)
+      gD += -(double)nb * ((double)xr * tr + (double)xi * ti); // Re(conj(G_D x) t)
+    }
+  }
+  red[0][threadIdx.x] = gO;
+  red[1][threadIdx.x] = gD;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + s];
+      red[1][threadIdx.x] += red[1][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    P.partials[2 * blockIdx.x] = red[0][0];
+    P.partials[2 * blockIdx.x + 1] = red[1][0];
+    __threadfence();
+    last = (atomicAdd(P.counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double a = 0.0, b = 0.0;
+    for (unsigned i = 0; i < gridDim.x; ++i) { a += __ldcg(&P.partials[2 * i]); b += __ldcg(&P.partials[2 * i + 1]); }
+    P.out[0] = a;
+    P.out[1] = b;
+    *P.counter = 0u;
+  }
+}
+
+// lam = O psi (elementwise, O real per row)
+template <typename S>
+__global__ void k_diag_mul(int64_t dim, const double *O, const S *psi, S *lam, double *partials,
+                           unsigned int *counter, double *out) {
+  __shared__ double red[256];
+  __shared__ bool last;
+  double f = 0.0;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < dim;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const double o = O[r], a = psi[2 * r], b = psi[2 * r + 1];
+    lam[2 * r] = (S)(o * a);
+    lam[2 * r + 1] = (S)(o * b);
+    f += o * (a * a + b * b);
+  }
+  red[threadIdx.x] = f;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = red[0];
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double s = 0.0;
+    for (unsigned i = 0; i < gridDim.x; ++i) s += __ldcg(&partials[i]);
+    out[0] = s;
+    *counter = 0u;
+  }
+}
+
+template <typename S>
+int adjoint_impl(el_ctx *ctx, el_ham *h, int dtype, int K, const double *tau, const double *omega_k,
+                 const double *delta_k, const double *oshape, const double *dshape, const void *psi0,
+                 const void *target, const double *obs_diag, double tol, double *F_out,
+                 double *gO_out, double *gD_out, void *psi_final) {
+  const int n = h->n;
+  const int64_t dim = h->basis->dim;
+  const size_t vb = (size_t)dim * 2 * sizeof(S);
+  std::vector<double> ash(n, 1.0), bsh(n, 1.0);
+  for (int i = 0; i < n; ++i) {
+    if (oshape) ash[i] = oshape[i];
+    if (dshape) bsh[i] = dshape[i];
+  }
+  auto set_drive = [&](int k) {
+    std::vector<double> ore(n), oim(n, 0.0), de(n);
+    for (int i = 0; i < n; ++i) { ore[i] = omega_k[k] * ash[i]; de[i] = -delta_k[k] * bsh[i]; }
+    return el_ham_set_drive(ctx, h, ore.data(), oim.data(), de.data());
+  };
+  // plans of all steps (bounds and coefficients)
+  std::vector<el::ChebPlan> plans(K);
+  int Mmax = 1;
+  for (int k = 0; k < K; ++k) {
+    int rc = set_drive(k);
+    if (rc) return rc;
+    rc = el::cheb_plan(ctx, h, tau[k], tol, &plans[k]);
+    if (rc) return rc;
+    Mmax = std::max(Mmax, plans[k].M);
+  }
+  // workspace: K+1 checkpoints, Mmax+1 terms, 3 adjoint vectors, lambda
+  char *buf = (char *)el::workspace(ctx, 11, (size_t)(K + 1 + Mmax + 1 + 4) * vb);
+  if (!buf) return EL_ENOMEM;
+  auto ckp = [&](int k) { return (void *)(buf + (size_t)k * vb); };
+  char *tb = buf + (size_t)(K + 1) * vb;
+  auto term = [&](int m) { return (void *)(tb + (size_t)m * vb); };
+  char *ub = tb + (size_t)(Mmax + 1) * vb;
+  void *U[3] = {ub, ub + vb, ub + 2 * vb};
+  void *lam = ub + 3 * vb;
+  double *d_g = (double *)el::workspace(ctx, 12, (size_t)K * (Mmax + 1) * 2 * sizeof(double) + 64);
+  if (!d_g) return EL_ENOMEM;
+  EL_CUDA_TRY(ctx, cudaMemsetAsync(d_g, 0, (size_t)K * (Mmax + 1) * 2 * sizeof(double), ctx->stream));
+  EL_CUDA_TRY(ctx, el::copy(ctx, ckp(0), psi0, vb, cudaMemcpyDeviceToDevice));
+  int rc;
+  // ---- forward: psi_k = U_k psi_{k-1}
+  for (int k = 0; k < K; ++k) {
+    if (el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
+    rc = set_drive(k);
+    if (rc) return rc;
+    const el::ChebPlan &pl = plans[k];
+    void *out = ckp(k + 1);
+    rc = el::launch_axpby(ctx, dtype, dim, pl.c_re[0], pl.c_im[0], ckp(k), 0, 0, out, nullptr);
+    if (rc) return rc;
+    ApplyArgs A;
+    memset(&A, 0, sizeof A);
+    A.dtype = dtype; A.nvec = 1; A.x = ckp(k); A.y = term(1); A.acc = out;
+    A.a = 1.0 / pl.a; A.b = -pl.b / pl.a; A.w_re = pl.c_re[1]; A.w_im = pl.c_im[1];
+    rc = el::launch_apply(ctx, h, A);
+    if (rc) return rc;
+    void *xm1 = ckp(k), *xc = term(1);
+    for (int m = 2; m <= pl.M; ++m) {
+      void *y = term(m);
+      memset(&A, 0, sizeof A);
+      A.dtype = dtype; A.nvec = 1; A.x = xc; A.z = xm1; A.y = y; A.acc = out;
+      A.a = 2.0 / pl.a; A.b = -2.0 * pl.b / pl.a; A.c = -1.0; A.w_re = pl.c_re[m]; A.w_im = pl.c_im[m];
+      rc = el::launch_apply(ctx, h, A);
+      if (rc) return rc;
+      xm1 = xc;
+      xc = y;
+    }
+  }
+  // ---- objective and lambda_K
+  double F = 0.0;
+  const int grid = el::grid_for(dim, 256);
+  rc = el::ensure_partials(ctx, (size_t)std::max(grid, 2) * 2);
+  if (rc) return rc;
+  if (target) {
+    rc = el::launch_gemv_t(ctx, dtype, dim, 1, target, dim, ckp(K), ctx->d_scalars);
+    if (rc) return rc;
+    double ov[2];
+    EL_CUDA_TRY(ctx, el::copy(ctx, ov, ctx->d_scalars, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+    EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    F = ov[0] * ov[0] + ov[1] * ov[1];
+    rc = el::launch_axpby(ctx, dtype, dim, ov[0], ov[1], target, 0, 0, lam, nullptr);
+    if (rc) return rc;
+  } else {
+    k_diag_mul<S><<<grid, 256, 0, ctx->stream>>>(dim, obs_diag, (const S *)ckp(K), (S *)lam,
+                                                  ctx->d_partials, ctx->d_counter, ctx->d_scalars);
+    EL_LAUNCH_CHECK(ctx);
+    double f;
+    EL_CUDA_TRY(ctx, el::copy(ctx, &f, ctx->d_scalars, sizeof(double), cudaMemcpyDeviceToHost));
+    EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    F = f;
+  }
+  // ---- backward
+  const BasisDev B = el::basis_dev(h->basis);
+  if (std::is_same<S, float>::value) { rc = el::ham_diag32(ctx, h); if (rc) return rc; }
+  const S *diagV = std::is_same<S, float>::value ? (const S *)(void *)h->d_diagV32
+                                                 : (const S *)(void *)h->d_diagV64;
+  for (int k = K - 1; k >= 0; --k) {
+    if (el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
+    rc = set_drive(k);
+    if (rc) return rc;
+    const el::ChebPlan &pl = plans[k];
+    const int M = pl.M;
+    // recompute t_0 .. t_{M-1} of this step from its checkpoint
+    EL_CUDA_TRY(ctx, el::copy(ctx, term(0), ckp(k), vb, cudaMemcpyDeviceToDevice));
+    ApplyArgs A;
+    if (M >= 2) {
+      memset(&A, 0, sizeof A);
+      A.dtype = dtype; A.nvec = 1; A.x = term(0); A.y = term(1); A.a = 1.0 / pl.a; A.b = -pl.b / pl.a;
+      rc = el::launch_apply(ctx, h, A);
+      if (rc) return rc;
+      for (int m = 2; m <= M - 1; ++m) {
+        memset(&A, 0, sizeof A);
+        A.dtype = dtype; A.nvec = 1; A.x = term(m - 1); A.z = term(m - 2); A.y = term(m);
+        A.a = 2.0 / pl.a; A.b = -2.0 * pl.b / pl.a; A.c = -1.0;
+        rc = el::launch_apply(ctx, h, A);
+        if (rc) return rc;
+      }
+    }
+    // reverse recurrence.  u_M = conj(c_M) lam
+    void *uM = U[M % 3];
+    rc = el::launch_axpby(ctx, dtype, dim, pl.c_re[M], -pl.c_im[M], lam, 0, 0, uM, nullptr);
+    if (rc) return rc;
+    AdjArgs<S> P;
+    memset(&P, 0, sizeof P);
+    P.diagV = diagV;
+    for (int q = 0; q < n; ++q) {
+      P.delta[q] = (S)h->delta[q];
+      P.ahalf[q] = (S)(0.5 * ash[n - 1 - q]);
+      P.bsh[q] = (S)bsh[n - 1 - q];
+    }
+    P.om = (S)omega_k[k];
+    P.partials = ctx->d_partials;
+    P.counter = ctx->d_counter;
+    for (int m = M - 1; m >= 0; --m) {
+      // u_m = conj(c_m) lam + s_{m+1} Htil u_{m+1} - u_{m+2}; dots pair u_{m+1} with t_m
+      const double s = (m == 0) ? 1.0 : 2.0;
+      P.alpha = (S)(s / pl.a);
+      P.beta = (S)(-s * pl.b / pl.a);
+      P.cl_re = (S)pl.c_re[m];
+      P.cl_im = (S)(-pl.c_im[m]);
+      P.x = (const S *)U[(m + 1) % 3];
+      P.z = (m + 2 <= M) ? (const S *)U[(m + 2) % 3] : nullptr;
+      P.lam = (const S *)lam;
+      P.t = (const S *)term(m);
+      P.y = (S *)U[m % 3];
+      P.out = d_g + ((size_t)k * (Mmax + 1) + (m + 1)) * 2;
+      k_adjoint_step<S><<<grid, 256, 0, ctx->stream>>>(B, P);
+      EL_LAUNCH_CHECK(ctx);
+    }
+    // lambda_{k-1} = u_0
+    EL_CUDA_TRY(ctx, el::copy(ctx, lam, U[0], vb, cudaMemcpyDeviceToDevice));
+  }
+  std::vector<double> hg((size_t)K * (Mmax + 1) * 2);
+  EL_CUDA_TRY(ctx, el::copy(ctx, hg.data(), d_g, hg.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  if (psi_final) EL_CUDA_TRY(ctx, el::copy(ctx, psi_final, ckp(K), vb, cudaMemcpyDeviceToDevice));
+  EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < K; ++k) {
+    const el::ChebPlan &pl = plans[k];
+    double go = 0.0, gd = 0.0;
+    for (int m = 1; m <= pl.M; ++m) {
+      const double s = (m == 1) ? 1.0 : 2.0;
+      go += s * hg[((size_t)k * (Mmax + 1) + m) * 2];
+      gd += s * hg[((size_t)k * (Mmax + 1) + m) * 2 + 1];
+    }
+    gO_out[k] = 2.0 * go / pl.a;
+    gD_out[k] = 2.0 * gd / pl.a;
+  }
+  *F_out = F;
+  return EL_OK;
+}
+
+}  // namespace
+
+extern "C" int el_adjoint_pulse(el_ctx *ctx, el_ham *h, int dtype, int K, const double *tau,
+                                const double *omega_k, const double *delta_k,
+                                const double *omega_shape, const double *delta_shape,
+                                const void *psi0, const void *target, const double *obs_diag,
+                                double tol, double *F, double *grad_omega, double *grad_delta,
+                                void *psi_final) {
+  if (!ctx || !h || !tau || !omega_k || !delta_k || !psi0 || !F || !grad_omega || !grad_delta)
+    return EL_EINVAL;
+  if (dtype != EL_C64 && dtype != EL_C128) return fail(ctx, EL_EINVAL, "adjoint needs EL_C64 or EL_C128");
+  if (K < 1) return fail(ctx, EL_EINVAL, "K must be >= 1");
+  if (!target && !obs_diag) return fail(ctx, EL_EINVAL, "give a target state or a diagonal observable");
+  if (!(tol > 0) || tol >= 1) return fail(ctx, EL_EINVAL, "tol must be in (0, 1)");
+  for (int k = 0; k < K; ++k)
+    if (!std::isfinite(tau[k]) || tau[k] < 0 || !std::isfinite(omega_k[k]) || !std::isfinite(delta_k[k]))
+      return fail(ctx, EL_EINVAL, "step %d: tau/Omega/Delta must be finite, tau >= 0", k);
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (dtype == EL_C64)
+    return adjoint_impl<float>(ctx, h, dtype, K, tau, omega_k, delta_k, omega_shape, delta_shape, psi0,
+                               target, obs_diag, tol, F, grad_omega, grad_delta, psi_final);
+  return adjoint_impl<double>(ctx, h, dtype, K, tau, omega_k, delta_k, omega_shape, delta_shape, psi0,
+                              target, obs_diag, tol, F, grad_omega, grad_delta, psi_final);
+}

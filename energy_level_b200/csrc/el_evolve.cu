@@ -47,6 +47,44 @@ void bessel_j(double x, int mmax, std::vector<double> &J) {
 
 }  // namespace
 
+namespace el {
+
+int cheb_plan(el_ctx *ctx, el_ham *h, double tau_ns, double tol, ChebPlan *plan) {
+  double lo, hi;
+  int rc = gershgorin(ctx, h, &lo, &hi);
+  if (rc) return rc;
+  plan->b = 0.5 * (hi + lo);
+  plan->a = std::max(0.5 * (hi - lo) * (1.0 + 1e-6), 1e-12);
+  const double x = plan->a * CONV * tau_ns;
+  const double phi = plan->b * CONV * tau_ns;
+  int mmax = (int)(x + 30.0 + 6.0 * std::cbrt(x + 1.0));
+  std::vector<double> J;
+  bessel_j(x, mmax, J);
+  int M = 1;
+  for (int m = mmax; m >= 1; --m)
+    if (std::fabs(J[m]) * 2.0 > tol * 0.25) { M = m + 1; break; }
+  M = std::min(M, mmax);
+  plan->M = M;
+  plan->c_re.assign(M + 1, 0.0);
+  plan->c_im.assign(M + 1, 0.0);
+  const double cph = std::cos(phi), sph = -std::sin(phi);
+  for (int m = 0; m <= M; ++m) {
+    const double mag = (m == 0 ? 1.0 : 2.0) * J[m];
+    double pr, pi;
+    switch (m & 3) {  // (-i)^m
+      case 0: pr = 1; pi = 0; break;
+      case 1: pr = 0; pi = -1; break;
+      case 2: pr = -1; pi = 0; break;
+      default: pr = 0; pi = 1; break;
+    }
+    plan->c_re[m] = mag * (pr * cph - pi * sph);
+    plan->c_im[m] = mag * (pr * sph + pi * cph);
+  }
+  return EL_OK;
+}
+
+}  // namespace el
+
 extern "C" int el_cheb_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
                             double tau_ns, double tol, int *n_terms) {
   if (!ctx || !h || !psi) return EL_EINVAL;
@@ -59,35 +97,12 @@ extern "C" int el_cheb_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   const int64_t dim = h->basis->dim;
   const size_t vb = (size_t)dim * el::dtype_size(dtype);
-  double lo, hi;
-  int rc = el::gershgorin(ctx, h, &lo, &hi);
+  el::ChebPlan plan;
+  int rc = el::cheb_plan(ctx, h, tau_ns, tol, &plan);
   if (rc) return rc;
-  const double b = 0.5 * (hi + lo);
-  const double a = std::max(0.5 * (hi - lo) * (1.0 + 1e-6), 1e-12);
-  const double x = a * CONV * tau_ns;
-  const double phi = b * CONV * tau_ns;
-  // number of terms: J_m(x) decays super-exponentially once m > x
-  int mmax = (int)(x + 30.0 + 6.0 * std::cbrt(x + 1.0));
-  std::vector<double> J;
-  bessel_j(x, mmax, J);
-  int M = 1;
-  for (int m = mmax; m >= 1; --m)
-    if (std::fabs(J[m]) * 2.0 > tol * 0.25) { M = m + 1; break; }
-  M = std::min(M, mmax);
-  // c_m = (2 - delta_m0) (-i)^m J_m(x) exp(-i phi)
-  const double cph = std::cos(phi), sph = -std::sin(phi);
-  auto coef = [&](int m, double *re, double *im) {
-    const double mag = (m == 0 ? 1.0 : 2.0) * J[m];
-    double pr, pi;
-    switch (m & 3) {  // (-i)^m
-      case 0: pr = 1; pi = 0; break;
-      case 1: pr = 0; pi = -1; break;
-      case 2: pr = -1; pi = 0; break;
-      default: pr = 0; pi = 1; break;
-    }
-    *re = mag * (pr * cph - pi * sph);
-    *im = mag * (pr * sph + pi * cph);
-  };
+  const double a = plan.a, b = plan.b;
+  const int M = plan.M;
+  auto coef = [&](int m, double *re, double *im) { *re = plan.c_re[m]; *im = plan.c_im[m]; };
   char *buf = (char *)el::workspace(ctx, 5, 4 * vb);
   if (!buf) return EL_ENOMEM;
   void *t0 = buf, *t1 = buf + vb, *t2 = buf + 2 * vb, *acc = buf + 3 * vb;

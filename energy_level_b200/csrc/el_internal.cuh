@@ -317,6 +317,14 @@ int launch_scale(el_ctx *ctx, int dtype, int64_t len, const double *scale_dev,
                  int invert_sqrt, void *x);
 int launch_observables(el_ctx *ctx, el_ham *h, int dtype, const void *psi,
                        double *out_dev);
+// Chebyshev propagator plan for exp(-i CONV H tau) (el_evolve.cu):
+// H = a Htil + b from the Gershgorin interval, coefficients c_0..c_M.
+struct ChebPlan {
+  double a = 1, b = 0;
+  int M = 1;
+  std::vector<double> c_re, c_im;
+};
+int cheb_plan(el_ctx *ctx, el_ham *h, double tau_ns, double tol, ChebPlan *plan);
 // TMA-fed tiled full-basis KPM recurrence (el_kpm_tma.cu), 20 <= N <= 25
 bool kpm_tma_eligible(const el_ham *h, int dtype, int chunk);
 int kpm_tma(el_ctx *ctx, el_ham *h, int dtype, int num, int nvec, int chunk, uint64_t seed,

@@ -218,6 +218,22 @@ int el_batch_destroy(el_batch *batch);
  * Replaces the expm_multiply step of engine_ed.py:125 and engine_ed.py:145. */
 int el_cheb_step(el_ctx *ctx, el_ham *ham, int dtype, void *psi,
                  double tau_ns, double tol, int *n_terms);
+/* Pulse gradient by the adjoint of the Chebyshev propagator.  K steps; step k
+ * lasts tau[k] ns with Omega_i = omega_k[k] * omega_shape[i] and
+ * delta_i = -delta_k[k] * delta_shape[i] (shapes NULL = 1), V from `ham`.
+ * Objective F = |<target|psi_K>|^2 (target: device state) or, with target
+ * NULL, F = sum_r obs_diag[r] |psi_K[r]|^2 (obs_diag: device FP64 [dim]).
+ * Returns F and dF/domega_k, dF/ddelta_k (host [K]) of the discretised map
+ * (discretise-then-differentiate: reverse recurrence through each
+ * Chebyshev expansion, terms recomputed per step from one checkpoint per
+ * step).  psi_final (device, may be NULL) receives psi_K.  The reference has
+ * no gradient code; it replaces central finite differences of
+ * engine_ed.py:130-147 evolutions. */
+int el_adjoint_pulse(el_ctx *ctx, el_ham *ham, int dtype, int K, const double *tau,
+                     const double *omega_k, const double *delta_k, const double *omega_shape,
+                     const double *delta_shape, const void *psi0, const void *target,
+                     const double *obs_diag, double tol, double *F, double *grad_omega,
+                     double *grad_delta, void *psi_final);
 /* Site occupations <n_i> (host double[n]) and squared norm of psi.  Replaces
  * the bits @ |psi|^2 reduction of engine_ed.py:259-263 (_reduce). */
 int el_observables(el_ctx *ctx, el_ham *ham, int dtype, const void *psi,

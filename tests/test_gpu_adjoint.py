@@ -1,0 +1,96 @@
+"""Adjoint pulse gradients vs central finite differences (h = 1e-4) and vs
+FP64 torch autograd through dense matrix exponentials (N <= 10)."""
+import numpy as np
+import pytest
+
+from energy_level_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(n, ring, dtype, target=True):
+    from energy_level_b200.adjoint import PulseProblem
+    calib = configs.calib_from_positions(configs.ring_positions(n) if ring else configs.chain_positions(n))
+    edges = configs.ring_edges(n) if ring else configs.chain_edges(n)
+    plan = {"projected": True, "blockade_edges": edges, "constraint": {"kind": "blockade"}}
+    tgt = "rg" * (n // 2) + ("r" if n % 2 else "")
+    if target:
+        return PulseProblem(calib, "g" * n, target=tgt, plan=plan, dtype=dtype), calib, edges
+    from oracle import ref
+    codes = ref.independent_states(n, edges, None)
+    obs = ref.basis_bits(n, codes).sum(axis=0).astype(float)     # total Rydberg number
+    return PulseProblem(calib, "g" * n, observable=obs, plan=plan, dtype=dtype), calib, edges
+
+
+def _pulse(K, seed):
+    rng = np.random.default_rng(seed)
+    tau = np.full(K, 40.0)
+    om = 2.0 + 0.3 * rng.standard_normal(K)
+    de = np.linspace(-4, 4, K) + 0.2 * rng.standard_normal(K)
+    return tau, om, de
+
+
+@pytest.mark.parametrize("ring,target", [(True, True), (False, True), (False, False)])
+def test_adjoint_matches_finite_differences(ctx, ring, target):
+    prob, _, _ = _problem(8, ring, "complex128", target)
+    tau, om, de = _pulse(6, 1)
+    F, go, gd = prob.evaluate(tau, om, de)
+    h = 1e-4
+    for k in range(6):
+        e = np.zeros(6); e[k] = h
+        fo = (prob.evaluate(tau, om + e, de)[0] - prob.evaluate(tau, om - e, de)[0]) / (2 * h)
+        fd = (prob.evaluate(tau, om, de + e)[0] - prob.evaluate(tau, om, de - e)[0]) / (2 * h)
+        assert abs(go[k] - fo) < 1e-6 * max(1.0, abs(fo)) + 1e-8
+        assert abs(gd[k] - fd) < 1e-6 * max(1.0, abs(fd)) + 1e-8
+
+
+def test_adjoint_matches_dense_autograd(ctx):
+    """FP64 torch autograd through matrix_exp of the dense projected H (N = 10)."""
+    import torch
+    from oracle import ref
+    n = 10
+    prob, calib, edges = _problem(n, True, "complex128")
+    tau, om, de = _pulse(5, 2)
+    F, go, gd = prob.evaluate(tau, om, de)
+    codes = ref.independent_states(n, edges, None)
+    pairs = [(p["i"], p["j"], p["V"]) for p in calib["pairs"]]
+    Hx = torch.tensor(ref.dense_h(n, codes, np.ones(n), np.zeros(n), []), dtype=torch.complex128)   # sum sigma^x / 2 ... (Omega=1)
+    Nd = torch.tensor(np.diag(ref.basis_bits(n, codes).sum(axis=0)).astype(float), dtype=torch.complex128)
+    Hv = torch.tensor(ref.dense_h(n, codes, np.zeros(n), np.zeros(n), pairs), dtype=torch.complex128)
+    omt = torch.tensor(om, dtype=torch.float64, requires_grad=True)
+    det = torch.tensor(de, dtype=torch.float64, requires_grad=True)
+    psi = torch.zeros(len(codes), dtype=torch.complex128); psi[0] = 1
+    for k in range(5):
+        H = Hv + omt[k] * Hx - det[k] * Nd
+        psi = torch.linalg.matrix_exp(-1j * ref.CONV * tau[k] * H) @ psi
+    tgt = torch.tensor(prob.target.cpu().numpy(), dtype=torch.complex128)
+    Ft = torch.abs(torch.vdot(tgt, psi)) ** 2
+    Ft.backward()
+    assert abs(F - Ft.item()) < 1e-10
+    assert np.max(np.abs(go - omt.grad.numpy())) < 1e-8
+    assert np.max(np.abs(gd - det.grad.numpy())) < 1e-8
+
+
+def test_complex64_gradient_close_to_fp64(ctx):
+    p64, _, _ = _problem(12, True, "complex128")
+    p32, _, _ = _problem(12, True, "complex64")
+    tau, om, de = _pulse(10, 3)
+    F64, g64, d64 = p64.evaluate(tau, om, de)
+    F32, g32, d32 = p32.evaluate(tau, om, de)
+    assert abs(F32 - F64) < 1e-5
+    scale = max(np.abs(g64).max(), np.abs(d64).max())
+    assert np.max(np.abs(g32 - g64)) < 1e-4 * scale and np.max(np.abs(d32 - d64)) < 1e-4 * scale
+
+
+def test_autograd_function(ctx):
+    import torch
+    from energy_level_b200.adjoint import pulse_fidelity
+    prob, _, _ = _problem(8, True, "complex128")
+    tau, om, de = _pulse(4, 4)
+    omt = torch.tensor(om, requires_grad=True, dtype=torch.float64)
+    det = torch.tensor(de, requires_grad=True, dtype=torch.float64)
+    F = pulse_fidelity(omt, det, prob, tau)
+    (3.0 * F).backward()
+    F2, go, gd = prob.evaluate(tau, om, de)
+    assert abs(F.item() - F2) < 1e-14
+    assert np.allclose(omt.grad.numpy(), 3.0 * go) and np.allclose(det.grad.numpy(), 3.0 * gd)
