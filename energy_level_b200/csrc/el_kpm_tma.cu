@@ -37,8 +37,6 @@ __device__ __forceinline__ float2 z8(float2) { return make_float2(0.f, 0.f); }
 __device__ __forceinline__ double z8(double) { return 0.0; }
 __device__ __forceinline__ float2 fma8(float s, float2 x, float2 y) { return make_float2(fmaf(s, x.x, y.x), fmaf(s, x.y, y.y)); }
 __device__ __forceinline__ double fma8(double s, double x, double y) { return fma(s, x, y); }
-__device__ __forceinline__ float2 add8(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double add8(double a, double b) { return a + b; }
 __device__ __forceinline__ float2 sub8(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double sub8(double a, double b) { return a - b; }
 __device__ __forceinline__ float2 scl8(float s, float2 x) { return make_float2(s * x.x, s * x.y); }
@@ -223,16 +221,20 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
     }
     U *S = cur ? Sb1 : Sb0;
     U *Sn = cur ? Sb0 : Sb1;
+    // S2 is refilled only after (1) the previous item's S2 store has read it
+    // (in a step pass that store is the older of the item's two groups and
+    // the S store may still be reading Sn; in the prologue it is the only
+    // group) and (2) every thread has finished the previous item, whose last
+    // pass reads S2 after its final barrier.
     if (tid == 0) {
-      // the previous item's S2 store (the older of its two groups) has read
-      // its source; the S store may still be reading Sn
-      bulk_wait_read<1>();
-      if (A.mode != MODE_PROLOGUE) {
-        mbar_expect(&bar[2], TILE_BYTES);
-        tile_load<KIND>(A, S2, &mapP, tile, g, &bar[2]);
-      }
+      if (A.mode == MODE_PROLOGUE) bulk_wait_read<0>();
+      else bulk_wait_read<1>();
     }
-    __syncthreads();   // nobody writes S2 before that store is done
+    __syncthreads();
+    if (tid == 0 && A.mode != MODE_PROLOGUE) {
+      mbar_expect(&bar[2], TILE_BYTES);
+      tile_load<KIND>(A, S2, &mapP, tile, g, &bar[2]);
+    }
     if (cur) { mbar_wait(&bar[1], par[1], A.err); par[1] ^= 1u; }
     else { mbar_wait(&bar[0], par[0], A.err); par[0] ^= 1u; }
 
