@@ -122,3 +122,19 @@ def observables(ham: Hamiltonian, psi):
     ham.ctx.call('el_observables', ham.handle, C.c_int(dt), C.c_void_p(psi.contiguous().data_ptr()),
                  _lib.dptr(ns), C.byref(nrm))
     return ns, float(nrm.value)
+
+
+def observables_noalloc(ham: Hamiltonian, psi):
+    """observables() through el_observables_noalloc: no device allocation,
+    static scratch shared per device (at most 40 sites; calls on one device
+    must not overlap in time)."""
+    torch = _torch()
+    dt = {torch.float32: _lib.EL_F32, torch.float64: _lib.EL_F64,
+          torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}[psi.dtype]
+    if not psi.is_contiguous():
+        raise ValueError('psi must be contiguous (no copy is made)')
+    ns = np.zeros(ham.n)
+    nrm = C.c_double()
+    ham.ctx.call('el_observables_noalloc', ham.handle, C.c_int(dt), C.c_void_p(psi.data_ptr()),
+                 _lib.dptr(ns), C.byref(nrm))
+    return ns, float(nrm.value)

@@ -238,6 +238,29 @@ int el_adjoint_pulse(el_ctx *ctx, el_ham *ham, int dtype, int K, const double *t
  * the bits @ |psi|^2 reduction of engine_ed.py:259-263 (_reduce). */
 int el_observables(el_ctx *ctx, el_ham *ham, int dtype, const void *psi,
                    double *n_site_host, double *norm_host);
+/* el_observables without any allocation.  This entry point has no
+ * counterpart in the reference; it exists for callers that must not allocate
+ * device memory once they are running, e.g. an evolution driver measuring
+ * <n_i> between propagation steps in a process whose own pool already holds
+ * the free HBM (a cudaMalloc would fail there, and cudaMalloc / cudaFree can
+ * stall the device).  el_observables may grow the context's reduction buffer
+ * on first use for a larger basis; this call never allocates: its reduction
+ * scratch is one static device array of fixed size (195,200 bytes per
+ * device), and the results pass through the context's pinned result area.
+ *  - Limit: at most 40 sites; larger systems return EL_EINVAL (message in
+ *    el_last_error) and are served by el_observables.
+ *  - The scratch's completion counter must be zero when a call starts: it is
+ *    zero when the library loads and every call leaves it zero.  Nothing else
+ *    in the scratch needs an initial value.
+ *  - All callers on one device share the scratch: calls on the same device
+ *    must not overlap in time (other host threads, other streams or other
+ *    contexts); overlapping calls race and return wrong values.
+ *  - The first call on each device looks up the scratch's device address
+ *    (cudaGetSymbolAddress); make it before any stream capture starts on that
+ *    device.
+ * Same arguments, results and dtypes as el_observables. */
+int el_observables_noalloc(el_ctx *ctx, el_ham *ham, int dtype, const void *psi,
+                           double *n_site_host, double *norm_host);
 
 #ifdef __cplusplus
 }
