@@ -9,14 +9,18 @@
 // reading two vectors and writing two per Chebyshev step.
 //
 // Here every byte of tile traffic moves by TMA, not through the LSU pipe:
-//   - vectors are [pair group][row] arrays of 8-byte cells (two FP32 probes
-//     or one FP64 probe), so an A tile (2^a consecutive rows) is one 64 KB box
-//     and a B tile (row bit 0 plus row bits a..N-1) is 2^(N-a) row pairs of
-//     16 bytes, 2^a rows apart, fetched as boxes of 256 pairs;
+//   - vectors are [probe][row] arrays (one probe per cell), so an A tile
+//     (2^a consecutive rows) is one 64 KB box;
+//   - a B tile holds the C lowest row bits as a contiguous piece of 32 bytes
+//     (C = 3 for FP32: one DRAM sector) or 16 bytes (C = 1 for FP64), carried
+//     but not flipped, plus row bits a..N-1; its 2^(N-a) pieces lie 2^a rows
+//     apart and are fetched as boxes of 256 pieces.  The tile index
+//     enumerates row bits C..a-1.  a = 14 (FP32) / 13 (FP64) at N = 25 keeps
+//     both tiles at 64 KB;
 //   - the t_{m-1} tile of the next work item is prefetched into a second
 //     buffer while the current one is processed;
 //   - t_m and p_{m+1} are written into shared memory and stored by TMA.
-// Shared memory per CTA: three 2^13-cell buffers (S_cur, S_next, S2) = 192 KB.
+// Shared memory per CTA: three 64 KB buffers (S_cur, S_next, S2) = 192 KB.
 // Waits on the TMA transaction barriers are bounded; on timeout the kernel
 // records an error flag (read by the host) and finishes without hanging.
 #include "el_internal.cuh"
@@ -29,19 +33,25 @@ namespace {
 
 using el::fail;
 
-template <typename T> struct Cell8;
-template <> struct Cell8<float> { typedef float2 U; static constexpr int PU = 2; };
-template <> struct Cell8<double> { typedef double U; static constexpr int PU = 1; };
+// One probe per cell.  CARRY: low row bits a B tile keeps as one contiguous
+// piece; LOGCH: log2 of the cells in a 256-byte A-map chunk.
+template <typename T> struct Cell {
+  typedef T U;
+  static constexpr int PU = 1;
+  static constexpr int CARRY = sizeof(T) == 4 ? 3 : 1;
+  static constexpr int LOGCH = sizeof(T) == 4 ? 6 : 5;
+  static constexpr int PIECE = (1 << CARRY) * (int)sizeof(T);   // bytes
+};
 
-__device__ __forceinline__ float2 z8(float2) { return make_float2(0.f, 0.f); }
+__device__ __forceinline__ float z8(float) { return 0.f; }
 __device__ __forceinline__ double z8(double) { return 0.0; }
-__device__ __forceinline__ float2 fma8(float s, float2 x, float2 y) { return make_float2(fmaf(s, x.x, y.x), fmaf(s, x.y, y.y)); }
+__device__ __forceinline__ float fma8(float s, float x, float y) { return fmaf(s, x, y); }
 __device__ __forceinline__ double fma8(double s, double x, double y) { return fma(s, x, y); }
-__device__ __forceinline__ float2 sub8(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float sub8(float a, float b) { return a - b; }
 __device__ __forceinline__ double sub8(double a, double b) { return a - b; }
-__device__ __forceinline__ float2 scl8(float s, float2 x) { return make_float2(s * x.x, s * x.y); }
+__device__ __forceinline__ float scl8(float s, float x) { return s * x; }
 __device__ __forceinline__ double scl8(double s, double x) { return s * x; }
-__device__ __forceinline__ float get8(float2 v, int i) { return i ? v.y : v.x; }
+__device__ __forceinline__ float get8(float v, int) { return v; }
 __device__ __forceinline__ double get8(double v, int) { return v; }
 
 
@@ -110,43 +120,42 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Tile <-> tensor-map coordinates.  A: 3-D map {256-byte chunk, chunk index,
-// group}; B: 4-D map {16-byte row pair, tile, h, group}.
+// probe}; B: 4-D map {low-bit piece, tile, h, probe}.
 template <int KIND, typename T>
 __device__ __forceinline__ void tile_load(const TmaArgs<T> &A, void *dst, const CUtensorMap *m,
                                           uint32_t tile, int g, uint64_t *bar) {
   if (KIND == KIND_A) {
-    tma_load3(dst, m, 0, (int)(tile << (A.a - 5)), g, bar);
+    tma_load3(dst, m, 0, (int)(tile << (A.a - Cell<T>::LOGCH)), g, bar);
   } else {
     for (int k = 0; k < A.nbox; ++k)
-      tma_load4((char *)dst + (size_t)k * A.hb * 16, m, 0, (int)tile, k * A.hb, g, bar);
+      tma_load4((char *)dst + (size_t)k * A.hb * Cell<T>::PIECE, m, 0, (int)tile, k * A.hb, g, bar);
   }
 }
 template <int KIND, typename T>
 __device__ __forceinline__ void tile_store(const TmaArgs<T> &A, const CUtensorMap *m, uint32_t tile,
                                            int g, const void *src) {
   if (KIND == KIND_A) {
-    tma_store3(m, 0, (int)(tile << (A.a - 5)), g, src);
+    tma_store3(m, 0, (int)(tile << (A.a - Cell<T>::LOGCH)), g, src);
   } else {
     for (int k = 0; k < A.nbox; ++k)
-      tma_store4(m, 0, (int)tile, k * A.hb, g, (const char *)src + (size_t)k * A.hb * 16);
+      tma_store4(m, 0, (int)tile, k * A.hb, g, (const char *)src + (size_t)k * A.hb * Cell<T>::PIECE);
   }
 }
 
-template <int KIND>
+template <int KIND, int C>
 __device__ __forceinline__ uint32_t row_of(int a, uint32_t tile, int l) {
   if (KIND == KIND_A) return (tile << a) + (uint32_t)l;
-  return (uint32_t)(l & 1) + ((uint32_t)(l >> 1) << a) + (tile << 1);
+  return (uint32_t)(l & ((1 << C) - 1)) + ((uint32_t)(l >> C) << a) + (tile << C);
 }
 
 // h[j] += sum_{k in [K0, KMAX)} amp_k * S[(tid ^ 2^k) + NT*j] for the R cells
 // of this thread.  Bit-outer order: one address per bit, R independent FMA
 // chains per bit.
 template <typename T, int R, int K0, int KMAX>
-__device__ __forceinline__ void gather_all(const typename Cell8<T>::U *S, int tid,
-                                           const TmaArgs<T> &A, typename Cell8<T>::U (&h)[R]) {
+__device__ __forceinline__ void gather_all(const T *S, int tid, const TmaArgs<T> &A, T (&h)[R]) {
 #pragma unroll
   for (int k = K0; k < KMAX; ++k) {
-    const typename Cell8<T>::U *base = S + (tid ^ (1 << k));
+    const T *base = S + (tid ^ (1 << k));
     const T a = A.amp[k];
 #pragma unroll
     for (int j = 0; j < R; ++j) h[j] = fma8(a, base[NT * j], h[j]);
@@ -157,13 +166,15 @@ template <typename T, int TB, int KIND>
 __global__ void __launch_bounds__(NT, 1)
 k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
           const __grid_constant__ CUtensorMap mapQ) {
-  typedef typename Cell8<T>::U U;
-  constexpr int PU = Cell8<T>::PU;
+  typedef typename Cell<T>::U U;
+  constexpr int PU = Cell<T>::PU;
+  constexpr int C = Cell<T>::CARRY;
   constexpr int R = (1 << TB) / NT;          // cells per thread (TB >= 10)
   constexpr int LOGNT = 10;
   constexpr int NWARP = NT / 32;
-  constexpr int K0 = (KIND == KIND_B) ? 1 : 0;
-  constexpr unsigned TILE_BYTES = (1u << TB) * 8u;
+  constexpr int K0 = (KIND == KIND_B) ? C : 0;
+  constexpr unsigned TILE_BYTES = (1u << TB) * (unsigned)sizeof(T);
+  static_assert(TILE_BYTES <= 65536, "three tile buffers must fit in shared memory");
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   U *const Sb0 = reinterpret_cast<U *>(smem_raw);
   U *const Sb1 = reinterpret_cast<U *>(smem_raw + TILE_BYTES);
@@ -267,7 +278,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         const int l = tid + NT * j;
-        const uint32_t row = row_of<KIND>(A.a, tile, l);
+        const uint32_t row = row_of<KIND, C>(A.a, tile, l);
         S2[l] = fma8(A.pro_beta, hx[j], scl8(A.pro_alpha * d2[row], own[j]));
 #pragma unroll
         for (int q = 0; q < PU; ++q) pt[q][j & 1] = fma(get8(own[j], q), get8(own[j], q), pt[q][j & 1]);
@@ -307,7 +318,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
 #pragma unroll
         for (int j = 0; j < R; ++j) {
           const int l = tid + NT * j;
-          const uint32_t row = row_of<KIND>(A.a, tile, l);
+          const uint32_t row = row_of<KIND, C>(A.a, tile, l);
           S[l] = sub8(fma8(A.two_r, h2[j], scl8(d2[row], hx[j])), S[l]);   // S[l] = t_{m-1}
         }
         fence_async_smem();
@@ -356,11 +367,11 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
   if (tid == 0) *A.counter = 0u;
 }
 
-// probes -> 8-byte cells [pair group][row]; probe p = g*PU + lane
+// probes -> cells [probe group][row]; probe p = g*PU + lane
 template <typename T>
 __global__ void k_cells8(int64_t dim, int ng, uint64_t seed, int64_t probe0, int nvalid,
                          const int8_t *probes, T *out) {
-  constexpr int PU = Cell8<T>::PU;
+  constexpr int PU = Cell<T>::PU;
   const int64_t total = dim * ng * PU;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -400,18 +411,20 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// A map: {chunk elems (256 B), chunks, groups}; B map: {pair elems (16 B), 2^(a-1), 2^(n-a), groups}
+// A map: {chunk cells (256 B), chunks, probes};
+// B map: {piece cells (2^C), 2^(a-C) tiles, 2^(n-a), probes}
 template <typename T>
 int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap *mA, CUtensorMap *mB) {
   auto enc = encode_fn();
   if (!enc) return fail(ctx, EL_ECUDA, "cuTensorMapEncodeTiled unavailable");
   const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-  const uint64_t dim = 1ull << n;
-  const uint64_t e256 = 256 / sizeof(T), e16 = 16 / sizeof(T);
+  constexpr int C = Cell<T>::CARRY, LOGCH = Cell<T>::LOGCH;
+  const uint64_t dim = 1ull << n, cb = sizeof(T);
+  const uint64_t e256 = 256 / cb, epc = 1ull << C;
   {
-    cuuint64_t gdim[3] = {e256, dim * 8 / 256, (cuuint64_t)ng};
-    cuuint64_t gstr[2] = {256, dim * 8};
-    cuuint32_t box[3] = {(cuuint32_t)e256, (cuuint32_t)(1u << (a - 5)), 1};
+    cuuint64_t gdim[3] = {e256, dim * cb / 256, (cuuint64_t)ng};
+    cuuint64_t gstr[2] = {256, dim * cb};
+    cuuint32_t box[3] = {(cuuint32_t)e256, (cuuint32_t)(1u << (a - LOGCH)), 1};
     cuuint32_t es[3] = {1, 1, 1};
     CUresult r = enc(mA, dt, 3, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -419,9 +432,9 @@ int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap
     if (r != CUDA_SUCCESS) return fail(ctx, EL_ECUDA, "tensor map A encode failed (%d)", (int)r);
   }
   {
-    cuuint64_t gdim[4] = {e16, 1ull << (a - 1), 1ull << (n - a), (cuuint64_t)ng};
-    cuuint64_t gstr[3] = {16, (1ull << a) * 8, dim * 8};
-    cuuint32_t box[4] = {(cuuint32_t)e16, 1, (cuuint32_t)hb, 1};
+    cuuint64_t gdim[4] = {epc, 1ull << (a - C), 1ull << (n - a), (cuuint64_t)ng};
+    cuuint64_t gstr[3] = {epc * cb, (1ull << a) * cb, dim * cb};
+    cuuint32_t box[4] = {(cuuint32_t)epc, 1, (cuuint32_t)hb, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
     CUresult r = enc(mB, dt, 4, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -434,7 +447,8 @@ int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap
 template <typename T>
 int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
             const int8_t *probes_host, int num, double c, double r, std::vector<double> &acc) {
-  constexpr int PU = Cell8<T>::PU;
+  constexpr int PU = Cell<T>::PU;
+  constexpr int C = Cell<T>::CARRY;
   const int n = h->n;
   const int64_t dim = h->basis->dim;
   const int ng = chunk / PU;
@@ -460,8 +474,10 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     k_d2_8<T><<<el::grid_for(dim, 256), 256, 0, ctx->stream>>>(n, dim, h->d_diagV64, d_delta, c, r, d2);
     EL_LAUNCH_CHECK(ctx);
   }
-  const int a = std::min(13, std::max((n + 2) / 2, n - 12));
-  const int TBA = a, TBB = n - a + 1;
+  // a: A-tile bits; the B tile has n - a + C bits; both at most 64 KB
+  const int amax = sizeof(T) == 4 ? 14 : 13;
+  const int a = std::min(amax, std::max((n + C + 1) / 2, n + C - amax));
+  const int TBA = a, TBB = n - a + C;
   const int hb = (int)std::min<int64_t>(256, (int64_t)1 << (n - a));
   CUtensorMap mA[2], mB[2];   // [P buffer, Q buffer]
   int rc = make_maps<T>(ctx, P, n, a, ng, hb, &mA[0], &mB[0]);
@@ -476,13 +492,13 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     const int TB = kind == KIND_B ? TBB : TBA;
     A.n = n; A.a = a; A.mode = mode; A.ng = ng; A.dim = dim; A.hb = hb;
     A.nbox = (int)(((int64_t)1 << (n - a)) / hb);
-    A.tiles = kind == KIND_A ? (dim >> a) : ((int64_t)1 << (a - 1));
+    A.tiles = kind == KIND_A ? (dim >> a) : ((int64_t)1 << (a - C));
     A.items = A.tiles * ng;
     A.log_tiles = 0;
     while (((int64_t)1 << A.log_tiles) < A.tiles) ++A.log_tiles;
     A.s_m = (T)s_m; A.two_r = (T)(2.0 / r); A.pro_alpha = (T)0.5; A.pro_beta = (T)(1.0 / r);
     for (int k = 0; k < TB && k < 16; ++k) {
-      int rowbit = (kind == KIND_A) ? k : (k >= 1 ? a + k - 1 : -1);
+      int rowbit = (kind == KIND_A) ? k : (k >= C ? a + k - C : -1);
       A.amp[k] = (T)((rowbit >= 0) ? 0.5 * h->om_re[rowbit] : 0.0);
     }
     A.d2 = d2; A.dots = dots; A.err = d_err; A.counter = ctx->d_counter;
@@ -492,7 +508,7 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     A.partials = ctx->d_partials;
     const CUtensorMap &mp = kind == KIND_A ? mA[pbuf] : mB[pbuf];
     const CUtensorMap &mq = kind == KIND_A ? mA[pbuf ^ 1] : mB[pbuf ^ 1];
-    const size_t smem = (size_t)3 * ((size_t)1 << TB) * 8;
+    const size_t smem = (size_t)3 * ((size_t)1 << TB) * sizeof(T);
     bool ok = false;
 #define EL_TCASE(TBV, KV)                                                                     \
   if (TB == TBV && kind == KV) {                                                              \
@@ -503,6 +519,7 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   }
     EL_TCASE(10, KIND_A) EL_TCASE(11, KIND_A) EL_TCASE(12, KIND_A) EL_TCASE(13, KIND_A)
     EL_TCASE(10, KIND_B) EL_TCASE(11, KIND_B) EL_TCASE(12, KIND_B) EL_TCASE(13, KIND_B)
+    if constexpr (sizeof(T) == 4) { EL_TCASE(14, KIND_A) EL_TCASE(14, KIND_B) }
 #undef EL_TCASE
     if (!ok) return fail(ctx, EL_EINVAL, "TMA pass with %d tile bits not instantiated", TB);
     EL_LAUNCH_CHECK(ctx);
@@ -557,9 +574,8 @@ namespace el {
 bool kpm_tma_eligible(const el_ham *h, int dtype, int chunk) {
   if (h->basis->layout != EL_LAYOUT_FULL || h->complex_drive) return false;
   if (h->n < 20 || h->n > 25) return false;
-  const int pu = (dtype == EL_F32) ? 2 : 1;
   if (dtype != EL_F32 && dtype != EL_F64) return false;
-  return chunk % pu == 0 && chunk / pu <= 128;
+  return chunk >= 1 && chunk <= 128;
 }
 
 int kpm_tma(el_ctx *ctx, el_ham *h, int dtype, int num, int nvec, int chunk, uint64_t seed,

@@ -135,7 +135,7 @@ def test_tiled_kpm_matches_oracle(ctx, n, dtype, tol):
     assert np.abs(gen - want).max() < tol
 
 
-@pytest.mark.parametrize("n", [20, 22])
+@pytest.mark.parametrize("n", [20, 21, 22, 23, 24, 25])
 @pytest.mark.parametrize("dtype,tol", [("float64", 1e-10), ("float32", 2e-4)])
 def test_tma_kpm_matches_generic_kernel(ctx, n, dtype, tol):
     """TMA-fed tiled KPM (20 <= N <= 25) vs the row-parallel kernel on the same
