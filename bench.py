@@ -34,18 +34,29 @@ NUM, NVEC, CHUNK = 1024, 32, 32
 WORKLOAD = "kpm_dos_square25"
 
 
-def workload():
+def workload(sites=25):
+    """The 5x5 lattice; sites < 25 keeps the first `sites` atoms (a smaller
+    case of the same kernels, for profiler captures)."""
     from energy_level_b200 import configs
     cfg = configs.square25()
+    if sites != 25:
+        if not 14 <= sites <= 25:
+            raise ValueError("--sites must be in [14, 25]")
+        calib = dict(cfg["calib"])
+        calib["atoms"] = calib["atoms"][:sites]
+        calib["pairs"] = [p for p in calib["pairs"] if p["i"] < sites and p["j"] < sites]
+        cfg = dict(cfg, n=sites, calib=calib, Om=cfg["Om"][:sites], delta=cfg["delta"][:sites])
     return cfg
 
 
 def config_dict(cfg, extra=None):
-    d = {"workload": WORKLOAD, "lattice": "5x5 square a=6um", "n_sites": 25, "basis": "full 2^25",
-         "dim": 1 << 25, "moments": NUM, "probes": NVEC, "probe_block": CHUNK,
+    n = cfg["n"]
+    d = {"workload": WORKLOAD if n == 25 else WORKLOAD + "_first%d" % n,
+         "lattice": "5x5 square a=6um" + ("" if n == 25 else " (first %d sites)" % n),
+         "n_sites": n, "basis": "full 2^%d" % n, "dim": 1 << n, "moments": NUM, "probes": NVEC, "probe_block": CHUNK,
          "vectors": "float32", "moment_accumulation": "float64",
          "recurrence": "Chebyshev doubling (T2n=2Tn^2-T0)",
-         "l2": "inputs larger than L2 (probe block 4.3 GB per vector)"}
+         "l2": "inputs larger than L2 (probe block %.2f GB per vector)" % ((1 << n) * NVEC * 4 / 1e9)}
     if extra:
         d.update(extra)
     return d
@@ -147,14 +158,14 @@ def cpu_sample(cfg, moments=8, probes=2):
     ob.kpm_full(n, cfg["Om"], d, c, r, moments, z)
     dt = time.perf_counter() - t0
     return dt / (moments * probes), int(lib.oracle_threads()), \
-        "N=25 full basis, %d probes x %d moments (direct recurrence, FP64)" % (probes, moments)
+        "N=%d full basis, %d probes x %d moments (direct recurrence, FP64)" % (n, probes, moments)
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    cfg = workload()
+    cfg = workload(args.sites)
     times = []
     for i in range(args.warmup + args.steps):
         tpm, threads, desc = cpu_sample(cfg)
@@ -195,7 +206,7 @@ def run_native(args):
     from energy_level_b200 import kpm as bkpm, solvers
     from energy_level_b200.core import Context, Basis, Hamiltonian
 
-    cfg = workload()
+    cfg = workload(args.sites)
     n = cfg["n"]
     pairs = [(p["i"], p["j"], p["V"]) for p in cfg["calib"]["pairs"]]
     ctx = Context(local)
@@ -302,7 +313,7 @@ def run_native(args):
             "config": config_dict(cfg, {"parallelism": "replicas" if world > 1 else "single GPU"}),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_kpm_pass (one Chebyshev step of 32 probes over 2^25 rows)",
+                         "kernel": "k_kpm_tma (one Chebyshev step of 32 probes over 2^%d rows)" % n,
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_s * 1e3,
                          "peak_source": peak_kind},
             "cpu_baseline": cpu,
@@ -322,16 +333,663 @@ def run_native(args):
     return 0
 
 
+# ------------------------------------------------- further workloads (C1, C3-C5, H.v)
+
+WORKLOADS = ("kpm_dos_square25", "hv_chain31", "lanczos_chain12", "ramp_chain31", "batch512",
+             "adjoint_ring20")
+DEFAULT_STEPS = {"kpm_dos_square25": 5, "hv_chain31": 200, "lanczos_chain12": 50, "ramp_chain31": 3,
+                 "batch512": 10, "adjoint_ring20": 5}
+
+
+class Harness:
+    """Device, optional process group (replicas), CUDA-event timing with
+    clock sampling, max over ranks."""
+
+    def __init__(self, args):
+        import torch
+        self.torch = torch
+        self.args = args
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        if not torch.cuda.is_available():
+            raise RuntimeError("CUDA 不可用")
+        torch.cuda.set_device(self.local)
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+        from energy_level_b200.build import build
+        build()
+        from energy_level_b200.core import default_context
+        self.ctx = default_context(self.local)        # the context the public API calls use too
+        self.stream = torch.cuda.current_stream()
+
+    def event(self):
+        return self.torch.cuda.Event(enable_timing=True)
+
+    def barrier(self):
+        self.torch.cuda.synchronize()
+        if self.dist:
+            self.dist.barrier()
+
+    def timed(self, fn, steps):
+        """Seconds for `steps` calls of fn between CUDA events (max over ranks),
+        launches counted by the context, clocks sampled meanwhile."""
+        self.barrier()
+        l0 = self.ctx.launches
+        with ClockSampler(self.local) as clk:
+            self.barrier()
+            a, b = self.event(), self.event()
+            a.record(self.stream)
+            for _ in range(steps):
+                fn()
+            b.record(self.stream)
+            self.barrier()
+        return self.max_over_ranks(a.elapsed_time(b) / 1e3), self.ctx.launches - l0, clk.summary()
+
+    def max_over_ranks(self, v):
+        if not self.dist:
+            return float(v)
+        t = self.torch.tensor([float(v)], device="cuda", dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t[0])
+
+    def close(self):
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def base_line(args, world, name, value, unit, steps, elapsed, dtype, config, higher=True):
+    return {"metric": METRIC, "value": value, "unit": unit, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": elapsed / steps * 1e3, "higher_is_better": higher,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic (seeded lattices, C6/r^6 couplings; no dataset)",
+            "config": dict({"workload": name, "parallelism": "replicas" if world > 1 else "single GPU"},
+                           **config)}
+
+
+def roofline(alg_bytes, launch_s, traffic=None, kernel=""):
+    peak, kind = measured_peak()
+    ach = alg_bytes / launch_s / 1e9
+    return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "traffic": traffic, "kernel": kernel, "algorithmic_bytes_per_launch": alg_bytes,
+            "launch_ms": launch_s * 1e3, "peak_source": kind}
+
+
+def chain_model(n, Om=2.0, Delta=0.0):
+    from energy_level_b200 import configs
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+    pairs = [(p["i"], p["j"], p["V"]) for p in calib["pairs"]]
+    return calib, pairs, np.full(n, Om), np.full(n, -Delta)
+
+
+def _threads():
+    try:
+        from oracle import build as ob
+        return int(ob.load().oracle_threads())
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# --- H.v GB/s on the 31-site chain blockade sector (dim F(33) = 3,524,578)
+
+HV_N, HV_NVEC = 31, 8
+
+
+def cpu_hv_sample(n=25):
+    """numpy restatement of ChannelKernel.matvec on a 25-site chain sector."""
+    from oracle import ref
+    calib, pairs, om, de = chain_model(n)
+    codes = ref.independent_states(n, [[i, i + 1] for i in range(n - 1)], None)
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=len(codes)) + 1j * rng.normal(size=len(codes))
+    ref.hv(n, codes, om, de, pairs, x)                       # warm
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        ref.hv(n, codes, om, de, pairs, x)
+    dt = (time.perf_counter() - t0) / reps
+    gbs = len(codes) * (2 * 16 + 8) / dt / 1e9
+    return gbs, "chain N=%d blockade sector (dim %d), complex128, 1 vector, numpy (1 thread)" % (n, len(codes))
+
+
+def native_hv(h, args):
+    torch = h.torch
+    import ctypes as C
+    from energy_level_b200 import _lib
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import configs
+    n = HV_N
+    calib, pairs, om, de = chain_model(n)
+    basis = Basis(h.ctx, n, "blockade", edges=configs.chain_edges(n))
+    ham = Hamiltonian(h.ctx, basis, om, de, pairs)
+    dim = basis.dim
+    g = torch.Generator(device="cuda").manual_seed(7 + h.rank)
+
+    def vecs(dt):
+        return torch.randn(dim, HV_NVEC, dtype=dt, device="cuda", generator=g)
+
+    def apply(x, y, code):
+        h.ctx.call("el_hv", ham.handle, C.c_int(code), C.c_int(HV_NVEC), C.c_void_p(x.data_ptr()),
+                   C.c_void_p(y.data_ptr()))
+
+    extra = {}
+    for dt, code, nv, sz in ((torch.complex64, _lib.EL_C64, 1, 8), (torch.complex128, _lib.EL_C128, 1, 16),
+                             (torch.complex64, _lib.EL_C64, 2, 8), (torch.complex64, _lib.EL_C64, 4, 8)):
+        xa = torch.randn(dim, nv, dtype=dt, device="cuda", generator=g)
+        ya = torch.empty_like(xa)
+        f = (lambda xa=xa, ya=ya, code=code, nv=nv: h.ctx.call(
+            "el_hv", ham.handle, C.c_int(code), C.c_int(nv), C.c_void_p(xa.data_ptr()), C.c_void_p(ya.data_ptr())))
+        for _ in range(args.warmup):
+            f()
+        tt, _, _ = h.timed(f, max(20, args.steps // 4))
+        tt /= max(20, args.steps // 4)
+        bb = dim * (2 * nv * sz + (4 if sz == 8 else 8))
+        extra["%s_x%d" % ("c64" if sz == 8 else "c128", nv)] = {"gbs": bb / tt / 1e9, "us_per_hv": tt * 1e6,
+                                                                "working_set_mb": bb / 1e6}
+        del xa, ya
+    x32, y32 = vecs(torch.complex64), torch.empty(dim, HV_NVEC, dtype=torch.complex64, device="cuda")
+    x64, y64 = x32.to(torch.complex128), torch.empty(dim, HV_NVEC, dtype=torch.complex128, device="cuda")
+    steps = args.steps
+    for _ in range(args.warmup):
+        apply(x32, y32, _lib.EL_C64)
+        apply(x64, y64, _lib.EL_C128)
+    el32, launches, clocks = h.timed(lambda: apply(x32, y32, _lib.EL_C64), steps)
+    el64, _, _ = h.timed(lambda: apply(x64, y64, _lib.EL_C128), steps)
+    apply(x32, y32, _lib.EL_C64)
+    apply(x64, y64, _lib.EL_C128)
+    torch.cuda.synchronize()
+    err = float((y32.to(torch.complex128) - y64).abs().max() / y64.abs().max())
+    b32 = dim * (2 * HV_NVEC * 8 + 4)
+    b64 = dim * (2 * HV_NVEC * 16 + 8)
+    t32, t64 = el32 / steps, el64 / steps
+    value = h.world * b32 / t32 / 1e9
+    # end to end: host (pinned) vectors in, H.v, result out, through el_hv_host
+    xh = x32.cpu().pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    b0 = h.ctx.copied_bytes
+    reps = max(3, min(steps, 20))
+    te = time.perf_counter()
+    for _ in range(reps):
+        h.ctx.call("el_hv_host", ham.handle, C.c_int(_lib.EL_C64), C.c_int(HV_NVEC),
+                   C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr()))
+    e2e_s = (time.perf_counter() - te) / reps
+    b1 = h.ctx.copied_bytes
+    line = base_line(args, h.world, "hv_chain31", value, "GB/s", steps, el32, "c64",
+                     {"n_sites": n, "basis": "chain nearest-neighbour blockade sector", "dim": dim,
+                      "vectors": HV_NVEC, "pairs": len(pairs), "form": "complex64 x 8 vectors",
+                      "l2": "inputs larger than L2 (x and y 225 MB each)"})
+    line.update({
+        "roofline": roofline(b32, t32, kernel="k_apply<float,complex> (fused H.v, 8 vectors)"),
+        "e2e": {"value": h.world * b32 / e2e_s / 1e9, "unit": "GB/s",
+                "h2d_bytes_per_step": (b1[0] - b0[0]) // reps, "d2h_bytes_per_step": (b1[1] - b0[1]) // reps},
+        "gpu_launches": launches, "clocks": clocks,
+        "plain_fp64": {"gbs": b64 / t64 / 1e9, "ms_per_hv": t64 * 1e3, "form": "complex128 x 8 vectors"},
+        "chosen_vs_plain_vectors_per_s": t64 / t32,
+        "other_shapes": extra,
+        "error_vs_fp64": {"max_rel_hv": err},
+    })
+    return line
+
+
+# --- C1: 12-site chain ground state
+
+def native_lanczos12(h, args):
+    torch = h.torch
+    from energy_level_b200 import configs, solvers
+    from energy_level_b200.batched import BatchedGroundStates
+    from energy_level_b200.core import Basis, Hamiltonian
+    cfg = configs.chain12()
+    n = cfg["n"]
+    pairs = [(p["i"], p["j"], p["V"]) for p in cfg["calib"]["pairs"]]
+    E_ref = -10.2963231346414
+    inst = [dict(calib=cfg["calib"], Om=cfg["Om"], delta=cfg["delta"], edges=None)]
+    b32 = BatchedGroundStates(inst, dtype="float32", max_iter=200, ctx=h.ctx)
+    b32.autotune()
+    steps = args.steps
+    for _ in range(args.warmup):
+        b32.run()
+    el, launches, clocks = h.timed(lambda: b32.run(), steps)
+    r32 = b32.results()
+    # plain FP64: the host-driven FP64 Lanczos (tol 1e-12, Gaussian start, seed 0)
+    basis = Basis(h.ctx, n, "full")
+    ham = Hamiltonian(h.ctx, basis, cfg["Om"], cfg["delta"], pairs)
+
+    def plain():
+        return solvers.lanczos_ground(ham, dtype="float64", seed=0, max_iter=300, tol=1e-12, nev=2)
+    for _ in range(args.warmup):
+        plain()
+    psteps = max(3, steps // 5)
+    el64, _, _ = h.timed(plain, psteps)
+    r64 = plain()
+    b64 = BatchedGroundStates(inst, dtype="float64", max_iter=200, tol=1e-12, ctx=h.ctx)
+    b64.run()
+    el64b, _, _ = h.timed(lambda: b64.run(), psteps)
+    r64b = b64.results()
+    e32 = float(r32["E0"][0])
+    value = h.world * steps / el
+    # end to end: public ground-state call with host model arrays, energies back
+    from energy_level_b200.batched import batched_ground_states
+    b0 = h.ctx.copied_bytes
+    reps = 5
+    te = time.perf_counter()
+    for _ in range(reps):
+        batched_ground_states(inst, dtype="float32")
+    e2e_s = (time.perf_counter() - te) / reps
+    b1 = h.ctx.copied_bytes
+    cpu = None
+    if h.rank == 0 and h.world == 1 and not args.no_cpu:
+        cpu = cpu_lanczos12()
+    line = base_line(args, h.world, "lanczos_chain12", value, "solves/s", steps, el, "f32",
+                     {"n_sites": n, "basis": "full 2^12", "dim": 4096, "Om": 2.0, "delta": -1.0,
+                      "form": "persistent Lanczos kernel, FP32 vectors, FP64 alpha/beta, one launch per solve",
+                      "l2": "latency-bound (dim 4096 fits in L2)"})
+    line.update({
+        "roofline": None,
+        "e2e": {"value": h.world / e2e_s, "unit": "solves/s",
+                "h2d_bytes_per_step": (b1[0] - b0[0]) // reps, "d2h_bytes_per_step": (b1[1] - b0[1]) // reps},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+        "plain_fp64": {"solves_per_s": psteps / el64, "form": "host-driven FP64 Lanczos (el_lanczos_ground, tol 1e-12)",
+                       "E0": float(r64["evals"][0])},
+        "fp64_persistent": {"solves_per_s": psteps / el64b, "E0": float(r64b["E0"][0])},
+        "chosen_vs_plain": (steps / el) / (psteps / el64),
+        "error_vs_fp64": {"rel_E0": abs(e32 - float(r64["evals"][0])) / abs(float(r64["evals"][0])),
+                          "abs_E0_vs_reference_golden": abs(float(r64["evals"][0]) - E_ref)},
+    })
+    b32.close()
+    b64.close()
+    return line
+
+
+def cpu_lanczos12():
+    """Reference path: eigsh(k=2, 'SA') on the numpy H.v (equilibrium.py:85)."""
+    import scipy.sparse.linalg as spla
+    from energy_level_b200 import configs
+    from oracle import ref
+    cfg = configs.chain12()
+    n = cfg["n"]
+    pairs = [(p["i"], p["j"], p["V"]) for p in cfg["calib"]["pairs"]]
+    op = spla.LinearOperator((4096, 4096), matvec=lambda v: ref.hv(n, None, cfg["Om"], cfg["delta"], pairs, v),
+                             dtype=float)
+    v0 = np.random.default_rng(0).normal(size=4096)
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        spla.eigsh(op, k=2, which="SA", v0=v0, tol=0)
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": 1.0 / dt, "unit": "solves/s", "cores": 1, "kind": "port",
+            "sample": "full C1 solve: ARPACK eigsh(k=2,'SA',tol=0) on the numpy H.v, 3 repetitions"}
+
+
+# --- C3: 31-site chain ramp, 300 piecewise-constant steps
+
+def ramp_runner(h, dtype, tol):
+    torch = h.torch
+    from energy_level_b200 import configs, solvers
+    from energy_level_b200.core import Basis, Hamiltonian
+    cfg = configs.chain31()
+    n = cfg["n"]
+    pairs = [(p["i"], p["j"], p["V"]) for p in cfg["calib"]["pairs"]]
+    basis = Basis(h.ctx, n, "blockade", edges=cfg["edges"])
+    segs = cfg["segments"]
+    ham = Hamiltonian(h.ctx, basis, segs[0]["Om"], segs[0]["delta"], pairs)
+    psi = torch.zeros(basis.dim, dtype=getattr(torch, dtype), device="cuda")
+    dt = 3000.0 / len(segs)
+
+    def solve():
+        psi.zero_()
+        psi[0] = 1.0                                          # all-g is code 0, rank 0
+        for s in segs:
+            ham.set_drive(s["Om"], s["delta"])
+            solvers.cheb_step(ham, psi, dt, tol=tol)
+        return psi
+    return cfg, basis, ham, solve
+
+
+def native_ramp31(h, args):
+    torch = h.torch
+    from energy_level_b200 import solvers
+    cfg, basis, ham32, solve32 = ramp_runner(h, "complex64", 1e-7)
+    steps = args.steps
+    for _ in range(args.warmup):
+        solve32()
+    el, launches, clocks = h.timed(solve32, steps)
+    psi32 = solve32().clone()
+    n32, _ = solvers.observables(ham32, psi32)
+    _, _, ham64, solve64 = ramp_runner(h, "complex128", 1e-13)
+    solve64()
+    psteps = max(1, steps)
+    el64, _, _ = h.timed(solve64, psteps)
+    psi64 = solve64().clone()
+    n64, _ = solvers.observables(ham64, psi64)
+    p32n = psi32.to(torch.complex128)
+    norm32, norm64 = float(p32n.norm()), float(psi64.norm())
+    fid = float(abs(torch.vdot(psi64, p32n)) ** 2) / (norm32 ** 2 * norm64 ** 2)
+    value = h.world * steps / el
+    # end to end through engine.evolve_manybody (public API, host state grammar in, observables out)
+    from energy_level_b200.engine import evolve_manybody
+    from energy_level_b200 import configs
+    plan = {"projected": True, "blockade_edges": cfg["edges"], "constraint": {"kind": "blockade"}}
+    b0 = h.ctx.copied_bytes
+    te = time.perf_counter()
+    res = evolve_manybody(cfg["calib"], psi0=cfg["psi0"], t_grid=cfg["t_grid"], segments=cfg["segments"],
+                          plan=plan, dtype="complex64", want_corr=False, want_entropy=False)
+    e2e_s = time.perf_counter() - te
+    b1 = h.ctx.copied_bytes
+    cpu = None
+    if h.rank == 0 and h.world == 1 and not args.no_cpu:
+        cpu = cpu_ramp_sample(basis.dim)
+    line = base_line(args, h.world, "ramp_chain31", value, "solves/s", steps, el, "c64",
+                     {"n_sites": 31, "basis": "chain nearest-neighbour blockade sector", "dim": basis.dim,
+                      "segments": 300, "T_ns": 3000.0, "Om": 2.0, "Delta": "-6 -> +6 linear (left rule)",
+                      "propagator": "Chebyshev (Jacobi-Anger), tol 1e-7", "psi0": "all g",
+                      "l2": "state 28 MB x 4 live vectors: partly L2-resident (reported, no HBM claim)"})
+    line.update({
+        "roofline": None,
+        "e2e": {"value": h.world / e2e_s, "unit": "solves/s",
+                "h2d_bytes_per_step": b1[0] - b0[0], "d2h_bytes_per_step": b1[1] - b0[1]},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+        "plain_fp64": {"solves_per_s": psteps / el64, "form": "complex128, tol 1e-13"},
+        "chosen_vs_plain": (steps / el) / (psteps / el64),
+        "error_vs_fp64": {"infidelity": 1.0 - fid, "norm_deviation": abs(norm32 - 1.0),
+                          "max_abs_n_i": float(np.max(np.abs(n32 - n64))),
+                          "max_abs_n_i_normalised": float(np.max(np.abs(n32 / norm32 ** 2 - n64 / norm64 ** 2))),
+                          "e2e_max_abs_n_i": float(np.max(np.abs(res["pops_atom"][-1] - n64)))},
+    })
+    return line
+
+
+def cpu_ramp_sample(full_dim, n=25, segments=8):
+    """Reference propagation (CSR per drive + expm_multiply, engine_ed.py:130-147)
+    on a 25-site chain sector for a few segments, extrapolated in dim x segments."""
+    from energy_level_b200 import configs
+    from oracle import ref
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+    pairs = [(p["i"], p["j"], p["V"]) for p in calib["pairs"]]
+    codes = ref.independent_states(n, configs.chain_edges(n), None)
+    dt = 10.0
+    segs = [{"t0": k * dt, "Om": np.full(n, 2.0), "delta": np.full(n, 6.0 - 0.04 * k)} for k in range(segments)]
+    psi0 = np.zeros(len(codes), complex)
+    psi0[0] = 1.0
+    t0 = time.perf_counter()
+    ref.evolve_segments(n, codes, pairs, segs, psi0, [0.0, segments * dt])
+    el = time.perf_counter() - t0
+    per = el / segments / len(codes)
+    solve_s = per * 300 * full_dim
+    return {"value": 1.0 / solve_s, "unit": "solves/s", "cores": _threads(), "kind": "port",
+            "sample": "chain N=%d sector (dim %d), %d segments of CSR build + expm_multiply; "
+                      "extrapolated linearly in dim x segments to dim %d x 300" % (n, len(codes), segments, full_dim)}
+
+
+# --- C4: 512 disordered chains in one persistent launch
+
+def native_batch512(h, args):
+    torch = h.torch
+    from energy_level_b200 import configs, solvers
+    from energy_level_b200.batched import BatchedGroundStates, batched_ground_states
+    from energy_level_b200.core import Basis, Hamiltonian
+    insts = configs.batch512()
+    b = BatchedGroundStates(insts, dtype="float32", max_iter=300, ctx=h.ctx)
+    best, timings = b.autotune()
+    graph = b.capture()
+    steps = args.steps
+    for _ in range(args.warmup):
+        graph.replay()
+    el, launches, clocks = h.timed(graph.replay, steps)
+    r32 = b.results()
+    # plain FP64: host-driven FP64 Lanczos per instance on a sample, extrapolated
+    sample = list(range(0, len(insts), 32))
+    hams = []
+    for i in sample:
+        inst = insts[i]
+        pairs = [(p["i"], p["j"], p["V"]) for p in inst["calib"]["pairs"]]
+        bs = Basis(h.ctx, inst["n"], "blockade", edges=inst["edges"])
+        hams.append((bs, Hamiltonian(h.ctx, bs, inst["Om"], inst["delta"], pairs)))
+    e64 = []
+
+    def plain():
+        e64.clear()
+        for _, hm in hams:
+            e64.append(float(solvers.lanczos_ground(hm, dtype="float64", seed=0, max_iter=300, tol=1e-10,
+                                                    nev=2)["evals"][0]))
+    plain()
+    el64, _, _ = h.timed(plain, 1)
+    plain_rate = len(sample) / el64
+    rel = np.abs(r32["E0"][sample] - np.asarray(e64)) / np.abs(np.asarray(e64))
+    value = h.world * len(insts) * steps / el
+    b0 = h.ctx.copied_bytes
+    te = time.perf_counter()
+    out = batched_ground_states(insts, dtype="float32", max_iter=300)
+    e2e_s = time.perf_counter() - te
+    b1 = h.ctx.copied_bytes
+    cpu = None
+    if h.rank == 0 and h.world == 1 and not args.no_cpu:
+        cpu = cpu_batch_sample(insts)
+    dims = [configs_fib(inst["n"] + 2) for inst in insts]
+    line = base_line(args, h.world, "batch512", value, "solves/s", steps, el, "f32",
+                     {"instances": len(insts), "n_sites": "16..22", "dims": [min(dims), max(dims)],
+                      "mean_dim": float(np.mean(dims)), "form": "one persistent launch (CUDA graph), FP32 vectors, "
+                      "FP64 alpha/beta and tridiagonal", "launch": {"threads": best[0], "ctas_per_sm": best[1]},
+                      "l2": "8.6M rows x 4 B per vector; working set partly L2-resident"})
+    line.update({
+        "roofline": None,
+        "e2e": {"value": h.world * len(insts) / e2e_s, "unit": "solves/s",
+                "h2d_bytes_per_step": b1[0] - b0[0], "d2h_bytes_per_step": b1[1] - b0[1]},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+        "autotune_ms": {"%dx%d" % k: v for k, v in timings.items()},
+        "converged": int(np.sum(r32["converged"])),
+        "plain_fp64": {"solves_per_s": plain_rate, "form": "host-driven FP64 Lanczos per instance "
+                       "(every 32nd instance timed, rate extrapolated)"},
+        "chosen_vs_plain": (len(insts) * steps / el) / plain_rate,
+        "error_vs_fp64": {"max_rel_E0": float(rel.max()), "e2e_max_rel_E0":
+                          float(np.max(np.abs(out["E0"][sample] - np.asarray(e64)) / np.abs(np.asarray(e64))))},
+    })
+    b.close()
+    return line
+
+
+def configs_fib(k):
+    a, b = 0, 1
+    for _ in range(k):
+        a, b = b, a + b
+    return a
+
+
+def cpu_batch_sample(insts, count=3):
+    """Reference per-instance path: eigsh(k=2,'SA') on the numpy H.v of the
+    blockade sector, a few instances, extrapolated by the instances' dims."""
+    import scipy.sparse.linalg as spla
+    from oracle import ref
+    idx = [0, 1, 2][:count]
+    tot_dim = sum(configs_fib(inst["n"] + 2) for inst in insts)
+    el, sd = 0.0, 0
+    for i in idx:
+        inst = insts[i]
+        n = inst["n"]
+        pairs = [(p["i"], p["j"], p["V"]) for p in inst["calib"]["pairs"]]
+        codes = ref.independent_states(n, inst["edges"], None)
+        H = ref.sparse_h(n, codes, inst["Om"], inst["delta"], pairs)
+        v0 = np.random.default_rng(0).normal(size=len(codes))
+        t0 = time.perf_counter()
+        spla.eigsh(H, k=2, which="SA", v0=v0, tol=0)
+        el += time.perf_counter() - t0
+        sd += len(codes)
+    solve_s = el / sd * tot_dim
+    return {"value": len(insts) / solve_s, "unit": "solves/s", "cores": _threads(), "kind": "port",
+            "sample": "%d instances, ARPACK eigsh(k=2,'SA') on CSR; extrapolated by total dim" % len(idx)}
+
+
+# --- C5: adjoint pulse gradient on the 20-site ring
+
+def native_adjoint20(h, args):
+    torch = h.torch
+    from energy_level_b200 import configs, solvers
+    from energy_level_b200.adjoint import PulseProblem, pulse_fidelity
+    cfg = configs.ring20()
+    n = cfg["n"]
+    plan = {"projected": True, "blockade_edges": cfg["edges"], "constraint": {"kind": "blockade"}}
+    tau, om, Delta = cfg["tau"], cfg["omega_k"], -cfg["delta_k"]
+    p32 = PulseProblem(cfg["calib"], cfg["psi0"], target=cfg["target"], plan=plan, dtype="complex64")
+    p64 = PulseProblem(cfg["calib"], cfg["psi0"], target=cfg["target"], plan=plan, dtype="complex128")
+    steps = args.steps
+    for _ in range(args.warmup):
+        p32.evaluate(tau, om, Delta)
+    el, launches, clocks = h.timed(lambda: p32.evaluate(tau, om, Delta), steps)
+    F32, g32, d32 = p32.evaluate(tau, om, Delta)
+    p64.evaluate(tau, om, Delta)
+    el64a, _, _ = h.timed(lambda: p64.evaluate(tau, om, Delta), max(1, steps // 2))
+    F64, g64, d64 = p64.evaluate(tau, om, Delta)
+    # plain FP64: central finite differences of complex128 forward evolutions
+    ham, psi0, tgt = p64.ham, p64.psi0, p64.target
+    psi = torch.empty_like(psi0)
+    tol = 1e-13
+
+    def forward(o, d):
+        psi.copy_(psi0)
+        for k in range(len(tau)):
+            ham.set_drive(np.full(n, o[k]), np.full(n, -d[k]))
+            solvers.cheb_step(ham, psi, tau[k], tol=tol)
+        return float(abs(torch.vdot(tgt, psi)) ** 2)
+    forward(om, Delta)
+    el_fw, _, _ = h.timed(lambda: forward(om, Delta), 2)
+    fd_grad_s = el_fw / 2 * (4 * len(tau) + 1)
+    hstep = 1e-4
+    fd = []
+    for k in (0, len(tau) // 2, len(tau) - 1):
+        e = np.zeros(len(tau))
+        e[k] = hstep
+        fd.append(((forward(om + e, Delta) - forward(om - e, Delta)) / (2 * hstep), g64[k]))
+        fd.append(((forward(om, Delta + e) - forward(om, Delta - e)) / (2 * hstep), d64[k]))
+    fd = np.asarray(fd)
+    scale = max(np.abs(g64).max(), np.abs(d64).max())
+    value = h.world * steps / el
+    # end to end: torch autograd through pulse_fidelity with host parameter tensors
+    omt = torch.tensor(om, dtype=torch.float64, requires_grad=True)
+    det = torch.tensor(Delta, dtype=torch.float64, requires_grad=True)
+    b0 = h.ctx.copied_bytes
+    reps = max(2, min(steps, 5))
+    te = time.perf_counter()
+    for _ in range(reps):
+        omt.grad = None
+        det.grad = None
+        Fv = pulse_fidelity(omt, det, p32, tau)
+        Fv.backward()
+    e2e_s = (time.perf_counter() - te) / reps
+    b1 = h.ctx.copied_bytes
+    cpu = None
+    if h.rank == 0 and h.world == 1 and not args.no_cpu:
+        cpu = cpu_adjoint_sample(cfg)
+    line = base_line(args, h.world, "adjoint_ring20", value, "grads/s", steps, el, "c64",
+                     {"n_sites": n, "basis": "ring nearest-neighbour blockade sector", "dim": p32.basis.dim,
+                      "pulse_steps": len(tau), "T_ns": float(np.sum(tau)), "objective": "|<Z2|psi(T)>|^2",
+                      "parameters": 2 * len(tau), "form": "adjoint through the Chebyshev steps, complex64, "
+                      "terms recomputed per step", "l2": "dim 15,127: L2-resident (latency-bound)"})
+    line.update({
+        "roofline": None,
+        "e2e": {"value": h.world / e2e_s, "unit": "grads/s",
+                "h2d_bytes_per_step": (b1[0] - b0[0]) // reps, "d2h_bytes_per_step": (b1[1] - b0[1]) // reps},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks, "F": F32,
+        "plain_fp64": {"grads_per_s": 1.0 / fd_grad_s, "form": "central FD (h=1e-4) of complex128 forward "
+                       "evolutions, 801 forwards per gradient (2 timed, extrapolated)"},
+        "adjoint_fp64": {"grads_per_s": max(1, steps // 2) / el64a},
+        "chosen_vs_plain": (steps / el) * fd_grad_s,
+        "error_vs_fp64": {"rel_grad_c64_vs_c128_adjoint": float(max(np.abs(g32 - g64).max(), np.abs(d32 - d64).max()) / scale),
+                          "abs_F": abs(F32 - F64),
+                          "rel_c128_adjoint_vs_fd": float(np.max(np.abs(fd[:, 0] - fd[:, 1])) / scale)},
+    })
+    return line
+
+
+def cpu_adjoint_sample(cfg):
+    """Reference forward (CSR per step + expm_multiply) on the first 40 pulse
+    steps, scaled to a full forward; an FD gradient needs 4K + 1 = 801 forwards."""
+    from oracle import ref
+    n = cfg["n"]
+    codes = ref.independent_states(n, cfg["edges"], None)
+    pairs = [(p["i"], p["j"], p["V"]) for p in cfg["calib"]["pairs"]]
+    tau = cfg["tau"]
+    t0s = np.concatenate([[0.0], np.cumsum(tau)[:-1]])
+    segs = [{"t0": float(t), "Om": np.full(n, cfg["omega_k"][k]), "delta": np.full(n, cfg["delta_k"][k])}
+            for k, t in enumerate(t0s)]
+    psi0 = np.zeros(len(codes), complex)
+    psi0[0] = 1.0
+    K = 40
+    t0 = time.perf_counter()
+    ref.evolve_segments(n, codes, pairs, segs[:K], psi0, [0.0, float(np.sum(tau[:K]))])
+    el = (time.perf_counter() - t0) * len(tau) / K
+    return {"value": 1.0 / (el * (4 * len(tau) + 1)), "unit": "grads/s", "cores": _threads(), "kind": "port",
+            "sample": "%d of %d pulse steps of one forward (CSR + expm_multiply), scaled to 801 forwards "
+                      "per FD gradient" % (K, len(tau))}
+
+
+NATIVE = {"hv_chain31": native_hv, "lanczos_chain12": native_lanczos12, "ramp_chain31": native_ramp31,
+          "batch512": native_batch512, "adjoint_ring20": native_adjoint20}
+
+
+def run_native_workload(args):
+    h = Harness(args)
+    line = NATIVE[args.workload](h, args)
+    if h.rank == 0:
+        print(json.dumps(line))
+    h.close()
+    return 0
+
+
+def run_reference_workload(args):
+    """CPU reference arm for the further workloads (rank 0 only)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    from energy_level_b200 import configs
+    w = args.workload
+    if w == "hv_chain31":
+        vals = [cpu_hv_sample()[0] for _ in range(args.steps)]
+        v, desc = float(np.mean(vals)), cpu_hv_sample()[1]
+        cb = {"value": v, "unit": "GB/s", "cores": 1, "kind": "port", "sample": desc}
+        unit = "GB/s"
+    elif w == "lanczos_chain12":
+        cb = cpu_lanczos12()
+        v, unit = cb["value"], "solves/s"
+    elif w == "ramp_chain31":
+        cb = cpu_ramp_sample(configs_fib(33))
+        v, unit = cb["value"], "solves/s"
+    elif w == "batch512":
+        cb = cpu_batch_sample(configs.batch512())
+        v, unit = cb["value"], "solves/s"
+    else:
+        cb = cpu_adjoint_sample(configs.ring20())
+        v, unit = cb["value"], "grads/s"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": unit, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w}, "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD, choices=WORKLOADS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--sites", type=int, default=25,
+                    help="keep the first SITES atoms of the 5x5 lattice (profiler-sized cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.steps is None:
+        args.steps = DEFAULT_STEPS[args.workload]
+    if args.workload != WORKLOAD:
+        if args.impl == "reference":
+            return run_reference_workload(args)
+        return run_native_workload(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_native(args)

@@ -157,6 +157,235 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev B, HamArgs<S> H, KArgs K
   if (K.want) reduce4(K, q0, q1, q2, q3);
 }
 
+// ------------------------------------------------- row kernel (FULL/CHAIN/RING)
+// One thread per row and all NV vectors of that row (NV <= 8): the code of a
+// row is recovered once and every flip gather moves the row's whole NV-vector
+// segment with 16-byte loads.  The bit loop runs over k = 0..n-1 in the same
+// order in every thread (warp-uniform k), so Fibonacci weights, amplitudes
+// and detunings are broadcast kernel-parameter reads; a flip that leaves the
+// basis only predicates its load off.  Four bits per round issue their
+// gathers before any of them is accumulated.  CT/RT are 32-bit when the
+// code has at most 32 bits and the basis fewer than 2^31 rows, which halves
+// the integer work of unranking and target arithmetic.
+
+template <typename S, int W>
+__device__ __forceinline__ void ld_row(const S *p, S (&v)[W]) {
+  constexpr int BYTES = W * (int)sizeof(S);
+  if constexpr (BYTES % 16 == 0) {
+    union { uint4 u[BYTES / 16]; S s[W]; } t;
+#pragma unroll
+    for (int i = 0; i < BYTES / 16; ++i) t.u[i] = reinterpret_cast<const uint4 *>(p)[i];
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = t.s[i];
+  } else if constexpr (BYTES == 8) {
+    union { uint2 u; S s[W]; } t;
+    t.u = *reinterpret_cast<const uint2 *>(p);
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = t.s[i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = p[i];
+  }
+}
+
+template <typename S, int W>
+__device__ __forceinline__ void st_row(S *p, const S (&v)[W]) {
+  constexpr int BYTES = W * (int)sizeof(S);
+  if constexpr (BYTES % 16 == 0) {
+    union { uint4 u[BYTES / 16]; S s[W]; } t;
+#pragma unroll
+    for (int i = 0; i < W; ++i) t.s[i] = v[i];
+#pragma unroll
+    for (int i = 0; i < BYTES / 16; ++i) reinterpret_cast<uint4 *>(p)[i] = t.u[i];
+  } else if constexpr (BYTES == 8) {
+    union { uint2 u; S s[W]; } t;
+#pragma unroll
+    for (int i = 0; i < W; ++i) t.s[i] = v[i];
+    *reinterpret_cast<uint2 *>(p) = t.u;
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) p[i] = v[i];
+  }
+}
+
+// Code of `row` (FULL / CHAIN / RING) in CT arithmetic.
+template <int LAY, typename CT, typename RT>
+__device__ __forceinline__ CT unrank_fib(const BasisDev &B, RT row) {
+  if constexpr (LAY == EL_LAYOUT_FULL) {
+    return (CT)row;
+  } else {
+    const int n = B.n;
+    RT r = row;
+    CT c = 0;
+    if constexpr (LAY == EL_LAYOUT_CHAIN) {
+      for (int k = n - 1; k >= 0; --k) {
+        const RT w = (RT)B.fib[k + 2];
+        if (r >= w) { c |= (CT)1 << k; r -= w; }
+      }
+      return c;
+    } else {
+      const RT split = (RT)B.fib[n + 1];
+      if (r < split) {
+        for (int k = n - 2; k >= 0; --k) {
+          const RT w = (RT)B.fib[k + 2];
+          if (r >= w) { c |= (CT)1 << k; r -= w; }
+        }
+        return c;
+      }
+      r -= split;
+      c = (CT)1 << (n - 1);
+      for (int k = n - 3; k >= 1; --k) {
+        const RT w = (RT)B.fib[k + 1];
+        if (r >= w) { c |= (CT)1 << k; r -= w; }
+      }
+      return c;
+    }
+  }
+}
+
+// Rank of an allowed ring code.
+template <typename CT, typename RT>
+__device__ __forceinline__ RT ring_rank_t(const BasisDev &B, CT c, int n) {
+  RT r = 0;
+  if ((c >> (n - 1)) & 1) {
+    r = (RT)B.fib[n + 1];
+    for (int k = 0; k < n - 1; ++k)
+      if ((c >> k) & 1) r += (RT)B.fib[k + 1];
+  } else {
+    for (int k = 0; k < n; ++k)
+      if ((c >> k) & 1) r += (RT)B.fib[k + 2];
+  }
+  return r;
+}
+
+template <typename S, bool C, int NV, int LAY, bool WANT, typename CT, typename RT>
+__global__ void __launch_bounds__(256) k_apply_row(BasisDev B, HamArgs<S> H, KArgs K) {
+  constexpr int W = NV * (C ? 2 : 1);
+  constexpr int U = 4;
+  const int n = B.n;
+  const CT full = (n >= (int)(8 * sizeof(CT))) ? ~(CT)0 : (((CT)1 << n) - 1);
+  const S *__restrict__ xp = (const S *)K.x;
+  double q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+  const RT dim = (RT)B.dim;
+  const RT stride = (RT)gridDim.x * blockDim.x;
+  for (RT row = (RT)blockIdx.x * blockDim.x + threadIdx.x; row < dim; row += stride) {
+    const CT code = unrank_fib<LAY, CT, RT>(B, row);
+    CT allowed = full;
+    if constexpr (LAY != EL_LAYOUT_FULL) {
+      CT occ = (code << 1) | (code >> 1);
+      if constexpr (LAY == EL_LAYOUT_RING) occ |= ((code >> (n - 1)) & 1) | ((code & 1) << (n - 1));
+      allowed = code | (~occ & full);
+    }
+    const bool top = (LAY == EL_LAYOUT_RING) && ((code >> (n - 1)) & 1);
+    S h[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) h[i] = S(0);
+    S dsum = S(0);
+    for (int k0 = 0; k0 < n; k0 += U) {
+      S xv[U][W];
+      S ar[U], ai[U];
+      bool ok[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u;
+        ok[u] = false;
+        ar[u] = S(0);
+        ai[u] = S(0);
+        if (k < n) {
+          const bool set = (code >> k) & 1;
+          if (set) dsum += H.delta[k];
+          ar[u] = H.up_re[k];
+          if constexpr (C) ai[u] = set ? H.up_im[k] : -H.up_im[k];
+          ok[u] = ((allowed >> k) & 1) && (ar[u] != S(0) || ai[u] != S(0));
+          if (ok[u]) {
+            RT tg;
+            if constexpr (LAY == EL_LAYOUT_FULL) {
+              tg = row ^ ((RT)1 << k);
+            } else if constexpr (LAY == EL_LAYOUT_CHAIN) {
+              const RT w = (RT)B.fib[k + 2];
+              tg = set ? row - w : row + w;
+            } else {
+              if (k == n - 1) {
+                tg = ring_rank_t<CT, RT>(B, code ^ ((CT)1 << k), n);
+              } else {
+                const RT w = (RT)(top ? B.fib[k + 1] : B.fib[k + 2]);
+                tg = set ? row - w : row + w;
+              }
+            }
+            ld_row<S, W>(xp + (size_t)tg * W, xv[u]);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (!ok[u]) continue;
+        if constexpr (C) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            h[2 * v] += ar[u] * xv[u][2 * v] - ai[u] * xv[u][2 * v + 1];
+            h[2 * v + 1] += ar[u] * xv[u][2 * v + 1] + ai[u] * xv[u][2 * v];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) h[v] += ar[u] * xv[u][v];
+        }
+      }
+    }
+    S xr[W];
+    ld_row<S, W>(xp + (size_t)row * W, xr);
+    if (!K.skip_diag) {
+      dsum += H.diagV[row];
+#pragma unroll
+      for (int i = 0; i < W; ++i) h[i] += dsum * xr[i];
+    }
+    S yv[W];
+    const S a = (S)K.a, b = (S)K.b;
+#pragma unroll
+    for (int i = 0; i < W; ++i) yv[i] = a * h[i] + b * xr[i];
+    if (K.z) {
+      S zv[W];
+      ld_row<S, W>((const S *)K.z + (size_t)row * W, zv);
+      const S c = (S)K.c;
+#pragma unroll
+      for (int i = 0; i < W; ++i) yv[i] += c * zv[i];
+    }
+    if (K.acc) {
+      S av[W];
+      S *ap = (S *)K.acc + (size_t)row * W;
+      ld_row<S, W>(ap, av);
+      const S wr = (S)K.w_re, wi = (S)K.w_im;
+      if constexpr (C) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          av[2 * v] += wr * yv[2 * v] - wi * yv[2 * v + 1];
+          av[2 * v + 1] += wr * yv[2 * v + 1] + wi * yv[2 * v];
+        }
+      } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) av[v] += wr * yv[v];
+      }
+      st_row<S, W>(ap, av);
+    }
+    if (K.y) st_row<S, W>((S *)K.y + (size_t)row * W, yv);
+    if constexpr (WANT) {
+      if constexpr (C) {
+        const double xre = xr[0], xim = xr[1], yre = yv[0], yim = yv[1];
+        q0 += xre * xre + xim * xim;
+        q1 += xre * yre + xim * yim;
+        q2 += xre * yim - xim * yre;
+        q3 += yre * yre + yim * yim;
+      } else {
+        const double xd = xr[0], yd = yv[0];
+        q0 += xd * xd;
+        q1 += xd * yd;
+        q3 += yd * yd;
+        if (K.probe) q2 += yd * (double)((const S *)K.probe)[row];
+      }
+    }
+  }
+  if constexpr (WANT) reduce4(K, q0, q1, q2, q3);
+}
+
 template <typename S>
 HamArgs<S> ham_args(const el_ham *h, const S *diagV) {
   HamArgs<S> A;
@@ -489,6 +718,77 @@ bool is_complex(int dtype) { return dtype == EL_C64 || dtype == EL_C128; }
 
 }  // namespace
 
+namespace {
+
+// The row kernel serves FULL/CHAIN/RING bases with 1..8 vectors per row
+// (dot products only for one vector) when every vector pointer is aligned for
+// its row-segment loads.
+bool row_kernel_ok(const el_ham *h, const ApplyArgs &A) {
+  const int lay = h->basis->layout;
+  if (lay != EL_LAYOUT_FULL && lay != EL_LAYOUT_CHAIN && lay != EL_LAYOUT_RING) return false;
+  if (A.nvec > 8) return false;
+  if (A.dots && A.nvec != 1) return false;
+  const size_t row_bytes = (size_t)A.nvec * el::dtype_size(A.dtype);
+  const size_t align = row_bytes >= 16 ? 16 : row_bytes;
+  for (const void *p : {A.x, (const void *)A.z, (const void *)A.y, (const void *)A.acc, A.probe})
+    if (p && ((uintptr_t)p % align) != 0) return false;
+  return true;
+}
+
+template <typename S, bool C, int NV, bool WANT, typename CT, typename RT>
+void launch_row_ct(el_ctx *ctx, int lay, int grid, const BasisDev &B, const HamArgs<S> &H, const KArgs &K) {
+  if (lay == EL_LAYOUT_FULL)
+    k_apply_row<S, C, NV, EL_LAYOUT_FULL, WANT, CT, RT><<<grid, 256, 0, ctx->stream>>>(B, H, K);
+  else if (lay == EL_LAYOUT_CHAIN)
+    k_apply_row<S, C, NV, EL_LAYOUT_CHAIN, WANT, CT, RT><<<grid, 256, 0, ctx->stream>>>(B, H, K);
+  else
+    k_apply_row<S, C, NV, EL_LAYOUT_RING, WANT, CT, RT><<<grid, 256, 0, ctx->stream>>>(B, H, K);
+}
+
+template <typename S, bool C, int NV, bool WANT>
+void launch_row_lay(el_ctx *ctx, int lay, int grid, const BasisDev &B, const HamArgs<S> &H, const KArgs &K) {
+  if (B.n <= 32 && B.dim < ((int64_t)1 << 31))
+    launch_row_ct<S, C, NV, WANT, uint32_t, int32_t>(ctx, lay, grid, B, H, K);
+  else
+    launch_row_ct<S, C, NV, WANT, uint64_t, int64_t>(ctx, lay, grid, B, H, K);
+}
+
+template <typename S, bool C>
+void launch_row_t(el_ctx *ctx, int lay, int nvec, bool want, int grid, const BasisDev &B,
+                  const HamArgs<S> &H, const KArgs &K) {
+  if (want) { launch_row_lay<S, C, 1, true>(ctx, lay, grid, B, H, K); return; }
+  switch (nvec) {
+    case 1: launch_row_lay<S, C, 1, false>(ctx, lay, grid, B, H, K); break;
+    case 2: launch_row_lay<S, C, 2, false>(ctx, lay, grid, B, H, K); break;
+    case 4: launch_row_lay<S, C, 4, false>(ctx, lay, grid, B, H, K); break;
+    default: launch_row_lay<S, C, 8, false>(ctx, lay, grid, B, H, K); break;
+  }
+}
+
+int launch_apply_row(el_ctx *ctx, el_ham *h, const ApplyArgs &A, const BasisDev &B, KArgs K) {
+  const int lay = h->basis->layout;
+  const int grid = el::grid_for(h->basis->dim, 256);
+  const bool want = K.want != 0;
+  if (want) {
+    K.nvec = 1;
+    K.lognv = 0;
+    int rc = el::ensure_partials(ctx, (size_t)grid * 4);
+    if (rc) return rc;
+    K.partials = ctx->d_partials;
+  }
+  switch (A.dtype) {
+    case EL_F32: launch_row_t<float, false>(ctx, lay, A.nvec, want, grid, B, ham_args<float>(h, h->d_diagV32), K); break;
+    case EL_F64: launch_row_t<double, false>(ctx, lay, A.nvec, want, grid, B, ham_args<double>(h, h->d_diagV64), K); break;
+    case EL_C64: launch_row_t<float, true>(ctx, lay, A.nvec, want, grid, B, ham_args<float>(h, h->d_diagV32), K); break;
+    case EL_C128: launch_row_t<double, true>(ctx, lay, A.nvec, want, grid, B, ham_args<double>(h, h->d_diagV64), K); break;
+    default: return el::fail(ctx, EL_EINVAL, "unknown dtype %d", A.dtype);
+  }
+  EL_LAUNCH_CHECK(ctx);
+  return EL_OK;
+}
+
+}  // namespace
+
 namespace el {
 
 int launch_apply(el_ctx *ctx, el_ham *h, const ApplyArgs &A) {
@@ -520,6 +820,7 @@ int launch_apply(el_ctx *ctx, el_ham *h, const ApplyArgs &A) {
     int rc = ham_diag32(ctx, h);
     if (rc) return rc;
   }
+  if (row_kernel_ok(h, A)) return launch_apply_row(ctx, h, A, B, K);
   switch (A.dtype) {
     case EL_F32:
       k_apply<float, false><<<grid, 256, 0, ctx->stream>>>(B, ham_args<float>(h, h->d_diagV32), K);

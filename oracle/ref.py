@@ -140,6 +140,46 @@ def hv(n, codes, omega, delta, pairs, x):
     return Y.reshape(x.shape) if vec else Y
 
 
+def sparse_h(n, codes, omega, delta, pairs):
+    """CSR H from the same channel list as hv (the reference assembles its CSR
+    in assemble.py:277-393 build_H_sparse; used here for the larger CPU
+    baseline samples, where a dense matrix does not fit)."""
+    import scipy.sparse as sp
+    n = int(n)
+    full = codes is None
+    codes = np.arange(1 << n, dtype=np.int64) if full else np.asarray(codes, np.int64)
+    dim = len(codes)
+    d = diagonal(n, codes, delta, pairs)
+    om = np.asarray(omega, complex)
+    cplx = np.any(om.imag != 0)
+    rows, cols, vals = [np.arange(dim)], [np.arange(dim)], [d.astype(complex if cplx else float)]
+    if not full:
+        order = np.argsort(codes)
+        sc = codes[order]
+    for i in range(n):
+        if om[i] == 0:
+            continue
+        mask = np.int64(1) << (n - 1 - i)
+        bit = (codes >> (n - 1 - i)) & 1
+        targets = codes ^ mask
+        if full:
+            loc = targets
+            ok = np.ones(dim, bool)
+        else:
+            pos = np.searchsorted(sc, targets)
+            ok = pos < dim
+            ok[ok] &= sc[pos[ok]] == targets[ok]
+            loc = np.zeros(dim, np.int64)
+            loc[ok] = order[pos[ok]]
+        amp = np.where(bit == 0, om[i] / 2.0, np.conj(om[i]) / 2.0)
+        src = np.flatnonzero(ok)
+        rows.append(loc[src])
+        cols.append(src)
+        vals.append(amp[src] if cplx else amp[src].real)
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                         shape=(dim, dim))
+
+
 def dense_h(n, codes, omega, delta, pairs):
     """Dense H by applying hv to unit vectors (small systems only)."""
     dim = (1 << n) if codes is None else len(codes)
@@ -257,7 +297,8 @@ def evolve_segments(n, codes, pairs, segments, psi0, t_grid):
             om, de = segment_drive(0.5 * (a + b), segments, n)
             key = (tuple(om), tuple(de))
             if key not in cache:
-                cache[key] = sp.csr_matrix(dense_h(n, codes, om, de, pairs))
+                cache[key] = (sp.csr_matrix(dense_h(n, codes, om, de, pairs)) if len(psi) <= 4096
+                              else sparse_h(n, codes, om, de, pairs))
             psi = expm_multiply((-1j * CONV * (b - a)) * cache[key], psi)
         out.append(psi.copy())
     return out

@@ -61,7 +61,7 @@ def test_hv_matches_oracle(ctx, name, n, edges, kind, k, dtype):
     h = Hamiltonian(ctx, b, om, de, pairs)
     codes = None if kind == "full" else oracle_codes(n, edges, kind, k)
     rng = np.random.default_rng(1)
-    for nvec in (1, 4, 32):
+    for nvec in (1, 2, 4, 8, 32):
         x = rng.normal(size=(b.dim, nvec))
         if cplx:
             x = x + 1j * rng.normal(size=(b.dim, nvec))
