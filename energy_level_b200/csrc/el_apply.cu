@@ -13,6 +13,8 @@
 // amplitude Omega/2 into |r>, conj(Omega)/2 into |g>).
 #include "el_internal.cuh"
 
+#include <algorithm>
+
 namespace {
 
 using el::fail;
@@ -380,6 +382,294 @@ __global__ void __launch_bounds__(256) k_apply_row(BasisDev B, HamArgs<S> H, KAr
         q1 += xd * yd;
         q3 += yd * yd;
         if (K.probe) q2 += yd * (double)((const S *)K.probe)[row];
+      }
+    }
+  }
+  if constexpr (WANT) reduce4(K, q0, q1, q2, q3);
+}
+
+// ------------------------------------------- chain tile kernel (CHAIN layout)
+// Rows of a nearest-neighbour chain sector that share the code bits >= L form
+// one contiguous block of F(L+2) rows (F(L+1) when bit L is set), ordered by
+// the low L bits exactly like the L-site chain itself.  A CTA takes one such
+// block (a tile) at a time:
+//   - flips of low bits k < L stay inside the tile: the tile of x is staged
+//     in shared memory and the partner is row +- F(k+2) of the same tile;
+//   - a flip of a high bit k >= L moves the whole tile by +- F(k+2) rows (the
+//     low part is unchanged), and whether it is allowed depends only on the
+//     tile's prefix (for k = L and bit L clear: on the tile's first F(L+1)
+//     rows), so it is a contiguous, coalesced read of x with one amplitude
+//     for the tile.
+// Low codes and their detuning sums are tabulated once per CTA in shared
+// memory.  Same fused epilogue as the row kernel.
+
+// Streaming (evict-first) row access for vectors that are touched once per
+// launch (y, z, acc), so that L2 keeps x, whose rows are re-read as flip
+// partners by other tiles.
+template <typename S, int W>
+__device__ __forceinline__ void ld_row_cs(const S *p, S (&v)[W]) {
+  constexpr int BYTES = W * (int)sizeof(S);
+  if constexpr (BYTES % 16 == 0) {
+    union { uint4 u[BYTES / 16]; S s[W]; } t;
+#pragma unroll
+    for (int i = 0; i < BYTES / 16; ++i) t.u[i] = __ldcs(reinterpret_cast<const uint4 *>(p) + i);
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = t.s[i];
+  } else if constexpr (BYTES == 8) {
+    union { uint2 u; S s[W]; } t;
+    t.u = __ldcs(reinterpret_cast<const uint2 *>(p));
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = t.s[i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = __ldcs(p + i);
+  }
+}
+
+template <typename S, int W>
+__device__ __forceinline__ void st_row_cs(S *p, const S (&v)[W]) {
+  constexpr int BYTES = W * (int)sizeof(S);
+  if constexpr (BYTES % 16 == 0) {
+    union { uint4 u[BYTES / 16]; S s[W]; } t;
+#pragma unroll
+    for (int i = 0; i < W; ++i) t.s[i] = v[i];
+#pragma unroll
+    for (int i = 0; i < BYTES / 16; ++i) __stcs(reinterpret_cast<uint4 *>(p) + i, t.u[i]);
+  } else if constexpr (BYTES == 8) {
+    union { uint2 u; S s[W]; } t;
+#pragma unroll
+    for (int i = 0; i < W; ++i) t.s[i] = v[i];
+    __stcs(reinterpret_cast<uint2 *>(p), t.u);
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) __stcs(p + i, v[i]);
+  }
+}
+
+// Shared tile of x: rows of more than 16 bytes are stored chunk-major
+// ([16-byte chunk][row]) so that the 16-byte loads of a warp's 32 rows hit
+// 32 consecutive chunks instead of a 4- or 8-way bank conflict.
+template <typename S, int W>
+__device__ __forceinline__ void tile_ld(const S *xt, int ts, int row, S (&v)[W]) {
+  constexpr int BYTES = W * (int)sizeof(S);
+  if constexpr (BYTES > 16 && BYTES % 16 == 0) {
+    union { uint4 u[BYTES / 16]; S s[W]; } t;
+#pragma unroll
+    for (int i = 0; i < BYTES / 16; ++i) t.u[i] = reinterpret_cast<const uint4 *>(xt)[(size_t)i * ts + row];
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = t.s[i];
+  } else {
+    ld_row<S, W>(xt + (size_t)row * W, v);
+  }
+}
+
+struct TileFlip {
+  int64_t off;   // row offset of the partner
+  int32_t len;   // rows [0, len) of the tile have this flip
+  int32_t k;     // bit
+};
+
+template <typename S, bool C, int NV>
+__device__ __forceinline__ void acc_flip(S (&h)[NV * (C ? 2 : 1)], S are, S aim,
+                                         const S (&xv)[NV * (C ? 2 : 1)]) {
+  if constexpr (C) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      h[2 * v] += are * xv[2 * v] - aim * xv[2 * v + 1];
+      h[2 * v + 1] += are * xv[2 * v + 1] + aim * xv[2 * v];
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) h[v] += are * xv[v];
+  }
+}
+
+template <typename S, bool C, int NV, bool WANT>
+__global__ void __launch_bounds__(256) k_apply_chain_tile(BasisDev B, HamArgs<S> H, KArgs K, int L,
+                                                          int64_t ntiles) {
+  constexpr int W = NV * (C ? 2 : 1);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = B.n;
+  const int TS = (int)B.fib[L + 2];                       // rows of a full tile
+  // [TS][W] tile of x, then the S-typed table, then the 4-byte table, so
+  // every array starts on a boundary of its element size
+  S *xt = reinterpret_cast<S *>(smem_raw);
+  S *ld = xt + (size_t)TS * W;                            // low detuning sums
+  uint32_t *lc = reinterpret_cast<uint32_t *>(ld + TS);   // low codes
+  __shared__ TileFlip hf[EL_MAX_SITES];
+  __shared__ S hf_re[EL_MAX_SITES], hf_im[EL_MAX_SITES];
+  __shared__ int nhf;
+  __shared__ int64_t t_base;
+  __shared__ int t_size;
+  __shared__ int t_bl;       // bit L of the tile's prefix
+  __shared__ S t_delta;      // detuning sum of the prefix bits
+  // low codes of the L-site chain in ascending order, and their detunings
+  for (int i = threadIdx.x; i < TS; i += blockDim.x) {
+    uint32_t c = 0;
+    int64_t r = i;
+    for (int k = L - 1; k >= 0; --k) {
+      const int64_t w = (int64_t)B.fib[k + 2];
+      if (r >= w) { c |= 1u << k; r -= w; }
+    }
+    lc[i] = c;
+    S d = S(0);
+    for (int k = 0; k < L; ++k)
+      if ((c >> k) & 1u) d += H.delta[k];
+    ld[i] = d;
+  }
+  const S *__restrict__ xp = (const S *)K.x;
+  double q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    __syncthreads();   // tables ready; previous tile done with xt / hf
+    if (threadIdx.x == 0) {
+      // prefix of tile t: the (n-L)-site chain code of rank t
+      uint64_t p = 0;
+      int64_t r = t;
+      for (int j = n - L - 1; j >= 0; --j) {
+        const int64_t w = (int64_t)B.fib[j + 2];
+        if (r >= w) { p |= 1ULL << j; r -= w; }
+      }
+      int64_t base = 0;
+      S dp = S(0);
+      for (int j = 0; j < n - L; ++j)
+        if ((p >> j) & 1ULL) { base += (int64_t)B.fib[L + j + 2]; dp += H.delta[L + j]; }
+      const int bl = (int)(p & 1ULL);
+      const int size = bl ? (int)B.fib[L + 1] : TS;
+      int cnt = 0;
+      for (int j = 0; j < n - L; ++j) {
+        const int k = L + j;
+        const S are = H.up_re[k];
+        const bool set = (p >> j) & 1ULL;
+        const S aim = C ? (set ? H.up_im[k] : -H.up_im[k]) : S(0);
+        if (are == S(0) && aim == S(0)) continue;
+        const int64_t w = (int64_t)B.fib[k + 2];
+        TileFlip f;
+        f.k = k;
+        if (set) {
+          f.off = -w;
+          f.len = size;
+        } else {
+          if (j + 1 < n - L && ((p >> (j + 1)) & 1ULL)) continue;
+          if (j >= 1 && ((p >> (j - 1)) & 1ULL)) continue;
+          f.off = w;
+          f.len = (j == 0) ? (int)B.fib[L + 1] : size;   // k = L needs low bit L-1 clear
+        }
+        hf[cnt] = f;
+        hf_re[cnt] = are;
+        hf_im[cnt] = aim;
+        ++cnt;
+      }
+      nhf = cnt;
+      t_base = base;
+      t_size = size;
+      t_bl = bl;
+      t_delta = dp;
+    }
+    __syncthreads();
+    const int64_t base = t_base;
+    const int size = t_size;
+    const int bl = t_bl;
+    const int nh = nhf;
+    // stage the tile of x (16-byte chunks when the row segment allows it)
+    {
+      constexpr int RB = W * (int)sizeof(S);
+      if constexpr (RB > 16 && RB % 16 == 0) {
+        constexpr int NC = RB / 16;
+        const uint4 *src = reinterpret_cast<const uint4 *>(xp + (size_t)base * W);
+        uint4 *dst = reinterpret_cast<uint4 *>(xt);
+        const int nch = size * NC;
+        for (int g = threadIdx.x; g < nch; g += blockDim.x) dst[(size_t)(g % NC) * TS + g / NC] = src[g];
+      } else if constexpr (RB % 16 == 0) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(xp + (size_t)base * W);
+        uint4 *dst = reinterpret_cast<uint4 *>(xt);
+        const int nch = size * (RB / 16);
+        for (int i = threadIdx.x; i < nch; i += blockDim.x) dst[i] = src[i];
+      } else {
+        const S *src = xp + (size_t)base * W;
+        for (int i = threadIdx.x; i < size * W; i += blockDim.x) xt[i] = src[i];
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < size; i += blockDim.x) {
+      const uint32_t c = lc[i];
+      S h[W];
+#pragma unroll
+      for (int q = 0; q < W; ++q) h[q] = S(0);
+      // low flips, partners in shared memory
+      for (int k = 0; k < L; ++k) {
+        const bool set = (c >> k) & 1u;
+        const bool up = (k + 1 < L) ? ((c >> (k + 1)) & 1u) : (bl != 0);
+        const bool dn = (k >= 1) && ((c >> (k - 1)) & 1u);
+        if (!set && (up || dn)) continue;
+        const S are = H.up_re[k];
+        const S aim = C ? (set ? H.up_im[k] : -H.up_im[k]) : S(0);
+        const int w = (int)B.fib[k + 2];
+        const int pi = set ? i - w : i + w;
+        S xv[W];
+        tile_ld<S, W>(xt, TS, pi, xv);
+        acc_flip<S, C, NV>(h, are, aim, xv);
+      }
+      // high flips: contiguous partner rows in global memory, two in flight
+      for (int f = 0; f < nh; f += 2) {
+        S xa[W], xb[W];
+        const bool oa = i < hf[f].len;
+        const bool ob = (f + 1 < nh) && (i < hf[f + 1].len);
+        if (oa) ld_row<S, W>(xp + (size_t)(base + i + hf[f].off) * W, xa);
+        if (ob) ld_row<S, W>(xp + (size_t)(base + i + hf[f + 1].off) * W, xb);
+        if (oa) acc_flip<S, C, NV>(h, hf_re[f], hf_im[f], xa);
+        if (ob) acc_flip<S, C, NV>(h, hf_re[f + 1], hf_im[f + 1], xb);
+      }
+      const int64_t row = base + i;
+      S xr[W];
+      tile_ld<S, W>(xt, TS, i, xr);
+      if (!K.skip_diag) {
+        const S dsum = H.diagV[row] + t_delta + ld[i];
+#pragma unroll
+        for (int q = 0; q < W; ++q) h[q] += dsum * xr[q];
+      }
+      S yv[W];
+      const S a = (S)K.a, b = (S)K.b;
+#pragma unroll
+      for (int q = 0; q < W; ++q) yv[q] = a * h[q] + b * xr[q];
+      if (K.z) {
+        S zv[W];
+        ld_row_cs<S, W>((const S *)K.z + (size_t)row * W, zv);
+        const S cc = (S)K.c;
+#pragma unroll
+        for (int q = 0; q < W; ++q) yv[q] += cc * zv[q];
+      }
+      if (K.acc) {
+        S av[W];
+        S *ap = (S *)K.acc + (size_t)row * W;
+        ld_row_cs<S, W>(ap, av);
+        const S wr = (S)K.w_re, wi = (S)K.w_im;
+        if constexpr (C) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            av[2 * v] += wr * yv[2 * v] - wi * yv[2 * v + 1];
+            av[2 * v + 1] += wr * yv[2 * v + 1] + wi * yv[2 * v];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) av[v] += wr * yv[v];
+        }
+        st_row_cs<S, W>(ap, av);
+      }
+      if (K.y) st_row_cs<S, W>((S *)K.y + (size_t)row * W, yv);
+      if constexpr (WANT) {
+        if constexpr (C) {
+          const double xre = xr[0], xim = xr[1], yre = yv[0], yim = yv[1];
+          q0 += xre * xre + xim * xim;
+          q1 += xre * yre + xim * yim;
+          q2 += xre * yim - xim * yre;
+          q3 += yre * yre + yim * yim;
+        } else {
+          const double xd = xr[0], yd = yv[0];
+          q0 += xd * xd;
+          q1 += xd * yd;
+          q3 += yd * yd;
+          if (K.probe) q2 += yd * (double)((const S *)K.probe)[row];
+        }
       }
     }
   }
@@ -765,6 +1055,46 @@ void launch_row_t(el_ctx *ctx, int lay, int nvec, bool want, int grid, const Bas
   }
 }
 
+// Tile bits L for the chain tile kernel: the largest L whose tile (rows x
+// row bytes, plus 4 + sizeof(S) bytes of tables per row) stays within 40 KB,
+// leaving at least 4 prefix bits; 0 if the chain is too short to tile.
+int chain_tile_bits(int n, int row_bytes, int scalar_bytes) {
+  uint64_t f[70];
+  f[0] = 0; f[1] = 1;
+  for (int i = 2; i < 70; ++i) f[i] = f[i - 1] + f[i - 2];
+  int best = 0;
+  for (int L = 4; L + 4 <= n && L + 2 < 70; ++L)
+    if (f[L + 2] * (uint64_t)(row_bytes + 4 + scalar_bytes) <= 40960) best = L;
+  return best;
+}
+
+template <typename S, bool C, int NV, bool WANT>
+int launch_chain_tile_t(el_ctx *ctx, int L, int64_t ntiles, const BasisDev &B, const HamArgs<S> &H,
+                        const KArgs &K) {
+  constexpr int W = NV * (C ? 2 : 1);
+  const size_t ts = (size_t)B.fib[L + 2];
+  const size_t smem = ts * W * sizeof(S) + ts * 4 + ts * sizeof(S) + 16;
+  cudaFuncSetAttribute(k_apply_chain_tile<S, C, NV, WANT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sms * 8);
+  k_apply_chain_tile<S, C, NV, WANT><<<grid, 256, smem, ctx->stream>>>(B, H, K, L, ntiles);
+  return EL_OK;
+}
+
+template <typename S, bool C>
+int launch_chain_tile_v(el_ctx *ctx, int nvec, bool want, int L, int64_t ntiles, const BasisDev &B,
+                        const HamArgs<S> &H, const KArgs &K) {
+  if (want) return launch_chain_tile_t<S, C, 1, true>(ctx, L, ntiles, B, H, K);
+  switch (nvec) {
+    case 1: return launch_chain_tile_t<S, C, 1, false>(ctx, L, ntiles, B, H, K);
+    case 2: return launch_chain_tile_t<S, C, 2, false>(ctx, L, ntiles, B, H, K);
+    case 4: return launch_chain_tile_t<S, C, 4, false>(ctx, L, ntiles, B, H, K);
+    default: return launch_chain_tile_t<S, C, 8, false>(ctx, L, ntiles, B, H, K);
+  }
+}
+
 int launch_apply_row(el_ctx *ctx, el_ham *h, const ApplyArgs &A, const BasisDev &B, KArgs K) {
   const int lay = h->basis->layout;
   const int grid = el::grid_for(h->basis->dim, 256);
@@ -772,9 +1102,28 @@ int launch_apply_row(el_ctx *ctx, el_ham *h, const ApplyArgs &A, const BasisDev 
   if (want) {
     K.nvec = 1;
     K.lognv = 0;
-    int rc = el::ensure_partials(ctx, (size_t)grid * 4);
+    // partial sums for the row grid or the tile grid (at most 8 CTAs per SM)
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    int rc = el::ensure_partials(ctx, (size_t)std::max(grid, 8 * sms) * 4);
     if (rc) return rc;
     K.partials = ctx->d_partials;
+  }
+  if (lay == EL_LAYOUT_CHAIN) {
+    const int ss = (A.dtype == EL_F32 || A.dtype == EL_C64) ? 4 : 8;
+    const int L = chain_tile_bits(h->n, (int)A.nvec * el::dtype_size(A.dtype), ss);
+    if (L > 0) {
+      const int64_t ntiles = (int64_t)B.fib[h->n - L + 2];
+      switch (A.dtype) {
+        case EL_F32: launch_chain_tile_v<float, false>(ctx, A.nvec, want, L, ntiles, B, ham_args<float>(h, h->d_diagV32), K); break;
+        case EL_F64: launch_chain_tile_v<double, false>(ctx, A.nvec, want, L, ntiles, B, ham_args<double>(h, h->d_diagV64), K); break;
+        case EL_C64: launch_chain_tile_v<float, true>(ctx, A.nvec, want, L, ntiles, B, ham_args<float>(h, h->d_diagV32), K); break;
+        case EL_C128: launch_chain_tile_v<double, true>(ctx, A.nvec, want, L, ntiles, B, ham_args<double>(h, h->d_diagV64), K); break;
+        default: return el::fail(ctx, EL_EINVAL, "unknown dtype %d", A.dtype);
+      }
+      EL_LAUNCH_CHECK(ctx);
+      return EL_OK;
+    }
   }
   switch (A.dtype) {
     case EL_F32: launch_row_t<float, false>(ctx, lay, A.nvec, want, grid, B, ham_args<float>(h, h->d_diagV32), K); break;
