@@ -61,15 +61,38 @@ __device__ double block_sum(double v, double *red) {
   return s;
 }
 
-// Sturm count of eigenvalues of T (a[0..m-1], b[0..m-2]) below x.
+// Characteristic polynomials chi_k(x) = det(x I - T_k) of the leading k x k
+// blocks of T (a[0..m-1], b[0..m-2]):
+//   chi_0 = 1, chi_1 = x - a_0, chi_k = (x - a_{k-1}) chi_{k-1} - b_{k-2}^2 chi_{k-2}.
+// The recurrence needs no division; the pair (chi_k, chi_{k-1}) is rescaled by
+// a power of two whenever it grows large, which keeps signs and ratios exact.
+__device__ __forceinline__ void rescale2(double &p, double &q) {
+  const double ap = fabs(p);
+  if (ap > 0x1p+400 || (ap < 0x1p-400 && ap > 0.0 && fabs(q) < 0x1p-400)) {
+    const int e = ilogb(ap);
+    p = scalbn(p, -e);
+    q = scalbn(q, -e);
+  }
+}
+
+// Number of eigenvalues of T below x: the number of k in 1..m at which
+// chi_k(x) and chi_{k-1}(x) have the same sign (a zero counts as the sign
+// opposite to its predecessor).
 __device__ int sturm(const double *a, const double *b, int m, double x) {
   int cnt = 0;
-  double q = a[0] - x;
-  if (q < 0) ++cnt;
+  double pm = 1.0, p = x - a[0];
+  double sprev = 1.0;
+  double sp = (p == 0.0) ? -sprev : p;
+  if (sp > 0) ++cnt;
+  sprev = sp;
   for (int i = 1; i < m; ++i) {
-    if (fabs(q) < 1e-300) q = (q < 0 ? -1e-300 : 1e-300);
-    q = a[i] - x - b[i - 1] * b[i - 1] / q;
-    if (q < 0) ++cnt;
+    const double pn = fma(x - a[i], p, -(b[i - 1] * b[i - 1]) * pm);
+    pm = p;
+    p = pn;
+    rescale2(p, pm);
+    const double s = (p == 0.0) ? -sprev : p;
+    if ((s > 0) == (sprev > 0)) ++cnt;
+    sprev = s;
   }
   return cnt;
 }
@@ -117,6 +140,7 @@ __device__ double last_component(const double *a, const double *b, int m, double
     }
   }
   d[m - 1] = fabs(cd) < eps ? (cd < 0 ? -eps : eps) : cd;
+  for (int i = 0; i < m; ++i) d[i] = 1.0 / d[i];            // reciprocal pivots
   for (int i = 0; i < m; ++i) x[i] = 1.0 + 0.01 * sin(1.0 + i);
   for (int it = 0; it < 3; ++it) {
     for (int i = 0; i < m - 1; ++i) {
@@ -127,13 +151,14 @@ __device__ double last_component(const double *a, const double *b, int m, double
       double s = x[i];
       if (i + 1 < m) s -= u1[i] * x[i + 1];
       if (i + 2 < m) s -= u2[i] * x[i + 2];
-      x[i] = s / d[i];
+      x[i] = s * d[i];
     }
     double nrm = 0.0;
     for (int i = 0; i < m; ++i) nrm += x[i] * x[i];
     nrm = sqrt(nrm);
     if (!(nrm > 0) || !isfinite(nrm)) return 1.0;
-    for (int i = 0; i < m; ++i) x[i] /= nrm;
+    const double inv = 1.0 / nrm;
+    for (int i = 0; i < m; ++i) x[i] *= inv;
   }
   return fabs(x[m - 1]);
 }
@@ -200,8 +225,9 @@ __global__ void __launch_bounds__(NT) k_lanczos_batch(const BatchArgs A) {
   __shared__ double red[NT / 32];
   __shared__ double al[MAXIT], be[MAXIT];
   __shared__ double wcur[MAXIT + 2], wprev[MAXIT + 2];
-  __shared__ double work[8 * MAXIT + 8];   // [0, MAXIT): omega row; [2 MAXIT, 8 MAXIT): inverse iteration
-  __shared__ int s_idx, s_flag, s_done, s_force;
+  __shared__ double work[8 * MAXIT + 8];   // [0, MAXIT): omega row; [2 MAXIT, 8 MAXIT): projection coefficients, then inverse iteration
+  __shared__ int s_idx, s_flag, s_done, s_force, s_trig, nsel;
+  __shared__ short sel[MAXIT + 2];         // vectors of the current reorthogonalisation
   __shared__ double s_th[2], s_res[2];
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -269,35 +295,90 @@ __global__ void __launch_bounds__(NT) k_lanczos_batch(const BatchArgs A) {
       double b2 = block_sum<NT>(pn, red);
       anorm = fmax(anorm, fabs(alpha) + beta);
       double bnext = sqrt(fmax(b2, 0.0));
-      // partial reorthogonalisation: omega recurrence on thread 0
-      if (tid == 0) {
-        al[j] = alpha;
-        int flag = s_force;
-        s_force = 0;
+      // partial reorthogonalisation (Simon): one warp advances the omega
+      // recurrence over k; when max |omega| exceeds sqrt(eps) the new vector
+      // is orthogonalised against the v_k with |omega_k| >= eps^(3/4) (plus
+      // v_{j-1}, v_j), and the next vector against the same set
+      if (tid < 32) {
+        const int forced = s_force;
+        double wmax = 0.0;
         if (j > 0 && bnext > 0) {
-          double wmax = 0.0;
-          for (int k = 0; k < j; ++k) {
-            double t = be[k] * wcur[k + 1] + (al[k] - alpha) * wcur[k] - beta * (k < j - 0 ? wprev[k] : 0.0);
+          for (int k = tid; k < j; k += 32) {
+            double t = be[k] * wcur[k + 1] + (al[k] - alpha) * wcur[k] - beta * wprev[k];
             if (k > 0) t += be[k - 1] * wcur[k - 1];
             t /= bnext;
             t += (t >= 0 ? 1.0 : -1.0) * A.eps * anorm / bnext;
             work[k] = t;
             wmax = fmax(wmax, fabs(t));
           }
-          if (wmax > sqrt(A.eps)) flag = 1;
+          for (int o = 16; o > 0; o >>= 1) wmax = fmax(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
         }
-        s_flag = flag;
+        const bool trig = (j > 0) && (bnext > 0) && (wmax > sqrt(A.eps)) && !forced;
+        __syncwarp();
+        if (trig) {
+          const double eta = pow(A.eps, 0.75);
+          int cnt = 0;
+          for (int k0 = 0; k0 <= j; k0 += 32) {
+            const int k = k0 + tid;
+            const bool pick = (k <= j) && (k >= j - 1 || fabs(work[k]) >= eta);
+            const unsigned bal = __ballot_sync(0xffffffffu, pick);
+            if (pick) sel[cnt + __popc(bal & ((1u << tid) - 1u))] = (short)k;
+            cnt += __popc(bal);
+          }
+          if (tid == 0) nsel = cnt;
+        } else if (forced && tid == 0) {
+          sel[nsel++] = (short)j;   // previous set (which holds j-1) plus the new v_j
+        }
+        if (tid == 0) {
+          al[j] = alpha;
+          s_force = 0;
+          s_flag = (trig || forced) ? 1 : 0;
+          s_trig = trig ? 1 : 0;
+        }
       }
       __syncthreads();
       if (s_flag && j > 0) {
+        // classical Gram-Schmidt, twice: each warp forms the dot products of
+        // its share of v_0..v_j with w (FP64, fixed order), then every thread
+        // subtracts all projections from its rows
+        double *cf = work + 2 * MAXIT;
         for (int pass = 0; pass < 2; ++pass) {
-          for (int k = 0; k <= j; ++k) {
-            const T *vk = Vb + (size_t)k * A.dim_max;
-            double pc = 0.0;
-            for (int64_t r = tid; r < dim; r += NT) pc += (double)vk[r] * (double)W[r];
-            const double cc = block_sum<NT>(pc, red);
-            for (int64_t r = tid; r < dim; r += NT) W[r] = (T)((double)W[r] - cc * (double)vk[r]);
+          const int lane = tid & 31, warp = tid >> 5;
+          const int ns = nsel;
+          for (int q = warp; q < ns; q += NT / 32) {
+            const T *vk = Vb + (size_t)sel[q] * A.dim_max;
+            double pc0 = 0.0, pc1 = 0.0, pc2 = 0.0, pc3 = 0.0;
+            int64_t r = lane;
+            for (; r + 96 < dim; r += 128) {
+              pc0 += (double)vk[r] * (double)W[r];
+              pc1 += (double)vk[r + 32] * (double)W[r + 32];
+              pc2 += (double)vk[r + 64] * (double)W[r + 64];
+              pc3 += (double)vk[r + 96] * (double)W[r + 96];
+            }
+            for (; r < dim; r += 32) pc0 += (double)vk[r] * (double)W[r];
+            double pc = (pc0 + pc1) + (pc2 + pc3);
+            for (int o = 16; o > 0; o >>= 1) pc += __shfl_xor_sync(0xffffffffu, pc, o);
+            if (lane == 0) cf[q] = pc;
           }
+          __syncthreads();
+          for (int64_t r = tid; r < dim; r += NT) {
+            const T *col = Vb + r;
+            double w0 = (double)W[r], w1 = 0.0, w2 = 0.0, w3 = 0.0;
+            int q = 0;
+            for (; q + 4 <= ns; q += 4) {
+              const double v0 = (double)col[(size_t)sel[q] * A.dim_max];
+              const double v1 = (double)col[(size_t)sel[q + 1] * A.dim_max];
+              const double v2 = (double)col[(size_t)sel[q + 2] * A.dim_max];
+              const double v3 = (double)col[(size_t)sel[q + 3] * A.dim_max];
+              w0 -= cf[q] * v0;
+              w1 -= cf[q + 1] * v1;
+              w2 -= cf[q + 2] * v2;
+              w3 -= cf[q + 3] * v3;
+            }
+            for (; q < ns; ++q) w0 -= cf[q] * (double)col[(size_t)sel[q] * A.dim_max];
+            W[r] = (T)((w0 + w1) + (w2 + w3));
+          }
+          __syncthreads();
         }
         double pn2 = 0.0;
         for (int64_t r = tid; r < dim; r += NT) pn2 += (double)W[r] * (double)W[r];
@@ -312,13 +393,11 @@ __global__ void __launch_bounds__(NT) k_lanczos_batch(const BatchArgs A) {
         } else {
           for (int k = 0; k <= j - 1; ++k) wprev[k] = wcur[k];
           wprev[j] = wcur[j];
-          if (s_flag) {
-            for (int k = 0; k <= j; ++k) wcur[k] = A.eps;
-            s_force = 1;   // Simon: also orthogonalise the next vector
-          } else {
-            for (int k = 0; k < j; ++k) wcur[k] = work[k];
-            wcur[j] = A.eps * sqrt((double)dim);
-          }
+          for (int k = 0; k < j; ++k) wcur[k] = work[k];
+          wcur[j] = A.eps * sqrt((double)dim);
+          if (s_flag)
+            for (int q = 0; q < nsel; ++q) wcur[sel[q]] = A.eps;
+          if (s_trig) s_force = 1;   // the next vector is orthogonalised against the same set
           wcur[j + 1] = 1.0;
         }
         be[j] = bnext;
