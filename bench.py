@@ -216,7 +216,7 @@ def run_native(args):
     stream = torch.cuda.current_stream()
 
     def solve(dtype="float32"):
-        lo, hi = solvers.bounds(ham, max_iter=300, tol=1e-12, seed=0)
+        lo, hi = solvers.bounds(ham, max_iter=300, tol=1e-10, seed=0)
         c, r = solvers.kpm_scale(lo, hi)
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)

@@ -295,7 +295,8 @@ extern "C" int el_lanczos_ground(el_ctx *ctx, el_ham *h, int dtype, const void *
       rc = el::launch_axpby(ctx, dtype, dim, -alpha, 0, Vj(j), 1, 0, w, d_sc + 8);
       if (rc) return rc;
       // reorthogonalisation decision
-      bool do_reorth = (reorth == 2) || force_next;
+      const bool forced = force_next;
+      bool do_reorth = (reorth == 2) || forced;
       double anorm = 0.0;
       for (size_t q = 0; q < al.size(); ++q) anorm = std::max(anorm, std::fabs(al[q]));
       for (size_t q = 0; q < be.size(); ++q) anorm = std::max(anorm, std::fabs(be[q]));
@@ -336,7 +337,7 @@ extern "C" int el_lanczos_ground(el_ctx *ctx, el_ham *h, int dtype, const void *
         if (reorth == 1) {
           for (int k = 0; k <= j; ++k) wnext[k] = eps;
           wnext[j + 1] = 1.0;
-          force_next = true;
+          force_next = !forced;   // Simon: the vector after a triggered step too, once
         }
       }
       if (reorth == 1) {
