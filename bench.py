@@ -200,7 +200,7 @@ def run_native(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from energy_level_b200.build import build
     build()
     from energy_level_b200 import kpm as bkpm, solvers
@@ -212,7 +212,8 @@ def run_native(args):
     ctx = Context(local)
     basis = Basis(ctx, n, "full")
     ham = Hamiltonian(ctx, basis, cfg["Om"], cfg["delta"], pairs)
-    seed = cfg["probe_seed"] + 1000 * rank          # replicas draw distinct probes
+    from energy_level_b200 import replicas
+    seed = replicas.replica_seed(cfg["probe_seed"], rank)   # replicas draw distinct probes
     stream = torch.cuda.current_stream()
 
     def solve(dtype="float32"):
@@ -253,11 +254,8 @@ def run_native(args):
     launches = ctx.launches - launches0
     elapsed = t0.elapsed_time(t1) / 1e3
     kpm_s = sum(a.elapsed_time(b) for a, b in kpm_events) / 1e3
-    if dist:
-        tt = torch.tensor([elapsed, kpm_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed, kpm_s = float(tt[0]), float(tt[1])
-    value = world * args.steps / elapsed
+    elapsed, kpm_s = replicas.max_over_ranks([elapsed, kpm_s], dist, device="cuda")
+    value = replicas.aggregate_rate(args.steps, world, elapsed)
 
     # roofline of the dominant kernel: one tiled pass = one Chebyshev step
     passes = (NUM + 1) // 2 + 1                    # prologue + M passes per probe block
@@ -359,7 +357,7 @@ class Harness:
         if self.world > 1:
             import datetime
             import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
             self.dist = dist
         from energy_level_b200.build import build
         build()
@@ -391,11 +389,8 @@ class Harness:
         return self.max_over_ranks(a.elapsed_time(b) / 1e3), self.ctx.launches - l0, clk.summary()
 
     def max_over_ranks(self, v):
-        if not self.dist:
-            return float(v)
-        t = self.torch.tensor([float(v)], device="cuda", dtype=self.torch.float64)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t[0])
+        from energy_level_b200 import replicas
+        return replicas.max_over_ranks([v], self.dist, device="cuda")[0]
 
     def close(self):
         if self.dist:
