@@ -307,6 +307,11 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
         __syncthreads();
         if (tid == 0) { tile_store<KIND>(A, &mapP, tile, g, S2); bulk_commit(); }
         // p_{m+1} = d2 t_m + (2/r) X_G t_m - t_{m-1}  (t_m in hx[], t_{m-1} in own[])
+        // the diagonal of this thread's rows, loaded before the gathers so
+        // that its latency hides behind them
+        T dv[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) dv[j] = d2[row_of<KIND, C>(A.a, tile, tid + NT * j)];
         U h2[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) h2[j] = z8(U{});
@@ -318,8 +323,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
 #pragma unroll
         for (int j = 0; j < R; ++j) {
           const int l = tid + NT * j;
-          const uint32_t row = row_of<KIND, C>(A.a, tile, l);
-          S[l] = sub8(fma8(A.two_r, h2[j], scl8(d2[row], hx[j])), S[l]);   // S[l] = t_{m-1}
+          S[l] = sub8(fma8(A.two_r, h2[j], scl8(dv[j], hx[j])), S[l]);   // S[l] = t_{m-1}
         }
         fence_async_smem();
         __syncthreads();
