@@ -31,6 +31,7 @@ if ROOT not in sys.path:
 
 METRIC = "Sector H·v GB/s; solves/s & grads/s, chosen vs plain FP64 B200 at fixed error"
 NUM, NVEC, CHUNK = 1024, 32, 32
+DIRECT_SAMPLE = 16
 WORKLOAD = "kpm_dos_square25"
 
 
@@ -273,6 +274,20 @@ def run_native(args):
     err_mu = float(np.max(np.abs(mu - mu64)))
     err_dos = float(np.max(np.abs(rho - rho64)) / max(np.max(np.abs(rho64)), 1e-300))
 
+    # the reference algorithm on the GPU in FP64: direct three-term recurrence,
+    # one H.v per moment (kpm.py:26-75), row-parallel kernel; timed on
+    # DIRECT_SAMPLE moments and scaled linearly to NUM
+    lo_, hi_ = solvers.bounds(ham, max_iter=300, tol=1e-10, seed=0)
+    c_, r_ = solvers.kpm_scale(lo_, hi_)
+    evd0, evd1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    evd0.record(stream)
+    mu_direct = solvers.kpm_moments(ham, DIRECT_SAMPLE, NVEC, c_, r_, dtype="float64", chunk=CHUNK, seed=seed,
+                                    mode="direct", generic=True)
+    evd1.record(stream)
+    torch.cuda.synchronize()
+    direct_s = evd0.elapsed_time(evd1) / 1e3 * NUM / DIRECT_SAMPLE
+    err_direct = float(np.max(np.abs(mu_direct - mu64[:DIRECT_SAMPLE + 1])))
+
     # end to end through the public API with host inputs (pinned) each step
     e2e_value, h2d, d2h = None, None, None
     if rank == 0 or world > 1:
@@ -321,6 +336,11 @@ def run_native(args):
             "clocks": clk.summary(),
             "plain_fp64": {"solves_per_s": 1.0 / (fp64_s + (elapsed / args.steps - kpm_s / args.steps)),
                            "moments_ms": fp64_s * 1e3, "form": "FP64 vectors, same tiled recurrence"},
+            "plain_fp64_direct": {"solves_per_s": 1.0 / (direct_s + (elapsed / args.steps - kpm_s / args.steps)),
+                                  "moments_ms": direct_s * 1e3,
+                                  "form": "reference recurrence (one H.v per moment) in FP64 on the GPU, "
+                                          "%d moments timed, scaled to %d" % (DIRECT_SAMPLE, NUM),
+                                  "max_abs_moment_vs_doubling": err_direct},
             "error_vs_fp64": {"max_abs_moment": err_mu, "max_rel_dos": err_dos},
             "hv_gbs": achieved,
         }
