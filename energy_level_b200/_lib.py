@@ -66,6 +66,8 @@ PROTOTYPES = {
     "el_batch_destroy": (C.c_int, [_vp]),
     "el_cheb_step": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, _ip]),
     "el_observables": (C.c_int, [_vp, _vp, C.c_int, _vp, _dp, _dp]),
+    "el_lanczos_tridiag": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, C.c_int, _dp, _dp,
+                                     C.POINTER(C.c_int), _dp, _dp, C.POINTER(C.c_int)]),
     "el_observables_noalloc": (C.c_int, [_vp, _vp, C.c_int, _vp, _dp, _dp]),
     "el_adjoint_pulse": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _vp, _vp, _vp,
                                    C.c_double, _dp, _dp, _dp, _vp]),

@@ -6,7 +6,7 @@ and time evolution through TIME_BACKENDS -> runspec._ENGINE_TABLE
 (backends.py:48-110, 177-179; runspec.py:660-697).  This module declares the
 B200 backends in the same shapes:
 
-    EQ_BACKENDS   'b200-lanczos': ('gs',)   'b200-kpm': ('thermal', 'dos')
+    EQ_BACKENDS   'b200-lanczos': ('gs', 'spectrum')   'b200-kpm': ('thermal', 'dos')
     TIME_BACKENDS 'b200-cheb': TimeBackend(segments, projected, return_state)
 
 ``solve_equilibrium`` accepts the reference's ``system`` dict and keyword
@@ -41,7 +41,7 @@ class TimeBackend:
 
 
 EQ_BACKENDS = {
-    'b200-lanczos': ('gs',),
+    'b200-lanczos': ('gs', 'spectrum'),
     'b200-kpm': ('thermal', 'dos'),
 }
 
@@ -166,6 +166,9 @@ def solve_equilibrium(system, want='gs', *, backend='b200-lanczos', betas=None, 
         if return_state:
             out['vec'] = vec
         return out
+    if want == 'spectrum':
+        return _solve_spectrum(system, base, sector=sector, memory_budget_mb=memory_budget_mb,
+                               progress_arr=progress_arr, dtype=dtype, seed=seed)
     if want == 'thermal':
         betas = np.atleast_1d(np.asarray([1.0] if betas is None else betas, float))
         if betas.ndim != 1 or not len(betas) or not np.isfinite(betas).all() or np.any(betas <= 0):
@@ -180,6 +183,77 @@ def solve_equilibrium(system, want='gs', *, backend='b200-lanczos', betas=None, 
                               chunk=system.get('kpm_chunk', 32))
         return dict(base, energies=r['energies'], rho=r['rho'])
     raise ValueError('want 需为 gs/thermal/dos，实=%r' % want)
+
+
+def _solve_spectrum(system, base, *, sector, memory_budget_mb, progress_arr, dtype, seed):
+    """Source-state spectrum (eq_route.py:260-337 _solve_spectrum) on the GPU:
+    |0> is system['psi0'] (state grammar or vector) or the b200 Lanczos ground
+    state; phi from system['source'] (eq_route.py:160-257); spectrum.py's
+    source_spectrum with the device Lanczos."""
+    from . import model, solvers
+    from . import spectrum as spec
+    from .state import state_vector
+    n_sites = int(base['n_sites'])
+    opts = dict(system.get('spectrum') or {})
+    source = system.get('source')
+    if source is None and system.get('psi0') is not None:
+        source = {'kind': 'psi0'}
+    if source is None:
+        raise ValueError('want=spectrum 需要 system["source"] 或 system["psi0"]'
+                         '（vector/psi0/diagonal/sparse/full_sparse）')
+    plan = system.get('plan') or {}
+    constraint = None
+    if sector is not None:
+        constraint = {'kind': 'charge', 'k': int(sector)}
+        if np.any(np.asarray(system.get('Om') if system.get('Om') is not None else 0) != 0):
+            raise ValueError('固定 charge_sector 要求 Omega=0')
+    ctx, basis, ham, perm = model.build(system['calib'], system.get('Om'), system.get('delta'),
+                                        system.get('gamma'), system.get('terms'),
+                                        plan=plan if (plan.get('projected') and constraint is None) else None,
+                                        constraint=constraint, device=system.get('device', 'cuda'))
+    restricted = constraint is not None or plan.get('projected')
+    codes = basis.codes().cpu().numpy() if restricted else None
+    dim = basis.dim
+    psi0 = system.get('psi0')
+    E0 = float('nan')
+    if psi0 is not None and not (isinstance(psi0, str) and psi0 == 'ground') and not isinstance(psi0, dict):
+        if isinstance(psi0, np.ndarray) and psi0.ndim == 1 and psi0.size == dim and psi0.size != (1 << n_sites):
+            vec = np.asarray(psi0, complex)
+        else:
+            vec = state_vector(psi0, n_sites, codes)
+    else:
+        r = solvers.lanczos_ground(ham, dtype='complex128' if ham.complex_drive else 'float64', seed=seed,
+                                   max_iter=min(300, dim), tol=1e-12, nev=1, return_vec=True)
+        vec = r['vec'].cpu().numpy().astype(complex)
+        E0 = float(r['evals'][0])
+    if progress_arr is not None and float(progress_arr[1]) != 0:
+        raise RuntimeError('用户取消')
+    phi, info = spec.resolve_source(source, vec, n_sites, codes)
+    if progress_arr is not None:
+        progress_arr[0] = 0.35
+    out = spec.source_spectrum(
+        ham, phi, shift=E0 if np.isfinite(E0) else 0.0,
+        eta=float(opts.get('eta') or 0.05), n_krylov=int(opts.get('n_krylov') or 0) or None,
+        omega_min=opts.get('omega_min'), omega_max=opts.get('omega_max'),
+        n_omega=int(opts.get('n_omega') or 800), reortho=bool(opts.get('reortho', True)),
+        memory_budget_mb=memory_budget_mb if memory_budget_mb is not None else 512.0,
+        dtype=dtype if dtype in ('complex64', 'complex128') else None)
+    if progress_arr is not None:
+        progress_arr[0] = 1.0
+    errors = dict(out.pop('error_report') or {})
+    errors.update({'source_kind': info.get('kind'), 'sector': None if sector is None else int(sector),
+                   'dim_basis': dim})
+    for key, value in info.items():
+        if key not in ('kind', 'dim'):
+            errors.setdefault(key, value)
+    res = dict(base, E0=E0 if np.isfinite(E0) else None, gap=None,
+               evals=out['evals'], spectrum_weights=out['spectrum_weights'],
+               energies=out['omega'], spectral=out['spectral'],
+               source_norm=out['source_norm'], eta=out['eta'],
+               krylov=out['krylov'], error_report=errors)
+    if constraint is not None:
+        res.update(sector_idx=codes, dim_sub=dim)
+    return res
 
 
 def install_into(reference_backends, shim_module='b200_shim'):

@@ -430,3 +430,100 @@ extern "C" int el_lanczos_ground(el_ctx *ctx, el_ham *h, int dtype, const void *
   }
   return EL_OK;
 }
+
+// ------------------------------------------------------- source-state Lanczos
+// Lanczos tridiagonalisation of H from a given source state phi, as in
+// spectrum.py:34-103 (lanczos): q_0 = phi/|phi|, w = H q_j, alpha_j =
+// Re<q_j, w>, w -= alpha_j q_j + beta_{j-1} q_{j-1}; with reorth, w is
+// orthogonalised twice against all q_0..q_j (classical Gram-Schmidt: all
+// coefficients in one pass, then one update); beta_j = |w|; the run stops
+// when beta_j <= 1e-12 or the Krylov space is the whole basis.  beta_j is
+// stored only while another step follows (j + 1 < n_krylov), so betas has
+// n - 1 entries.  ortho_loss = |<q_0, q_last>| of the last vector formed.
+extern "C" int el_lanczos_tridiag(el_ctx *ctx, el_ham *h, int dtype, const void *phi, int n_krylov,
+                                  int reorth, double *alphas, double *betas, int *n_out,
+                                  double *norm2_out, double *ortho_loss, int *converged) {
+  if (!ctx || !h || !phi || !alphas || !betas || !n_out) return EL_EINVAL;
+  if (!el::dtype_size(dtype)) return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
+  if (h->complex_drive && !is_cplx(dtype)) return fail(ctx, EL_EINVAL, "complex Omega needs a complex dtype");
+  if (n_krylov < 1) return fail(ctx, EL_EINVAL, "n_krylov must be positive");
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int64_t dim = h->basis->dim;
+  const size_t vb = (size_t)dim * el::dtype_size(dtype);
+  const int k = (int)std::min<int64_t>(n_krylov, dim);
+  if (2 * (k + 1) + 64 > EL_SCALARS) return fail(ctx, EL_EINVAL, "n_krylov too large (<= %d)", EL_SCALARS / 2 - 40);
+  char *Vb = (char *)el::workspace(ctx, 3, (size_t)(reorth ? k + 1 : 3) * vb);
+  char *Wb = (char *)el::workspace(ctx, 4, vb);
+  if (!Vb || !Wb) return EL_ENOMEM;
+  void *w = Wb;
+  double *d_sc = ctx->d_scalars;
+  double *d_coef = ctx->d_scalars + 64;
+  // with reorth every q_j is kept; without, three slots rotate
+  auto Q = [&](int j) { return (void *)(Vb + (size_t)(reorth ? j : j % 3) * vb); };
+  int rc;
+  EL_CUDA_TRY(ctx, el::copy(ctx, Q(0), phi, vb, cudaMemcpyDeviceToDevice));
+  rc = el::launch_axpby(ctx, dtype, dim, 0, 0, nullptr, 1, 0, Q(0), d_sc + 8);
+  if (rc) return rc;
+  double n2;
+  rc = sync_read(ctx, d_sc + 8, 1, &n2);
+  if (rc) return rc;
+  if (!(n2 > 0) || !std::isfinite(n2)) return fail(ctx, EL_EINVAL, "source state has zero or non-finite norm");
+  rc = el::launch_axpby(ctx, dtype, dim, 0, 0, nullptr, 1.0 / std::sqrt(n2), 0, Q(0), nullptr);
+  if (rc) return rc;
+  double beta = 0.0;
+  int n = 0, nb = 0;
+  bool conv = false;
+  int last = 0;   // index of the last vector formed
+  for (int j = 0; j < k; ++j) {
+    if (el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
+    ApplyArgs A;
+    memset(&A, 0, sizeof A);
+    A.dtype = dtype; A.nvec = 1; A.x = Q(j); A.z = j ? Q(j - 1) : nullptr; A.y = w;
+    A.a = 1.0; A.c = -beta; A.dots = d_sc; A.want_dots = 2;
+    rc = el::launch_apply(ctx, h, A);
+    if (rc) return rc;
+    double dots[4];
+    rc = sync_read(ctx, d_sc, 4, dots);
+    if (rc) return rc;
+    const double alpha = dots[1];
+    rc = el::launch_axpby(ctx, dtype, dim, -alpha, 0, Q(j), 1, 0, w, reorth ? nullptr : d_sc + 8);
+    if (rc) return rc;
+    if (reorth) {
+      for (int pass = 0; pass < 2; ++pass) {
+        rc = el::launch_gemv_t(ctx, dtype, dim, j + 1, Vb, dim, w, d_coef);
+        if (rc) return rc;
+        rc = el::launch_gemv_n_sub(ctx, dtype, dim, j + 1, Vb, dim, d_coef, w);
+        if (rc) return rc;
+      }
+      rc = el::launch_axpby(ctx, dtype, dim, 0, 0, nullptr, 1, 0, w, d_sc + 8);
+      if (rc) return rc;
+    }
+    double w2;
+    rc = sync_read(ctx, d_sc + 8, 1, &w2);
+    if (rc) return rc;
+    beta = std::sqrt(std::max(w2, 0.0));
+    alphas[n++] = alpha;
+    if (beta <= 1e-12 || n >= dim) { conv = true; break; }
+    if (j + 1 < k) betas[nb++] = beta;
+    rc = el::launch_axpby(ctx, dtype, dim, 1.0 / beta, 0, w, 0, 0, Q(j + 1), nullptr);
+    if (rc) return rc;
+    last = j + 1;
+    if (j + 1 == k && !reorth) break;
+  }
+  if (ortho_loss) {
+    double ol = 0.0;
+    if (reorth) {
+      rc = el::launch_gemv_t(ctx, dtype, dim, 1, Q(last), dim, Q(0), d_sc);
+      if (rc) return rc;
+      double ov[2];
+      rc = sync_read(ctx, d_sc, 2, ov);
+      if (rc) return rc;
+      ol = std::sqrt(ov[0] * ov[0] + (is_cplx(dtype) ? ov[1] * ov[1] : 0.0));
+    }
+    *ortho_loss = ol;
+  }
+  *n_out = n;
+  if (norm2_out) *norm2_out = n2;
+  if (converged) *converged = conv ? 1 : 0;
+  return EL_OK;
+}

@@ -181,6 +181,16 @@ int el_lanczos_ground(el_ctx *ctx, el_ham *ham, int dtype, const void *v0,
                       double tol, int nev, int reorth, double *evals,
                       double *residuals, int *iters, int *converged,
                       void *vec_out);
+/* Lanczos tridiagonalisation from a source state (device phi, not modified):
+ * alphas[n] and betas[n-1] of H in the Krylov basis of phi, with full
+ * reorthogonalisation (twice per step) when reorth != 0.  Stops at
+ * n_krylov steps, at beta <= 1e-12 or when the Krylov space is the whole
+ * basis (converged = 1 then).  norm2 = |phi|^2; ortho_loss = |<q_0, q_last>|
+ * (0 without reorth).  Replaces spectrum.py:34-103 (lanczos) for
+ * spectrum.py:138-180 (source_spectrum) and eq_route.py:260-337. */
+int el_lanczos_tridiag(el_ctx *ctx, el_ham *ham, int dtype, const void *phi, int n_krylov,
+                       int reorth, double *alphas, double *betas, int *n, double *norm2,
+                       double *ortho_loss, int *converged);
 
 /* ---- batched ground states ---------------------------------------------- */
 

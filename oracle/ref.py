@@ -309,3 +309,37 @@ def site_occupations(n, codes, psi):
     codes = np.arange(1 << n) if codes is None else codes
     p = np.abs(np.asarray(psi)) ** 2
     return basis_bits(n, codes).astype(float) @ p
+
+
+# ---------------------------------------------------------------- spectrum
+
+def lanczos_tridiag(apply_h, phi, k, reorth=True):
+    """alphas, betas, n of the Lanczos run from phi (spectrum.py:34-103):
+    q_0 = phi/|phi|, alpha_j = Re<q_j, H q_j>, three-term recurrence, full
+    Gram-Schmidt twice per step against the stored q's, stop at beta <= 1e-12
+    or when the Krylov space is the whole space; beta_j kept while another
+    step follows."""
+    v = np.asarray(phi, complex).reshape(-1)
+    dim = v.size
+    k = min(int(k), dim)
+    q = v / np.linalg.norm(v)
+    q_prev = np.zeros_like(q)
+    al, be, basis = [], [], []
+    beta = 0.0
+    for j in range(k):
+        basis.append(q)
+        w = np.asarray(apply_h(q), complex)
+        alpha = float(np.vdot(q, w).real)
+        w = w - alpha * q - (beta * q_prev if j else 0.0)
+        if reorth:
+            for _ in range(2):
+                for b in basis:
+                    w = w - np.vdot(b, w) * b
+        beta = float(np.linalg.norm(w))
+        al.append(alpha)
+        if beta <= 1e-12 or len(al) >= dim:
+            break
+        if j + 1 < k:
+            be.append(beta)
+        q_prev, q = q, w / beta
+    return np.asarray(al), np.asarray(be), len(al)

@@ -164,5 +164,62 @@ def main(ref_root: str) -> None:
     print("golden fixtures written to", HERE)
 
 
+def spectrum_fixture(ref_root: str) -> None:
+    """Source-state spectrum: eq_route.solve_equilibrium(want='spectrum')
+    (eq_route.py:260-337) with a site-weight source minus its mean, and the
+    Lanczos tridiagonal of spectrum.lanczos (spectrum.py:34-103) from the same
+    source state, on a 10-site chain blockade plan."""
+    sys.path.insert(0, ref_root)
+    from src.core.manybody import eq_route as rroute                    # eq_route.py
+    from src.core.manybody import spectrum as rspec                     # spectrum.py
+    from src.core.manybody import matrix_free as rmf                    # matrix_free.py
+    from src.core.manybody import hamiltonian_plan as rplan             # hamiltonian_plan.py
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from energy_level_b200 import configs
+    n = 10
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+    om, de = np.full(n, 2.0), np.full(n, -1.5)
+    plan = rplan.build_plan(calib, Om=om, delta=de, terms=["I1"],
+                            constraint={"kind": "blockade", "edges": configs.chain_edges(n)})
+    codes = np.asarray(plan["states"], np.int64)
+    weights = np.cos(np.pi * np.arange(n) / 3.0)
+    source = {"kind": "site_weights", "weights": weights, "subtract_mean": True}
+    opts = {"eta": 0.1, "n_krylov": 40, "n_omega": 300}
+    # the route on the full 2^N basis (the reference's spectrum route takes no
+    # projected plan: its |0> and H live on the full space)
+    sysd = {"calib": calib, "Om": om, "delta": de, "terms": ["I1"],
+            "source": source, "spectrum": opts}
+    try:
+        res = rroute.solve_equilibrium(sysd, want="spectrum", backend="lanczos")
+    except Exception as exc:   # route unavailable for this plan: keep the Lanczos part only
+        print("spectrum route:", exc)
+        res = None
+    H = rmf.hamiltonian_linear_operator(calib, om, de, None, ["I1"], basis_indices=codes)
+    rng = np.random.default_rng(7)
+    psi = rng.normal(size=len(codes)) + 1j * rng.normal(size=len(codes))
+    psi /= np.linalg.norm(psi)
+    bits = np.asarray([((codes >> (n - 1 - i)) & 1) for i in range(n)], float)
+    d = bits.T @ weights
+    phi = d * psi
+    lz = rspec.lanczos(H, phi, 40)
+    sp = rspec.source_spectrum(H, phi, shift=0.3, eta=0.1, n_krylov=40, n_omega=300)
+    out = dict(n=np.int64(n), om=om, de=de, codes=codes, weights=weights,
+               pairs=np.asarray([[p["i"], p["j"], p["V"]] for p in calib["pairs"]]),
+               psi=psi, phi=phi, alphas=lz["alphas"], betas=lz["betas"], norm2=lz["norm2"],
+               lz_n=np.int64(lz["n"]), sp_omega=sp["omega"], sp_spectral=sp["spectral"],
+               sp_evals=sp["evals"], sp_weights=sp["spectrum_weights"])
+    if res is not None:
+        out.update(route_E0=np.float64(res["E0"] if res["E0"] is not None else np.nan),
+                   route_energies=res["energies"], route_spectral=res["spectral"],
+                   route_source_norm=np.float64(res["source_norm"]))
+    np.savez_compressed(os.path.join(HERE, "spectrum.npz"), **out)
+    print("spectrum fixture written to", HERE)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) > 2 and sys.argv[2] == "spectrum":
+        spectrum_fixture(root)
+    else:
+        main(root)
+        spectrum_fixture(root)
