@@ -6,7 +6,7 @@ and time evolution through TIME_BACKENDS -> runspec._ENGINE_TABLE
 (backends.py:48-110, 177-179; runspec.py:660-697).  This module declares the
 B200 backends in the same shapes:
 
-    EQ_BACKENDS   'b200-lanczos': ('gs', 'spectrum')   'b200-kpm': ('thermal', 'dos')
+    EQ_BACKENDS   'b200-lanczos': ('gs', 'spectrum', 'ramp')   'b200-kpm': ('thermal', 'dos')
     TIME_BACKENDS 'b200-cheb': TimeBackend(segments, projected, return_state)
 
 ``solve_equilibrium`` accepts the reference's ``system`` dict and keyword
@@ -41,7 +41,7 @@ class TimeBackend:
 
 
 EQ_BACKENDS = {
-    'b200-lanczos': ('gs', 'spectrum'),
+    'b200-lanczos': ('gs', 'spectrum', 'ramp'),
     'b200-kpm': ('thermal', 'dos'),
 }
 
@@ -101,7 +101,8 @@ def engine_entries():
 
 def solve_equilibrium(system, want='gs', *, backend='b200-lanczos', betas=None, k=2, v0=None,
                       seed=0, num=400, nvec=200, dtype=None, memory_budget_mb=None,
-                      return_state=False, sector=None, progress_arr=None, **unused):
+                      return_state=False, sector=None, progress_arr=None, ramp=None, log=None,
+                      **unused):
     """eq_route.solve_equilibrium for the b200 names (same result keys)."""
     from . import kpm as bkpm
     from .matrix_free import b200_lanczos_ground_state
@@ -166,6 +167,8 @@ def solve_equilibrium(system, want='gs', *, backend='b200-lanczos', betas=None, 
         if return_state:
             out['vec'] = vec
         return out
+    if want == 'ramp':
+        return _solve_ramp(system, base, ramp, v0, seed, log, dtype, progress_arr)
     if want == 'spectrum':
         return _solve_spectrum(system, base, sector=sector, memory_budget_mb=memory_budget_mb,
                                progress_arr=progress_arr, dtype=dtype, seed=seed)
@@ -183,6 +186,82 @@ def solve_equilibrium(system, want='gs', *, backend='b200-lanczos', betas=None, 
                               chunk=system.get('kpm_chunk', 32))
         return dict(base, energies=r['energies'], rho=r['rho'])
     raise ValueError('want 需为 gs/thermal/dos，实=%r' % want)
+
+
+def _solve_ramp(system, base, ramp, v0, seed, log, dtype, progress_arr):
+    """Adiabatic sequence of ground states (eq_route.py:493-536 _solve_ramp)
+    on the GPU: at every point tau_i, H(Omega_t[i], delta_t[i]) with the drive
+    uniform over the sites (times system['Om_shape'] / ['delta_shape'] when
+    given), ground state and gap by the device Lanczos, warm-started from the
+    previous point's ground state when ramp['v0_warm'] (default).  The
+    reference takes a host H_builder(Om, delta); this backend builds H from
+    system['calib'] (and a projected plan, if any) instead."""
+    from . import model, solvers
+    if ramp is None:
+        raise ValueError("want='ramp' 需要 ramp=dict(Om_t, de_t, L, ...)")
+    if 'calib' not in system:
+        raise ValueError("b200 ramp 需要 system['calib']（H_builder 是主机算子）")
+    Om_t = np.asarray(ramp['Om_t'], float)
+    de_t = np.asarray(ramp['de_t'], float)
+    taus = np.asarray(ramp.get('taus', np.linspace(0.0, 1.0, len(Om_t))), float)
+    if len(de_t) != len(Om_t) or len(taus) != len(Om_t):
+        raise ValueError('ramp 的 Om_t/de_t/taus 长度须一致')
+    L = ramp.get('L')
+    if L is None:
+        raise ValueError('ramp 需要 L（密度归一格点数）')
+    n = len(system['calib']['atoms'])
+    om_shape = np.asarray(system.get('Om_shape', np.ones(n)), float)
+    de_shape = np.asarray(system.get('delta_shape', np.ones(n)), float)
+    n_tot = np.asarray(ramp['n_tot'], float) if ramp.get('n_tot') is not None else None
+    v0_warm = bool(ramp.get('v0_warm', True))
+    plan = system.get('plan') or {}
+    ctx, basis, ham, perm = model.build(system['calib'], Om_t[0] * om_shape, de_t[0] * de_shape,
+                                        system.get('gamma'), system.get('terms'),
+                                        plan=plan if plan.get('projected') else None,
+                                        device=system.get('device', 'cuda'))
+    if n_tot is not None and n_tot.size != basis.dim:
+        raise ValueError('ramp n_tot 长度 %d ≠ 基维度 %d' % (n_tot.size, basis.dim))
+    vdt = dtype or 'float64'
+    v_i = v0
+    gaps, ns, e0s, conv = [], [], [], []
+    for it in range(len(taus)):
+        if progress_arr is not None and float(progress_arr[1]) != 0:
+            raise RuntimeError('用户取消')
+        ham.set_drive(Om_t[it] * om_shape, de_t[it] * de_shape)
+        r = solvers.lanczos_ground(ham, dtype=vdt, v0=v_i, seed=seed, max_iter=min(300, basis.dim),
+                                   tol=1e-10 if vdt in ('float64', 'complex128') else 2e-5,
+                                   nev=min(2, basis.dim), return_vec=True)
+        if not r['converged'] and v_i is not None:
+            r = solvers.lanczos_ground(ham, dtype=vdt, v0=None, seed=seed + 1, max_iter=min(300, basis.dim),
+                                       tol=1e-10 if vdt in ('float64', 'complex128') else 2e-5,
+                                       nev=min(2, basis.dim), return_vec=True)
+        if v0_warm:
+            # previous ground state plus a small seeded random part: a start
+            # vector with the ground state's symmetry alone would never reach
+            # an excited state of another symmetry sector, and the gap would
+            # be that of the wrong state
+            import torch
+            gen = torch.Generator(device=r['vec'].device).manual_seed(int(seed) + 7919 * (it + 1))
+            noise = torch.randn(r['vec'].shape, dtype=r['vec'].dtype, device=r['vec'].device, generator=gen)
+            v_i = r['vec'] + 1e-2 * noise / noise.norm()
+        else:
+            v_i = None
+        ev = np.asarray(r['evals'], float)
+        e0s.append(float(ev[0]))
+        gaps.append(float(ev[1] - ev[0]) if len(ev) > 1 else 0.0)
+        conv.append(bool(r['converged']))
+        if n_tot is not None:
+            p = (r['vec'].abs() ** 2).double().cpu().numpy()
+            ns.append(float(n_tot @ p) / float(L))
+        else:
+            ns.append(float('nan'))
+        if progress_arr is not None:
+            progress_arr[0] = (it + 1) / len(taus)
+        if log is not None and (it % max(1, len(taus) // 10) == 0 or it == len(taus) - 1):
+            log('ramp %d/%d Ω=%.3f δ=%.3f gap=%.4f n=%.4f' % (it + 1, len(taus), Om_t[it], de_t[it],
+                                                             gaps[-1], ns[-1]))
+    return dict(base, taus=taus, gaps=np.asarray(gaps, float), ns=np.asarray(ns, float),
+                Om_t=Om_t, de_t=de_t, E0s=np.asarray(e0s), converged=np.asarray(conv))
 
 
 def _solve_spectrum(system, base, *, sector, memory_budget_mb, progress_arr, dtype, seed):

@@ -216,10 +216,40 @@ def spectrum_fixture(ref_root: str) -> None:
     print("spectrum fixture written to", HERE)
 
 
+def ramp_fixture(ref_root: str) -> None:
+    """Equilibrium ramp: eq_route.solve_equilibrium(want='ramp') (eq_route.py:
+    493-536) on an 8-site chain, H_builder = assemble.build_H_sparse with a
+    uniform drive (assemble.py:277), n_tot = excitation count per state."""
+    sys.path.insert(0, ref_root)
+    from src.core.manybody import eq_route as rroute                    # eq_route.py
+    from src.core.manybody import assemble as rasm                      # assemble.py
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from energy_level_b200 import configs
+    n = 8
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+
+    def hb(om, de):
+        return rasm.build_H_sparse(calib, np.full(n, om), np.full(n, de), terms=["I1"])
+
+    codes = np.arange(1 << n, dtype=np.int64)
+    n_tot = np.asarray([bin(int(c)).count("1") for c in codes], float)
+    Om_t = np.linspace(0.5, 2.5, 9)
+    de_t = np.linspace(4.0, -6.0, 9)
+    res = rroute.solve_equilibrium({"calib": calib, "H_builder": hb, "n_sites": n}, want="ramp",
+                                   backend="ed", ramp={"Om_t": Om_t, "de_t": de_t, "L": n, "n_tot": n_tot})
+    np.savez_compressed(os.path.join(HERE, "ramp.npz"), n=np.int64(n), Om_t=Om_t, de_t=de_t,
+                        taus=res["taus"], gaps=res["gaps"], ns=res["ns"])
+    print("ramp fixture written to", HERE)
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    if len(sys.argv) > 2 and sys.argv[2] == "spectrum":
+    which = sys.argv[2] if len(sys.argv) > 2 else "all"
+    if which == "spectrum":
         spectrum_fixture(root)
+    elif which == "ramp":
+        ramp_fixture(root)
     else:
         main(root)
         spectrum_fixture(root)
+        ramp_fixture(root)
