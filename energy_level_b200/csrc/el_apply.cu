@@ -499,10 +499,24 @@ __global__ void __launch_bounds__(256) k_apply_chain_tile(BasisDev B, HamArgs<S>
   __shared__ TileFlip hf[EL_MAX_SITES];
   __shared__ S hf_re[EL_MAX_SITES], hf_im[EL_MAX_SITES];
   __shared__ int nhf;
+  __shared__ int s_w[EL_MAX_SITES];            // F(k+2) of the low bits
+  __shared__ S s_are[EL_MAX_SITES], s_aim[EL_MAX_SITES];
+  __shared__ uint32_t s_amp;                    // low bits with a nonzero amplitude
   __shared__ int64_t t_base;
   __shared__ int t_size;
   __shared__ int t_bl;       // bit L of the tile's prefix
   __shared__ S t_delta;      // detuning sum of the prefix bits
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    s_w[k] = (int)B.fib[k + 2];
+    s_are[k] = H.up_re[k];
+    s_aim[k] = C ? H.up_im[k] : S(0);
+  }
+  if (threadIdx.x == 0) {
+    uint32_t am = 0;
+    for (int k = 0; k < L; ++k)
+      if (H.up_re[k] != S(0) || (C && H.up_im[k] != S(0))) am |= 1u << k;
+    s_amp = am;
+  }
   // low codes of the L-site chain in ascending order, and their detunings
   for (int i = threadIdx.x; i < TS; i += blockDim.x) {
     uint32_t c = 0;
@@ -595,19 +609,25 @@ __global__ void __launch_bounds__(256) k_apply_chain_tile(BasisDev B, HamArgs<S>
       S h[W];
 #pragma unroll
       for (int q = 0; q < W; ++q) h[q] = S(0);
-      // low flips, partners in shared memory
-      for (int k = 0; k < L; ++k) {
-        const bool set = (c >> k) & 1u;
-        const bool up = (k + 1 < L) ? ((c >> (k + 1)) & 1u) : (bl != 0);
-        const bool dn = (k >= 1) && ((c >> (k - 1)) & 1u);
-        if (!set && (up || dn)) continue;
-        const S are = H.up_re[k];
-        const S aim = C ? (set ? H.up_im[k] : -H.up_im[k]) : S(0);
-        const int w = (int)B.fib[k + 2];
-        const int pi = set ? i - w : i + w;
-        S xv[W];
-        tile_ld<S, W>(xt, TS, pi, xv);
-        acc_flip<S, C, NV>(h, are, aim, xv);
+      // low flips, partners in shared memory: the flippable bits are the set
+      // ones and those with both neighbours empty (bit L above the top low
+      // bit is the tile's bl); walk the set bits of that mask
+      {
+        const uint32_t lowmask = (L >= 32) ? ~0u : ((1u << L) - 1u);
+        const uint32_t occ = (c << 1) | (c >> 1) | ((uint32_t)bl << (L - 1));
+        uint32_t m = (c | (~occ & lowmask)) & s_amp;
+        while (m) {
+          const int k = __ffs(m) - 1;
+          m &= m - 1;
+          const bool set = (c >> k) & 1u;
+          const int w = s_w[k];
+          const int pi = set ? i - w : i + w;
+          const S are = s_are[k];
+          const S aim = set ? s_aim[k] : -s_aim[k];
+          S xv[W];
+          tile_ld<S, W>(xt, TS, pi, xv);
+          acc_flip<S, C, NV>(h, are, aim, xv);
+        }
       }
       // high flips: contiguous partner rows in global memory, two in flight
       for (int f = 0; f < nh; f += 2) {
