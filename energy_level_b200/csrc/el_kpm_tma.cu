@@ -57,7 +57,6 @@ __device__ __forceinline__ double get8(double v, int) { return v; }
 
 enum { KIND_A = 0, KIND_B = 1 };
 enum { MODE_STEP = 0, MODE_PROLOGUE = 1, MODE_LAST = 2 };
-constexpr int NT = 1024;
 
 template <typename T>
 struct TmaArgs {
@@ -149,8 +148,8 @@ __device__ __forceinline__ uint32_t row_of(int a, uint32_t tile, int l) {
 }
 
 // h[j] += sum_{k in [K0, KMAX)} amp_k * S[(tid ^ 2^k) + NT*j] for the R cells
-// of this thread.  Bit-outer order: one address per bit, R independent FMA
-// chains per bit.
+// of this thread (NT = 2^KMAX threads).  Bit-outer order: one address per
+// bit, R independent FMA chains per bit.
 template <typename T, int R, int K0, int KMAX>
 __device__ __forceinline__ void gather_all(const T *S, int tid, const TmaArgs<T> &A, T (&h)[R]) {
 #pragma unroll
@@ -158,19 +157,20 @@ __device__ __forceinline__ void gather_all(const T *S, int tid, const TmaArgs<T>
     const T *base = S + (tid ^ (1 << k));
     const T a = A.amp[k];
 #pragma unroll
-    for (int j = 0; j < R; ++j) h[j] = fma8(a, base[NT * j], h[j]);
+    for (int j = 0; j < R; ++j) h[j] = fma8(a, base[(1 << KMAX) * j], h[j]);
   }
 }
 
-template <typename T, int TB, int KIND>
-__global__ void __launch_bounds__(NT, 1)
+template <typename T, int TB, int KIND, int LNT>
+__global__ void __launch_bounds__(1 << LNT, 1)
 k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
           const __grid_constant__ CUtensorMap mapQ) {
   typedef typename Cell<T>::U U;
   constexpr int PU = Cell<T>::PU;
   constexpr int C = Cell<T>::CARRY;
-  constexpr int R = (1 << TB) / NT;          // cells per thread (TB >= 10)
-  constexpr int LOGNT = 10;
+  constexpr int NT = 1 << LNT;               // threads per CTA
+  constexpr int R = (1 << TB) / NT;          // cells per thread (TB >= LNT)
+  constexpr int LOGNT = LNT;
   constexpr int NWARP = NT / 32;
   constexpr int K0 = (KIND == KIND_B) ? C : 0;
   constexpr unsigned TILE_BYTES = (1u << TB) * (unsigned)sizeof(T);
@@ -513,17 +513,21 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     const CUtensorMap &mp = kind == KIND_A ? mA[pbuf] : mB[pbuf];
     const CUtensorMap &mq = kind == KIND_A ? mA[pbuf ^ 1] : mB[pbuf ^ 1];
     const size_t smem = (size_t)3 * ((size_t)1 << TB) * sizeof(T);
+    // 512 threads with 2^(TB-9) cells each for large tiles: one more tile bit
+    // per thread in registers (one fewer shared-memory gather per cell per X
+    // application) measured faster than 1024 (2^(TB-10) cells) or 256 threads
+    const int lnt = (TB >= 12) ? 9 : 10;
     bool ok = false;
-#define EL_TCASE(TBV, KV)                                                                     \
-  if (TB == TBV && kind == KV) {                                                              \
-    cudaFuncSetAttribute(k_kpm_tma<T, TBV, KV>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                         (int)smem);                                                          \
-    k_kpm_tma<T, TBV, KV><<<grid, NT, smem, ctx->stream>>>(A, mp, mq);                        \
-    ok = true;                                                                                \
+#define EL_TCASE(TBV, KV, LV)                                                                     \
+  if (TB == TBV && kind == KV && lnt == LV) {                                                     \
+    cudaFuncSetAttribute(k_kpm_tma<T, TBV, KV, LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                         (int)smem);                                                              \
+    k_kpm_tma<T, TBV, KV, LV><<<grid, 1 << LV, smem, ctx->stream>>>(A, mp, mq);                   \
+    ok = true;                                                                                    \
   }
-    EL_TCASE(10, KIND_A) EL_TCASE(11, KIND_A) EL_TCASE(12, KIND_A) EL_TCASE(13, KIND_A)
-    EL_TCASE(10, KIND_B) EL_TCASE(11, KIND_B) EL_TCASE(12, KIND_B) EL_TCASE(13, KIND_B)
-    if constexpr (sizeof(T) == 4) { EL_TCASE(14, KIND_A) EL_TCASE(14, KIND_B) }
+    EL_TCASE(10, KIND_A, 10) EL_TCASE(11, KIND_A, 10) EL_TCASE(10, KIND_B, 10) EL_TCASE(11, KIND_B, 10)
+    EL_TCASE(12, KIND_A, 9) EL_TCASE(13, KIND_A, 9) EL_TCASE(12, KIND_B, 9) EL_TCASE(13, KIND_B, 9)
+    if constexpr (sizeof(T) == 4) { EL_TCASE(14, KIND_A, 9) EL_TCASE(14, KIND_B, 9) }
 #undef EL_TCASE
     if (!ok) return fail(ctx, EL_EINVAL, "TMA pass with %d tile bits not instantiated", TB);
     EL_LAUNCH_CHECK(ctx);
