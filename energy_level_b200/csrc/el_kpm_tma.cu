@@ -278,8 +278,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         const int l = tid + NT * j;
-        const uint32_t row = row_of<KIND, C>(A.a, tile, l);
-        S2[l] = fma8(A.pro_beta, hx[j], scl8(A.pro_alpha * d2[row], own[j]));
+        S2[l] = fma8(A.pro_beta, hx[j], scl8(A.pro_alpha * d2[((size_t)tile << TB) + l], own[j]));
 #pragma unroll
         for (int q = 0; q < PU; ++q) pt[q][j & 1] = fma(get8(own[j], q), get8(own[j], q), pt[q][j & 1]);
       }
@@ -311,7 +310,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
         // that its latency hides behind them
         T dv[R];
 #pragma unroll
-        for (int j = 0; j < R; ++j) dv[j] = d2[row_of<KIND, C>(A.a, tile, tid + NT * j)];
+        for (int j = 0; j < R; ++j) dv[j] = d2[((size_t)tile << TB) + tid + NT * j];
         U h2[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) h2[j] = z8(U{});
@@ -403,6 +402,18 @@ __global__ void k_d2_8(int n, int64_t dim, const double *diagV, const double *de
   }
 }
 
+// out[(tile << tb) + l] = d[row of cell l of B tile `tile`]
+template <typename T>
+__global__ void k_d2_border(int64_t dim, int a, int tb, const T *d, T *out) {
+  constexpr int C = Cell<T>::CARRY;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < dim;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t tile = (uint32_t)(q >> tb);
+    const int l = (int)(q & (((int64_t)1 << tb) - 1));
+    out[q] = d[row_of<KIND_B, C>(a, tile, l)];
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -457,11 +468,12 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   const int64_t dim = h->basis->dim;
   const int ng = chunk / PU;
   const size_t vb = (size_t)dim * chunk * sizeof(T);
-  char *buf = (char *)el::workspace(ctx, 6, 2 * vb + (size_t)dim * sizeof(T) + 64);
+  char *buf = (char *)el::workspace(ctx, 6, 2 * vb + 2 * (size_t)dim * sizeof(T) + 64);
   if (!buf) return EL_ENOMEM;
   void *P = buf, *Q = buf + vb;
   T *d2 = reinterpret_cast<T *>(buf + 2 * vb);
-  int *d_err = reinterpret_cast<int *>(buf + 2 * vb + (size_t)dim * sizeof(T));
+  T *d2b = d2 + dim;   // the same diagonal in B-tile order
+  int *d_err = reinterpret_cast<int *>(buf + 2 * vb + 2 * (size_t)dim * sizeof(T));
   const int M = (num + 1) / 2;
   double *d_dots = (double *)el::workspace(ctx, 7, (size_t)(M + 1) * chunk * 2 * sizeof(double));
   if (!d_dots) return EL_ENOMEM;
@@ -482,6 +494,10 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   const int amax = sizeof(T) == 4 ? 14 : 13;
   const int a = std::min(amax, std::max((n + C + 1) / 2, n + C - amax));
   const int TBA = a, TBB = n - a + C;
+  // tiles read the diagonal as d[(tile << TB) + l]: row order for A tiles,
+  // a B-tile-ordered copy for B tiles (coalesced like the A reads)
+  k_d2_border<T><<<el::grid_for(dim, 256), 256, 0, ctx->stream>>>(dim, a, TBB, d2, d2b);
+  EL_LAUNCH_CHECK(ctx);
   const int hb = (int)std::min<int64_t>(256, (int64_t)1 << (n - a));
   CUtensorMap mA[2], mB[2];   // [P buffer, Q buffer]
   int rc = make_maps<T>(ctx, P, n, a, ng, hb, &mA[0], &mB[0]);
@@ -505,7 +521,7 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
       int rowbit = (kind == KIND_A) ? k : (k >= C ? a + k - C : -1);
       A.amp[k] = (T)((rowbit >= 0) ? 0.5 * h->om_re[rowbit] : 0.0);
     }
-    A.d2 = d2; A.dots = dots; A.err = d_err; A.counter = ctx->d_counter;
+    A.d2 = kind == KIND_A ? d2 : d2b; A.dots = dots; A.err = d_err; A.counter = ctx->d_counter;
     const int grid = (int)std::min<int64_t>(A.items, sms);
     int e = el::ensure_partials(ctx, (size_t)grid * ng * PU * 2);
     if (e) return e;
