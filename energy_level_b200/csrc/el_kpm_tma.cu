@@ -147,6 +147,15 @@ __device__ __forceinline__ uint32_t row_of(int a, uint32_t tile, int l) {
   return (uint32_t)(l & ((1 << C) - 1)) + ((uint32_t)(l >> C) << a) + (tile << C);
 }
 
+// Index of cell l of a tile in the diagonal array the kernel is given: FP32
+// B tiles read a B-tile-ordered copy (one coalesced request per warp); A
+// tiles, and FP64 B tiles (measured slower with the copy), read row order.
+template <typename T, int KIND, int TB>
+__device__ __forceinline__ size_t d2_index(int a, uint32_t tile, int l) {
+  if (KIND == KIND_B && sizeof(T) == 8) return row_of<KIND_B, Cell<T>::CARRY>(a, tile, l);
+  return ((size_t)tile << TB) + (size_t)l;
+}
+
 // h[j] += sum_{k in [K0, KMAX)} amp_k * S[(tid ^ 2^k) + NT*j] for the R cells
 // of this thread (NT = 2^KMAX threads).  Bit-outer order: one address per
 // bit, R independent FMA chains per bit.
@@ -278,7 +287,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         const int l = tid + NT * j;
-        S2[l] = fma8(A.pro_beta, hx[j], scl8(A.pro_alpha * d2[((size_t)tile << TB) + l], own[j]));
+        S2[l] = fma8(A.pro_beta, hx[j], scl8(A.pro_alpha * d2[d2_index<T, KIND, TB>(A.a, tile, l)], own[j]));
 #pragma unroll
         for (int q = 0; q < PU; ++q) pt[q][j & 1] = fma(get8(own[j], q), get8(own[j], q), pt[q][j & 1]);
       }
@@ -310,7 +319,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
         // that its latency hides behind them
         T dv[R];
 #pragma unroll
-        for (int j = 0; j < R; ++j) dv[j] = d2[((size_t)tile << TB) + tid + NT * j];
+        for (int j = 0; j < R; ++j) dv[j] = d2[d2_index<T, KIND, TB>(A.a, tile, tid + NT * j)];
         U h2[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) h2[j] = z8(U{});
@@ -494,10 +503,10 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   const int amax = sizeof(T) == 4 ? 14 : 13;
   const int a = std::min(amax, std::max((n + C + 1) / 2, n + C - amax));
   const int TBA = a, TBB = n - a + C;
-  // tiles read the diagonal as d[(tile << TB) + l]: row order for A tiles,
-  // a B-tile-ordered copy for B tiles (coalesced like the A reads)
-  k_d2_border<T><<<el::grid_for(dim, 256), 256, 0, ctx->stream>>>(dim, a, TBB, d2, d2b);
-  EL_LAUNCH_CHECK(ctx);
+  if (sizeof(T) == 4) {   // B-tile-ordered copy of the diagonal (see d2_index)
+    k_d2_border<T><<<el::grid_for(dim, 256), 256, 0, ctx->stream>>>(dim, a, TBB, d2, d2b);
+    EL_LAUNCH_CHECK(ctx);
+  }
   const int hb = (int)std::min<int64_t>(256, (int64_t)1 << (n - a));
   CUtensorMap mA[2], mB[2];   // [P buffer, Q buffer]
   int rc = make_maps<T>(ctx, P, n, a, ng, hb, &mA[0], &mB[0]);
@@ -521,7 +530,7 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
       int rowbit = (kind == KIND_A) ? k : (k >= C ? a + k - C : -1);
       A.amp[k] = (T)((rowbit >= 0) ? 0.5 * h->om_re[rowbit] : 0.0);
     }
-    A.d2 = kind == KIND_A ? d2 : d2b; A.dots = dots; A.err = d_err; A.counter = ctx->d_counter;
+    A.d2 = (kind == KIND_B && sizeof(T) == 4) ? d2b : d2; A.dots = dots; A.err = d_err; A.counter = ctx->d_counter;
     const int grid = (int)std::min<int64_t>(A.items, sms);
     int e = el::ensure_partials(ctx, (size_t)grid * ng * PU * 2);
     if (e) return e;
@@ -529,10 +538,11 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     const CUtensorMap &mp = kind == KIND_A ? mA[pbuf] : mB[pbuf];
     const CUtensorMap &mq = kind == KIND_A ? mA[pbuf ^ 1] : mB[pbuf ^ 1];
     const size_t smem = (size_t)3 * ((size_t)1 << TB) * sizeof(T);
-    // 512 threads with 2^(TB-9) cells each for large tiles: one more tile bit
-    // per thread in registers (one fewer shared-memory gather per cell per X
-    // application) measured faster than 1024 (2^(TB-10) cells) or 256 threads
-    const int lnt = (TB >= 12) ? 9 : 10;
+    // FP32, large tiles: 512 threads with 2^(TB-9) cells each (one more tile
+    // bit per thread in registers, one fewer shared-memory gather per cell per
+    // X application) measured faster than 1024 or 256 threads.  FP64 keeps
+    // 1024 threads: twice the registers per cell made 512 threads slower.
+    const int lnt = (sizeof(T) == 4 && TB >= 12) ? 9 : 10;
     bool ok = false;
 #define EL_TCASE(TBV, KV, LV)                                                                     \
   if (TB == TBV && kind == KV && lnt == LV) {                                                     \
@@ -542,8 +552,12 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     ok = true;                                                                                    \
   }
     EL_TCASE(10, KIND_A, 10) EL_TCASE(11, KIND_A, 10) EL_TCASE(10, KIND_B, 10) EL_TCASE(11, KIND_B, 10)
-    EL_TCASE(12, KIND_A, 9) EL_TCASE(13, KIND_A, 9) EL_TCASE(12, KIND_B, 9) EL_TCASE(13, KIND_B, 9)
-    if constexpr (sizeof(T) == 4) { EL_TCASE(14, KIND_A, 9) EL_TCASE(14, KIND_B, 9) }
+    if constexpr (sizeof(T) == 4) {
+      EL_TCASE(12, KIND_A, 9) EL_TCASE(13, KIND_A, 9) EL_TCASE(12, KIND_B, 9) EL_TCASE(13, KIND_B, 9)
+      EL_TCASE(14, KIND_A, 9) EL_TCASE(14, KIND_B, 9)
+    } else {
+      EL_TCASE(12, KIND_A, 10) EL_TCASE(13, KIND_A, 10) EL_TCASE(12, KIND_B, 10) EL_TCASE(13, KIND_B, 10)
+    }
 #undef EL_TCASE
     if (!ok) return fail(ctx, EL_EINVAL, "TMA pass with %d tile bits not instantiated", TB);
     EL_LAUNCH_CHECK(ctx);
