@@ -124,8 +124,8 @@ def solve_equilibrium(system, want='gs', *, backend='b200-lanczos', betas=None, 
         constraint = None
         if sector is not None or system.get('charge_sector') is not None:
             kq = int(sector if sector is not None else system['charge_sector'])
-            if np.any(np.asarray(system.get('Om') if system.get('Om') is not None else 0) != 0):
-                raise ValueError('固定 charge_sector 要求 Omega=0')
+            from .model import check_number_conserving
+            check_number_conserving(system['calib'], system.get('Om'), system.get('terms'))
             constraint = {'kind': 'charge', 'k': kq}
         from . import model, solvers
         if constraint is not None:
@@ -284,8 +284,7 @@ def _solve_spectrum(system, base, *, sector, memory_budget_mb, progress_arr, dty
     constraint = None
     if sector is not None:
         constraint = {'kind': 'charge', 'k': int(sector)}
-        if np.any(np.asarray(system.get('Om') if system.get('Om') is not None else 0) != 0):
-            raise ValueError('固定 charge_sector 要求 Omega=0')
+        model.check_number_conserving(system['calib'], system.get('Om'), system.get('terms'))
     ctx, basis, ham, perm = model.build(system['calib'], system.get('Om'), system.get('delta'),
                                         system.get('gamma'), system.get('terms'),
                                         plan=plan if (plan.get('projected') and constraint is None) else None,

@@ -18,6 +18,10 @@ Workloads:
   ring20    ring N=20, NN spacing 5.5 um, NN blockade incl. (19, 0),
             200 steps of (Omega_k, Delta_k) from a smooth random ramp (seed 5),
             objective |<Z2|psi(T)>|^2
+  xy_chain  dipolar XY chain (Omega = 0): exchange J_ij = j0 (a / r_ij)^3 for
+            every pair (I2) plus a van der Waals V_ij (I1), random fields
+            delta_i ~ U(-1, 1); number-conserving, so it splits into the
+            fixed-excitation sectors that the sector scan solves one by one
 """
 from __future__ import annotations
 
@@ -129,3 +133,18 @@ def ring20(n=20, steps=200, seed=5, total_ns=2000.0):
     return dict(name='ring%d' % n, n=n, calib=calib, edges=ring_edges(n), omega_k=om,
                 delta_k=-Delta, tau=np.full(steps, total_ns / steps),
                 target='rg' * (n // 2) + ('r' if n % 2 else ''), psi0='g' * n)
+
+
+def xy_chain(n, a=5.5, j0=-0.7, seed=7, c6=C6_70S, v_scale=1e-3):
+    """Dipolar XY chain: calib with J (I2) and a weak V (I1) on every pair,
+    per-site delta ~ U(-1, 1) (seed), Om = 0."""
+    rng = np.random.default_rng(seed)
+    pos = chain_positions(n, a=a)
+    pairs = []
+    for i in range(n):
+        for j in range(i + 1, n):
+            r = float(np.linalg.norm(pos[j] - pos[i]))
+            pairs.append({'i': i, 'j': j, 'V': v_scale * c6 / r ** 6, 'J': j0 * (a / r) ** 3, 'A': 0.0})
+    calib = {'atoms': [{'id': i, 'pos': [float(x) for x in p]} for i, p in enumerate(pos)],
+             'pairs': pairs, 'terms': ['I1', 'I2']}
+    return dict(calib=calib, n=n, Om=np.zeros(n), delta=rng.uniform(-1.0, 1.0, n))

@@ -153,9 +153,11 @@ class Basis:
 
 
 class Hamiltonian:
-    """H = sum delta_i n_i + (Omega_i/2) sigma^x_i + sum V_ij n_i n_j on a basis."""
+    """H = sum delta_i n_i + (Omega_i/2) sigma^x_i + sum V_ij n_i n_j on a basis,
+    plus optional exchange channels ``exchange`` = [(i, j, J, A), ...]
+    (I2 hopping J and I3 pair creation A, channels.py:119-131)."""
 
-    def __init__(self, ctx: Context, basis: Basis, omega, delta, pairs):
+    def __init__(self, ctx: Context, basis: Basis, omega, delta, pairs, exchange=None):
         self.ctx = ctx
         self.basis = basis
         n = basis.n
@@ -180,10 +182,28 @@ class Hamiltonian:
         self.omega = om
         self.delta = de
         self.pairs = list(zip(pi.tolist(), pj.tolist(), V.tolist()))
+        self.exchange = []
+        if exchange:
+            self.set_exchange(exchange)
+
+    def set_exchange(self, exchange):
+        """Replace the exchange channels: [(i, j, J, A), ...] (complex J, A)."""
+        ex = [(int(e[0]), int(e[1]), complex(e[2]), complex(e[3])) for e in (exchange or [])]
+        pi = np.ascontiguousarray([e[0] for e in ex], dtype=np.int32)
+        pj = np.ascontiguousarray([e[1] for e in ex], dtype=np.int32)
+        amp = [np.ascontiguousarray([f(e) for e in ex], dtype=np.float64)
+               for f in (lambda e: e[2].real, lambda e: e[2].imag, lambda e: e[3].real, lambda e: e[3].imag)]
+        k = len(ex)
+        self.ctx.call('el_ham_set_exchange', self.handle, C.c_int(k),
+                      C.c_void_p(pi.ctypes.data) if k else None, C.c_void_p(pj.ctypes.data) if k else None,
+                      *[_lib.dptr(a) if k else None for a in amp])
+        self.exchange = ex
 
     @property
     def complex_drive(self) -> bool:
-        return bool(np.any(self.omega.imag != 0))
+        """H is complex: a complex Omega, J or A."""
+        return bool(np.any(self.omega.imag != 0)) or any(e[2].imag != 0 or e[3].imag != 0
+                                                         for e in getattr(self, 'exchange', ()))
 
     def set_drive(self, omega, delta):
         om = np.asarray(omega, complex).reshape(-1)

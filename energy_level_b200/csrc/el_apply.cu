@@ -25,7 +25,19 @@ struct HamArgs {
   S delta[EL_MAX_SITES];
   S up_re[EL_MAX_SITES];  // amplitude into a row whose bit k is 1: Omega/2
   S up_im[EL_MAX_SITES];  // (into a row whose bit k is 0: conj(Omega)/2)
+  const ExPair *px;       // exchange channels (generic kernel only)
+  int npx;
 };
+
+// Amplitude <row|H|row ^ (bit bi | bit bj)> of exchange pair e for a row whose
+// bits at bi, bj are (si, sj): J channel (channels.py:121-125) when the bits
+// differ -- J into (r, g), conj(J) into (g, r) -- and A channel
+// (channels.py:126-130) when they agree -- A into (r, r), conj(A) into (g, g).
+__device__ __forceinline__ void exchange_amp(const ExPair &e, bool si, bool sj,
+                                             double &re, double &im) {
+  if (si != sj) { re = e.jre; im = si ? e.jim : -e.jim; }
+  else { re = e.are; im = si ? e.aim : -e.aim; }
+}
 
 struct KArgs {
   int64_t nvec;
@@ -109,6 +121,22 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev B, HamArgs<S> H, KArgs K
       const int64_t tg = el::flip_target(B, code, row, k);
       if (tg < 0) continue;
       const V xs = V::load(K.x, (tg << K.lognv) + v);
+      if constexpr (C) {
+        hre += are * xs.re - aim * xs.im;
+        him += are * xs.im + aim * xs.re;
+      } else {
+        hre += are * xs.v;
+      }
+    }
+    for (int p = 0; p < H.npx; ++p) {
+      const ExPair e = H.px[p];
+      double pre, pim;
+      exchange_amp(e, (code >> e.bi) & 1ULL, (code >> e.bj) & 1ULL, pre, pim);
+      if (pre == 0.0 && pim == 0.0) continue;
+      const int64_t tg = el::rank_any(B, code ^ ((1ULL << e.bi) | (1ULL << e.bj)));
+      if (tg < 0) continue;
+      const V xs = V::load(K.x, (tg << K.lognv) + v);
+      const S are = (S)pre, aim = (S)pim;
       if constexpr (C) {
         hre += are * xs.re - aim * xs.im;
         him += are * xs.im + aim * xs.re;
@@ -701,6 +729,8 @@ HamArgs<S> ham_args(const el_ham *h, const S *diagV) {
   HamArgs<S> A;
   memset(&A, 0, sizeof A);
   A.diagV = diagV;
+  A.px = h->d_px;
+  A.npx = (int)h->px.size();
   for (int k = 0; k < h->n; ++k) {
     A.delta[k] = (S)h->delta[k];
     A.up_re[k] = (S)(0.5 * h->om_re[k]);
@@ -768,6 +798,13 @@ __global__ void k_gershgorin(BasisDev B, HamArgs<double> H, double *partials,
       const double amp = sqrt(H.up_re[k] * H.up_re[k] + H.up_im[k] * H.up_im[k]);
       if (amp == 0.0) continue;
       if (el::flip_target(B, code, r, k) >= 0) R += amp;
+    }
+    for (int p = 0; p < H.npx; ++p) {
+      const ExPair e = H.px[p];
+      double pre, pim;
+      exchange_amp(e, (code >> e.bi) & 1ULL, (code >> e.bj) & 1ULL, pre, pim);
+      if (pre == 0.0 && pim == 0.0) continue;
+      if (el::rank_any(B, code ^ ((1ULL << e.bi) | (1ULL << e.bj))) >= 0) R += sqrt(pre * pre + pim * pim);
     }
     lo = fmin(lo, d - R);
     hi = fmax(hi, d + R);
@@ -1034,6 +1071,7 @@ namespace {
 // (dot products only for one vector) when every vector pointer is aligned for
 // its row-segment loads.
 bool row_kernel_ok(const el_ham *h, const ApplyArgs &A) {
+  if (!h->px.empty()) return false;   // exchange channels: generic kernel
   const int lay = h->basis->layout;
   if (lay != EL_LAYOUT_FULL && lay != EL_LAYOUT_CHAIN && lay != EL_LAYOUT_RING) return false;
   if (A.nvec > 8) return false;
@@ -1165,7 +1203,7 @@ int launch_apply(el_ctx *ctx, el_ham *h, const ApplyArgs &A) {
   if (nvec < 1 || nvec > 256 || (nvec & (nvec - 1)))
     return fail(ctx, EL_EINVAL, "nvec must be a power of two in [1, 256], got %lld", (long long)nvec);
   if (!is_complex(A.dtype) && (h->complex_drive))
-    return fail(ctx, EL_EINVAL, "complex Omega needs a complex vector dtype");
+    return fail(ctx, EL_EINVAL, "complex Omega, J or A needs a complex vector dtype");
   BasisDev B = basis_dev(h->basis);
   KArgs K;
   K.nvec = nvec;
@@ -1463,7 +1501,54 @@ int el_ham_set_drive(el_ctx *ctx, el_ham *h, const double *omega_re,
     h->delta[q] = d;
     if (oim != 0.0) cplx = true;
   }
-  h->complex_drive = cplx;
+  h->drive_complex = cplx;
+  h->complex_drive = h->drive_complex || h->px_complex;
+  return EL_OK;
+}
+
+int el_ham_set_exchange(el_ctx *ctx, el_ham *h, int n_pairs, const int32_t *pi,
+                        const int32_t *pj, const double *J_re, const double *J_im,
+                        const double *A_re, const double *A_im) {
+  if (!ctx || !h) return EL_EINVAL;
+  if (n_pairs < 0 || (n_pairs > 0 && (!pi || !pj))) return fail(ctx, EL_EINVAL, "bad exchange pair list");
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int n = h->n;
+  std::vector<ExPair> px;
+  bool cplx = false;
+  for (int p = 0; p < n_pairs; ++p) {
+    const int i = pi[p], j = pj[p];
+    ExPair e;
+    e.jre = J_re ? J_re[p] : 0.0;
+    e.jim = J_im ? J_im[p] : 0.0;
+    e.are = A_re ? A_re[p] : 0.0;
+    e.aim = A_im ? A_im[p] : 0.0;
+    if (i < 0 || j < 0 || i >= n || j >= n || i == j)
+      return fail(ctx, EL_EINVAL, "exchange pair %d: bad sites (%d, %d)", p, i, j);
+    if (!std::isfinite(e.jre) || !std::isfinite(e.jim) || !std::isfinite(e.are) || !std::isfinite(e.aim))
+      return fail(ctx, EL_EINVAL, "exchange pair %d: non-finite J or A", p);
+    if (e.jre == 0.0 && e.jim == 0.0 && e.are == 0.0 && e.aim == 0.0) continue;
+    e.bi = n - 1 - i;
+    e.bj = n - 1 - j;
+    if (e.jim != 0.0 || e.aim != 0.0) cplx = true;
+    px.push_back(e);
+  }
+  ExPair *d = nullptr;
+  if (!px.empty()) {
+    cudaError_t e = cudaMalloc(&d, px.size() * sizeof(ExPair));
+    if (e != cudaSuccess) return el::fail(ctx, EL_ENOMEM, "cannot allocate exchange pairs (%s)", cudaGetErrorString(e));
+    e = el::copy(ctx, d, px.data(), px.size() * sizeof(ExPair), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { cudaFree(d); return el::cuda_fail(ctx, e, "exchange pairs"); }
+  }
+  // the previous list may still be read by work queued on the stream
+  if (h->d_px) {
+    EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(h->d_px);
+  }
+  h->d_px = d;
+  h->px.swap(px);
+  h->px_complex = cplx;
+  h->complex_drive = h->drive_complex || h->px_complex;
   return EL_OK;
 }
 
@@ -1478,6 +1563,7 @@ int el_ham_destroy(el_ham *h) {
   if (h->basis) cudaSetDevice(h->basis->device);
   if (h->d_diagV64) cudaFree(h->d_diagV64);
   if (h->d_diagV32) cudaFree(h->d_diagV32);
+  if (h->d_px) cudaFree(h->d_px);
   delete h;
   return EL_OK;
 }

@@ -82,6 +82,14 @@ struct BasisDev {
   uint64_t fib[EL_MAX_SITES + 3];  // fib[i] = F(i), F(1)=F(2)=1
 };
 
+// One two-site exchange channel pair (bit positions bi, bj of sites i, j):
+// J moves an excitation between the sites, A creates or removes both.
+struct ExPair {
+  int32_t bi, bj;
+  double jre, jim;   // J: amplitude conj(J) into a row with (i, j) = (g, r), J into (r, g)
+  double are, aim;   // A: amplitude A into a row with (r, r), conj(A) into (g, g)
+};
+
 struct el_ham {
   el_basis *basis = nullptr;
   int n = 0;
@@ -92,7 +100,12 @@ struct el_ham {
   std::vector<double> Vbits;   // [n*n] by bit positions, symmetric
   double *d_diagV64 = nullptr;  // per-row sum of V_ij n_i n_j (FP64)
   float *d_diagV32 = nullptr;   // FP32 copy, built on first use
-  bool complex_drive = false;
+  // exchange channels (I2 J, I3 A); empty for the Omega/delta/V model
+  std::vector<ExPair> px;
+  ExPair *d_px = nullptr;
+  bool drive_complex = false;     // Omega has an imaginary part
+  bool px_complex = false;        // some J or A has an imaginary part
+  bool complex_drive = false;     // H is complex: drive_complex || px_complex
 };
 
 // ---------------------------------------------------------------- helpers

@@ -437,6 +437,7 @@ namespace el {
 bool kpm_full_eligible(const el_ham *h, int dtype, int chunk, int mode) {
   if (mode != EL_KPM_DOUBLING) return false;
   if (h->basis->layout != EL_LAYOUT_FULL) return false;
+  if (!h->px.empty()) return false;   // sigma^x channels only
   if (h->n < 6 || h->n > 25) return false;
   if (h->complex_drive) return false;
   const int pg = (dtype == EL_F32) ? 4 : 2;

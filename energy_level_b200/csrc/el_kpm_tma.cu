@@ -611,6 +611,7 @@ namespace el {
 
 bool kpm_tma_eligible(const el_ham *h, int dtype, int chunk) {
   if (h->basis->layout != EL_LAYOUT_FULL || h->complex_drive) return false;
+  if (!h->px.empty()) return false;   // sigma^x channels only
   if (h->n < 20 || h->n > 25) return false;
   if (dtype != EL_F32 && dtype != EL_F64) return false;
   return chunk >= 1 && chunk <= 128;

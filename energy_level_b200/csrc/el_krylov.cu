@@ -127,7 +127,7 @@ extern "C" int el_kpm_moments(el_ctx *ctx, el_ham *h, int dtype, int num, int nv
                               int mode, double c, double r, double *mu_host) {
   if (!ctx || !h || !mu_host) return EL_EINVAL;
   if (dtype != EL_F32 && dtype != EL_F64) return fail(ctx, EL_EINVAL, "KPM vectors must be EL_F32 or EL_F64");
-  if (h->complex_drive) return fail(ctx, EL_EINVAL, "KPM needs a real Hamiltonian (real Omega)");
+  if (h->complex_drive) return fail(ctx, EL_EINVAL, "KPM needs a real Hamiltonian (real Omega, J and A)");
   if (num < 1 || nvec < 1) return fail(ctx, EL_EINVAL, "num and nvec must be positive integers");
   if (chunk < 1 || chunk > 256 || (chunk & (chunk - 1))) return fail(ctx, EL_EINVAL, "chunk must be a power of two <= 256");
   if (!(r > 0) || !std::isfinite(r) || !std::isfinite(c)) return fail(ctx, EL_EINVAL, "bad scaling c, r");
@@ -227,7 +227,7 @@ extern "C" int el_lanczos_ground(el_ctx *ctx, el_ham *h, int dtype, const void *
                                  void *vec_out) {
   if (!ctx || !h || !evals || !residuals) return EL_EINVAL;
   if (!el::dtype_size(dtype)) return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
-  if (h->complex_drive && !is_cplx(dtype)) return fail(ctx, EL_EINVAL, "complex Omega needs a complex dtype");
+  if (h->complex_drive && !is_cplx(dtype)) return fail(ctx, EL_EINVAL, "complex Omega, J or A needs a complex dtype");
   if (nev < 1 || nev > 2) return fail(ctx, EL_EINVAL, "nev must be 1 or 2");
   if (max_iter < 2 || max_restarts < 0) return fail(ctx, EL_EINVAL, "max_iter must be >= 2, max_restarts >= 0");
   if (!(tol > 0) || !std::isfinite(tol)) return fail(ctx, EL_EINVAL, "tol must be positive and finite");
@@ -445,7 +445,7 @@ extern "C" int el_lanczos_tridiag(el_ctx *ctx, el_ham *h, int dtype, const void 
                                   double *norm2_out, double *ortho_loss, int *converged) {
   if (!ctx || !h || !phi || !alphas || !betas || !n_out) return EL_EINVAL;
   if (!el::dtype_size(dtype)) return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
-  if (h->complex_drive && !is_cplx(dtype)) return fail(ctx, EL_EINVAL, "complex Omega needs a complex dtype");
+  if (h->complex_drive && !is_cplx(dtype)) return fail(ctx, EL_EINVAL, "complex Omega, J or A needs a complex dtype");
   if (n_krylov < 1) return fail(ctx, EL_EINVAL, "n_krylov must be positive");
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   const int64_t dim = h->basis->dim;

@@ -3,9 +3,11 @@
 Accepts the reference engine's inputs unchanged: a ``calib`` dict
 (atoms + pairs with V/J/A), per-site ``Om``/``delta``/``gamma`` arrays,
 ``terms`` and an optional HamiltonianPlan or ``basis_indices``.
-The B200 path implements the I1 model (Omega, delta, V); J/A exchange
-channels and non-Hermitian gamma are refused with ConfigConflict, never
-silently dropped (backends.py:9-18 semantics).
+The B200 path implements Omega, delta, the I1 density interaction V and the
+I2 / I3 exchange channels J / A (channels.py:91-132); non-Hermitian gamma is
+refused with ConfigConflict, never silently dropped (backends.py:9-18
+semantics).  The batched persistent solver implements the Omega/delta/V model
+only and refuses J/A the same way.
 """
 from __future__ import annotations
 
@@ -36,8 +38,11 @@ def active_terms(calib):
     return out
 
 
-def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None):
-    """Validate and flatten a calib to (n, Om complex[n], delta[n], pairs)."""
+def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None, exchange=None):
+    """Validate and flatten a calib to (n, Om complex[n], delta[n], pairs).
+
+    ``exchange``: a list that receives the (i, j, J, A) exchange channels of
+    the terms in use; None refuses a nonzero J or A with ConfigConflict."""
     atoms = (calib or {}).get('atoms') or []
     n = len(atoms)
     if n == 0:
@@ -55,10 +60,17 @@ def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None):
         i, j = int(p['i']), int(p['j'])
         if not (0 <= i < n and 0 <= j < n) or i == j:
             raise ValueError('pair (%d, %d) out of range' % (i, j))
+        amps = []
         for key, term in (('J', 'I2'), ('A', 'I3')):
-            if term in use and abs(complex(p.get(key) or 0.0)) > 0.0:
-                raise ConfigConflict('b200 backends implement the I1 model only (%s channel %s != 0)'
-                                     % (term, key), keys=('manybody.calib',))
+            a = complex(p.get(key) or 0.0) if term in use else 0j
+            if not np.isfinite(a):
+                raise ValueError('pair (%d, %d): %s must be finite' % (i, j, key))
+            if a != 0 and exchange is None:
+                raise ConfigConflict('this b200 solver implements the Omega/delta/V model only '
+                                     '(%s channel %s != 0)' % (term, key), keys=('manybody.calib',))
+            amps.append(a)
+        if exchange is not None and (amps[0] != 0 or amps[1] != 0):
+            exchange.append((i, j, amps[0], amps[1]))
         if 'I1' in use:
             V = complex(p.get('V') or 0.0)
             if V.imag != 0:
@@ -123,10 +135,21 @@ def basis_for(ctx: Context, n, plan=None, basis_indices=None, constraint=None, m
                      'the b200 backends need one of those')
 
 
+def check_number_conserving(calib, Om=None, terms=None):
+    """Refuse a fixed-excitation basis for a model that leaves it: Omega != 0
+    or a nonzero I3 pair creation A (matrix_free.py:41-48)."""
+    use = set(calib.get('terms', ()) if terms is None else terms)
+    if Om is not None and np.any(np.asarray(Om, complex) != 0):
+        raise ValueError('固定 charge_sector 要求 Omega=0')
+    if 'I3' in use and any(complex(p.get('A', 0)) != 0 for p in calib.get('pairs', ())):
+        raise ValueError('固定 charge_sector 不支持 I3 双激发项')
+
+
 def build(calib, Om=None, delta=None, gamma=None, terms=None, plan=None, basis_indices=None,
           constraint=None, device=0, ctx=None, max_states=None):
     """(ctx, basis, hamiltonian, permutation) for a reference-style model."""
-    n, Om, delta, pairs = model_arrays(calib, Om, delta, gamma, terms)
+    exchange = []
+    n, Om, delta, pairs = model_arrays(calib, Om, delta, gamma, terms, exchange=exchange)
     dev = device
     if isinstance(dev, str):
         if dev.startswith('cpu'):
@@ -135,5 +158,5 @@ def build(calib, Om=None, delta=None, gamma=None, terms=None, plan=None, basis_i
     ctx = ctx or default_context(int(dev))
     b, perm = basis_for(ctx, n, plan=plan, basis_indices=basis_indices, constraint=constraint,
                         max_states=max_states)
-    h = Hamiltonian(ctx, b, Om, delta, pairs)
+    h = Hamiltonian(ctx, b, Om, delta, pairs, exchange=exchange)
     return ctx, b, h, perm

@@ -129,6 +129,18 @@ int el_ham_create(el_ctx *ctx, el_basis *basis, const double *omega_re,
  * engine_ed.py:141-144. */
 int el_ham_set_drive(el_ctx *ctx, el_ham *ham, const double *omega_re,
                      const double *omega_im, const double *delta);
+/* Set (replace) the two-site exchange channels of ham: for each pair p the
+ * sites (pi[p], pj[p]), J = J_re + i J_im (I2: <g_i r_j|H|r_i g_j> = conj(J),
+ * <r_i g_j|H|g_i r_j> = J) and A = A_re + i A_im (I3: <r_i r_j|H|g_i g_j> = A,
+ * <g_i g_j|H|r_i r_j> = conj(A)); any of the four amplitude arrays may be
+ * NULL (zero).  Targets outside a restricted basis are dropped, as for the
+ * sigma^x channels.  A complex J or A makes H complex (complex vector dtypes
+ * only).  n_pairs = 0 removes all exchange channels.  With exchange channels
+ * every product runs the generic row kernel and KPM the generic recurrence.
+ * Replaces the I2/I3 channels of channels.py:119-131 channel_spec. */
+int el_ham_set_exchange(el_ctx *ctx, el_ham *ham, int n_pairs, const int32_t *pi,
+                        const int32_t *pj, const double *J_re, const double *J_im,
+                        const double *A_re, const double *A_im);
 /* Full diagonal d(s) = sum delta_i n_i + sum V_ij n_i n_j into a device array
  * of type dtype (EL_F32 or EL_F64).  Replaces channels.py:58-77. */
 int el_ham_diag(el_ctx *ctx, el_ham *ham, int dtype, void *out);

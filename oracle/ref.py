@@ -97,13 +97,65 @@ def diagonal(n, codes, delta, pairs):
     return d
 
 
-def hv(n, codes, omega, delta, pairs, x):
+def channel_list(n, omega, exchange=None):
+    """(selector, mask, amp) channels as channel_spec builds them
+    (channels.py:114-131): per site with Omega != 0 a g->r channel with
+    Omega/2 and an r->g channel with conj(Omega)/2; per exchange pair
+    (i, j, J, A) the I2 channels (i r, j g) -> conj(J), (i g, j r) -> J and
+    the I3 channels (i g, j g) -> A, (i r, j r) -> conj(A).  The selector
+    names the SOURCE bits; the target is source ^ mask."""
+    n = int(n)
+    om = np.asarray(omega, complex)
+    out = []
+    for i in range(n):
+        if om[i] == 0:
+            continue
+        m = np.int64(1) << (n - 1 - i)
+        out.append((((i, 0),), m, om[i] / 2.0))
+        out.append((((i, 1),), m, np.conj(om[i]) / 2.0))
+    for i, j, J, A in (exchange or ()):
+        i, j, J, A = int(i), int(j), complex(J), complex(A)
+        m = (np.int64(1) << (n - 1 - i)) ^ (np.int64(1) << (n - 1 - j))
+        if J != 0:
+            out.append((((i, 1), (j, 0)), m, np.conj(J)))
+            out.append((((i, 0), (j, 1)), m, J))
+        if A != 0:
+            out.append((((i, 0), (j, 0)), m, A))
+            out.append((((i, 1), (j, 1)), m, np.conj(A)))
+    return out
+
+
+def _channel_entries(n, codes, full, channels):
+    """(target rows, source rows, amp) per channel; targets outside a
+    restricted basis are dropped (channels.py:177-192)."""
+    if not full:
+        order = np.argsort(codes)
+        sc = codes[order]
+    for selector, mask, amp in channels:
+        sel = np.ones(len(codes), bool)
+        for site, bit in selector:
+            sel &= ((codes >> (n - 1 - int(site))) & 1) == int(bit)
+        src = np.flatnonzero(sel)
+        targets = codes[src] ^ mask
+        if full:
+            yield targets, src, amp
+            continue
+        pos = np.searchsorted(sc, targets)
+        ok = pos < len(sc)
+        ok[ok] &= sc[pos[ok]] == targets[ok]
+        yield order[pos[ok]], src[ok], amp
+
+
+def _is_complex(omega, exchange):
+    return bool(np.any(np.asarray(omega).imag != 0)) or any(
+        complex(e[2]).imag != 0 or complex(e[3]).imag != 0 for e in (exchange or ()))
+
+
+def hv(n, codes, omega, delta, pairs, x, exchange=None):
     """y = H x on the full (codes=None) or restricted basis.
 
-    Follows ChannelKernel.matvec (channels.py:210-221) with the channel list of
-    channel_spec (channels.py:114-118): a source with site i in |g> feeds the
-    target code^mask with Omega_i/2, a source in |r> with conj(Omega_i)/2;
-    targets outside a restricted basis are dropped (channels.py:177-192)."""
+    Follows ChannelKernel.matvec (channels.py:210-221): the diagonal, then
+    every channel of channel_list scatters amp * x[source] into its target."""
     n = int(n)
     full = codes is None
     codes = np.arange(1 << n, dtype=np.int64) if full else np.asarray(codes, np.int64)
@@ -111,36 +163,14 @@ def hv(n, codes, omega, delta, pairs, x):
     vec = x.ndim == 1
     X = x.reshape(len(codes), -1)
     d = diagonal(n, codes, delta, pairs)
-    cplx = np.iscomplexobj(X) or np.any(np.asarray(omega).imag != 0)
+    cplx = np.iscomplexobj(X) or _is_complex(omega, exchange)
     Y = (d[:, None] * X).astype(complex if cplx else X.dtype)
-    if not full:
-        order = np.argsort(codes)
-        sc = codes[order]
-    om = np.asarray(omega, complex)
-    for i in range(n):
-        if om[i] == 0:
-            continue
-        mask = np.int64(1) << (n - 1 - i)
-        bit = (codes >> (n - 1 - i)) & 1
-        targets = codes ^ mask
-        if full:
-            loc = targets
-            ok = np.ones(len(codes), bool)
-        else:
-            pos = np.searchsorted(sc, targets)
-            ok = pos < len(sc)
-            ok[ok] &= sc[pos[ok]] == targets[ok]
-            loc = np.zeros(len(codes), np.int64)
-            loc[ok] = order[pos[ok]]
-        amp = np.where(bit == 0, om[i] / 2.0, np.conj(om[i]) / 2.0)
-        if not cplx:
-            amp = amp.real
-        src = np.flatnonzero(ok)
-        np.add.at(Y, loc[src], amp[src, None] * X[src])
+    for loc, src, amp in _channel_entries(n, codes, full, channel_list(n, omega, exchange)):
+        np.add.at(Y, loc, (amp if cplx else amp.real) * X[src])
     return Y.reshape(x.shape) if vec else Y
 
 
-def sparse_h(n, codes, omega, delta, pairs):
+def sparse_h(n, codes, omega, delta, pairs, exchange=None):
     """CSR H from the same channel list as hv (the reference assembles its CSR
     in assemble.py:277-393 build_H_sparse; used here for the larger CPU
     baseline samples, where a dense matrix does not fit)."""
@@ -150,42 +180,21 @@ def sparse_h(n, codes, omega, delta, pairs):
     codes = np.arange(1 << n, dtype=np.int64) if full else np.asarray(codes, np.int64)
     dim = len(codes)
     d = diagonal(n, codes, delta, pairs)
-    om = np.asarray(omega, complex)
-    cplx = np.any(om.imag != 0)
+    cplx = _is_complex(omega, exchange)
     rows, cols, vals = [np.arange(dim)], [np.arange(dim)], [d.astype(complex if cplx else float)]
-    if not full:
-        order = np.argsort(codes)
-        sc = codes[order]
-    for i in range(n):
-        if om[i] == 0:
-            continue
-        mask = np.int64(1) << (n - 1 - i)
-        bit = (codes >> (n - 1 - i)) & 1
-        targets = codes ^ mask
-        if full:
-            loc = targets
-            ok = np.ones(dim, bool)
-        else:
-            pos = np.searchsorted(sc, targets)
-            ok = pos < dim
-            ok[ok] &= sc[pos[ok]] == targets[ok]
-            loc = np.zeros(dim, np.int64)
-            loc[ok] = order[pos[ok]]
-        amp = np.where(bit == 0, om[i] / 2.0, np.conj(om[i]) / 2.0)
-        src = np.flatnonzero(ok)
-        rows.append(loc[src])
+    for loc, src, amp in _channel_entries(n, codes, full, channel_list(n, omega, exchange)):
+        rows.append(loc)
         cols.append(src)
-        vals.append(amp[src] if cplx else amp[src].real)
+        vals.append(np.full(len(src), amp if cplx else amp.real))
     return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
                          shape=(dim, dim))
 
 
-def dense_h(n, codes, omega, delta, pairs):
+def dense_h(n, codes, omega, delta, pairs, exchange=None):
     """Dense H by applying hv to unit vectors (small systems only)."""
     dim = (1 << n) if codes is None else len(codes)
-    cplx = np.any(np.asarray(omega).imag != 0)
-    E = np.eye(dim, dtype=complex if cplx else float)
-    return hv(n, codes, omega, delta, pairs, E)
+    E = np.eye(dim, dtype=complex if _is_complex(omega, exchange) else float)
+    return hv(n, codes, omega, delta, pairs, E, exchange=exchange)
 
 
 # ------------------------------------------------------------------- KPM
@@ -283,7 +292,7 @@ def segment_drive(t, segments, n):
     return om * np.exp(1j * ph), de
 
 
-def evolve_segments(n, codes, pairs, segments, psi0, t_grid):
+def evolve_segments(n, codes, pairs, segments, psi0, t_grid, exchange=None):
     """Piecewise-constant exact propagation (engine_ed.py:130-147): for each
     output interval and each drive piece, psi <- expm_multiply(-i CONV dt H)."""
     import scipy.sparse as sp
@@ -297,8 +306,8 @@ def evolve_segments(n, codes, pairs, segments, psi0, t_grid):
             om, de = segment_drive(0.5 * (a + b), segments, n)
             key = (tuple(om), tuple(de))
             if key not in cache:
-                cache[key] = (sp.csr_matrix(dense_h(n, codes, om, de, pairs)) if len(psi) <= 4096
-                              else sparse_h(n, codes, om, de, pairs))
+                cache[key] = (sp.csr_matrix(dense_h(n, codes, om, de, pairs, exchange=exchange))
+                              if len(psi) <= 4096 else sparse_h(n, codes, om, de, pairs, exchange=exchange))
             psi = expm_multiply((-1j * CONV * (b - a)) * cache[key], psi)
         out.append(psi.copy())
     return out
@@ -309,6 +318,32 @@ def site_occupations(n, codes, psi):
     codes = np.arange(1 << n) if codes is None else codes
     p = np.abs(np.asarray(psi)) ** 2
     return basis_bits(n, codes).astype(float) @ p
+
+
+def corr_matrix(bits, p):
+    """C_ij = <n_i n_j> - <n_i><n_j> with weights p (observables.py:40-47)."""
+    bits = np.asarray(bits, float)
+    ni = bits @ p
+    return (bits * p) @ bits.T - np.outer(ni, ni)
+
+
+# ------------------------------------------------------------ sector scan
+
+def sector_scan(n, delta, pairs, exchange, sectors=None):
+    """Per fixed-excitation sector the lowest two eigenvalues of H restricted
+    to it, Omega = 0 (sector_scan.py:61-132; dense eigh per sector replaces
+    its per-sector Krylov solve).  Returns (E0, best sector, rows) with rows
+    (k, dim, E0, gap)."""
+    n = int(n)
+    ks = list(range(n + 1)) if sectors is None else [int(k) for k in sectors]
+    rows = []
+    for k in ks:
+        codes = number_sector_basis(n, k)
+        H = dense_h(n, codes, np.zeros(n), delta, pairs, exchange=exchange)
+        w = np.linalg.eigvalsh(H)
+        rows.append((k, len(codes), float(w[0]), float(w[1] - w[0]) if len(w) > 1 else 0.0))
+    best = min(rows, key=lambda r: r[2])
+    return best[2], best[0], rows
 
 
 # ---------------------------------------------------------------- spectrum

@@ -242,6 +242,100 @@ def ramp_fixture(ref_root: str) -> None:
     print("ramp fixture written to", HERE)
 
 
+def exchange_fixture(ref_root: str) -> None:
+    """Exchange channels (I2 J, I3 A; channels.py:91-132):
+    hamiltonian_linear_operator (matrix_free.py:51-62) on the full basis with
+    complex J/A/Omega, on a fixed-excitation sector and on a blockade chain;
+    scan_ground_sectors (sector_scan.py:61-132) of a dipolar XY chain; and a
+    fixed-sector ground state through solve_equilibrium (eq_route.py:575-612)."""
+    sys.path.insert(0, ref_root)
+    from src.core.manybody import basis as rbasis                       # basis.py
+    from src.core.manybody import matrix_free as rmf                    # matrix_free.py
+    from src.core.manybody import sector_scan as rscan                  # sector_scan.py
+    from src.core.manybody import eq_route as rroute                    # eq_route.py
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from energy_level_b200 import configs
+    rng = np.random.default_rng(20261204)
+    out = {}
+
+    def pairs_of(n, jfun, afun, vscale):
+        pos = configs.chain_positions(n, a=5.5, jitter=rng.uniform(-0.3, 0.3, n))
+        ps = []
+        for i in range(n):
+            for j in range(i + 1, n):
+                r = float(np.linalg.norm(pos[j] - pos[i]))
+                ps.append({'i': i, 'j': j, 'V': vscale * configs.C6_70S / r ** 6,
+                           'J': jfun(i, j, r), 'A': afun(i, j, r)})
+        return {'atoms': [{'id': i, 'pos': [float(x) for x in p]} for i, p in enumerate(pos)],
+                'pairs': ps}
+
+    cases = {
+        # full basis, every channel complex
+        "full7": (7, None, ['I1', 'I2', 'I3'],
+                  lambda i, j, r: (0.6 - 0.25j) * (5.5 / r) ** 3,
+                  lambda i, j, r: (0.05 + 0.03j) if j == i + 1 else 0.0,
+                  rng.uniform(0.5, 2.0, 7) * np.exp(1j * rng.uniform(0, 1, 7)), 1e-2),
+        # fixed-excitation sector, real J
+        "charge10_4": (10, ('charge', 4), ['I1', 'I2'],
+                       lambda i, j, r: -0.7 * (5.5 / r) ** 3, lambda i, j, r: 0.0,
+                       np.zeros(10), 1e-3),
+        # fixed-excitation sector, complex J
+        "charge9_3c": (9, ('charge', 3), ['I1', 'I2'],
+                       lambda i, j, r: (0.4 + 0.3j) * (5.5 / r) ** 3, lambda i, j, r: 0.0,
+                       np.zeros(9), 1e-3),
+        # blockade chain: J/A targets outside the sector are dropped
+        "chain10": (10, ('blockade', configs.chain_edges(10)), ['I1', 'I2', 'I3'],
+                    lambda i, j, r: 0.5 * (5.5 / r) ** 3,
+                    lambda i, j, r: 0.2 if j == i + 2 else 0.0,
+                    rng.uniform(0.5, 2.0, 10), 1.0),
+    }
+    for name, (n, basis, use, jf, af, om, vs) in cases.items():
+        calib = pairs_of(n, jf, af, vs)
+        de = rng.uniform(-2.0, 2.0, n)
+        if basis is None:
+            idx = None
+        elif basis[0] == 'charge':
+            idx = np.asarray(rmf.number_sector_basis(n, basis[1]), np.int64)
+        else:
+            idx = np.asarray(rbasis.independent_states(n, basis[1]), np.int64)
+        op = rmf.hamiltonian_linear_operator(calib, Om=om, delta=de, terms=use, basis_indices=idx)
+        dim = op.shape[0]
+        x = rng.normal(size=dim) + 1j * rng.normal(size=dim)
+        out["x_" + name] = x
+        out["y_" + name] = op @ x
+        out["n_" + name] = np.int64(n)
+        out["om_" + name] = np.asarray(om, complex)
+        out["de_" + name] = de
+        out["codes_" + name] = np.arange(1 << n, dtype=np.int64) if idx is None else idx
+        out["pairs_" + name] = np.asarray([[p['i'], p['j']] for p in calib['pairs']], np.int64)
+        out["V_" + name] = np.asarray([p['V'] for p in calib['pairs']], float)
+        out["J_" + name] = np.asarray([complex(p['J']) for p in calib['pairs']], complex)
+        out["A_" + name] = np.asarray([complex(p['A']) for p in calib['pairs']], complex)
+        out["terms_" + name] = np.asarray(use)
+
+    # sector scan of a dipolar XY chain (N = 10, Omega = 0)
+    xy = configs.xy_chain(10)
+    r = rscan.scan_ground_sectors(xy['calib'], delta=xy['delta'], Om=np.zeros(10),
+                                  terms=['I1', 'I2'], device='cpu', dense_max=64)
+    out["scan_E0"] = np.float64(r['E0'])
+    out["scan_sector"] = np.int64(r['sector'])
+    out["scan_sector_E0"] = np.asarray([row['E0'] for row in r['per_sector']], float)
+    out["scan_sector_gap"] = np.asarray([row['gap'] for row in r['per_sector']], float)
+    out["scan_sector_dim"] = np.asarray([row['dim'] for row in r['per_sector']], np.int64)
+    out["scan_dimension_sum"] = np.int64(r['dimension_sum'])
+
+    # fixed-sector ground state through the equilibrium route (ED backend)
+    g = rroute.solve_equilibrium({'calib': xy['calib'], 'Om': np.zeros(10), 'delta': xy['delta'],
+                                  'terms': ['I1', 'I2']}, want='gs', backend='ed', sector=5)
+    out["gs5_E0"] = np.float64(g['E0'])
+    out["gs5_gap"] = np.float64(g['gap'])
+    out["gs5_n_atom"] = np.asarray(g['n_atom'], float)
+    out["gs5_corr"] = np.asarray(g['corr'], float)
+    out["gs5_sector_idx"] = np.asarray(g['sector_idx'], np.int64)
+    np.savez_compressed(os.path.join(HERE, "exchange.npz"), **out)
+    print("exchange fixture written to", HERE)
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     which = sys.argv[2] if len(sys.argv) > 2 else "all"
@@ -249,7 +343,10 @@ if __name__ == "__main__":
         spectrum_fixture(root)
     elif which == "ramp":
         ramp_fixture(root)
+    elif which == "exchange":
+        exchange_fixture(root)
     else:
         main(root)
         spectrum_fixture(root)
         ramp_fixture(root)
+        exchange_fixture(root)

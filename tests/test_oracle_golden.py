@@ -135,3 +135,70 @@ def test_evolution_matches_reference():
     assert np.max(np.abs(states[-1] - g["psi_final"])) < 1e-10
     pops = np.array([ref.site_occupations(n, codes, s) for s in states])
     assert np.max(np.abs(pops - g["pops_atom"])) < 1e-10
+
+
+def exchange_case(g, name):
+    """(n, codes, om, de, V pairs, exchange) of one exchange fixture case."""
+    n = int(g["n_" + name])
+    terms = set(str(t) for t in g["terms_" + name])
+    ij = g["pairs_" + name]
+    pairs = [(int(i), int(j), float(v)) for (i, j), v in zip(ij, g["V_" + name])] if "I1" in terms else []
+    ex = []
+    for (i, j), J, A in zip(ij, g["J_" + name], g["A_" + name]):
+        J = complex(J) if "I2" in terms else 0j
+        A = complex(A) if "I3" in terms else 0j
+        if J != 0 or A != 0:
+            ex.append((int(i), int(j), J, A))
+    codes = g["codes_" + name]
+    full = len(codes) == (1 << n)
+    return n, (None if full else codes), g["om_" + name], g["de_" + name], pairs, ex
+
+
+@pytest.mark.parametrize("name", ["full7", "charge10_4", "charge9_3c", "chain10"])
+def test_exchange_hv_matches_reference(name):
+    g = load("exchange")
+    n, codes, om, de, pairs, ex = exchange_case(g, name)
+    y = ref.hv(n, codes, om, de, pairs, g["x_" + name], exchange=ex)
+    assert np.max(np.abs(y - g["y_" + name])) < 1e-12 * max(1.0, np.abs(g["y_" + name]).max())
+
+
+def test_exchange_hermitian_and_sparse_agree():
+    g = load("exchange")
+    n, codes, om, de, pairs, ex = exchange_case(g, "full7")
+    H = ref.dense_h(n, codes, om, de, pairs, exchange=ex)
+    assert np.allclose(H, H.conj().T, atol=1e-14)
+    S = ref.sparse_h(n, codes, om, de, pairs, exchange=ex).toarray()
+    assert np.max(np.abs(S - H)) < 1e-14
+
+
+def test_sector_scan_matches_reference():
+    from energy_level_b200 import configs
+    g = load("exchange")
+    xy = configs.xy_chain(10)
+    pairs = [(p['i'], p['j'], p['V']) for p in xy['calib']['pairs']]
+    ex = [(p['i'], p['j'], p['J'], 0.0) for p in xy['calib']['pairs']]
+    E0, k, rows = ref.sector_scan(10, xy['delta'], pairs, ex)
+    assert k == int(g["scan_sector"])
+    assert abs(E0 - float(g["scan_E0"])) < 1e-10
+    assert np.allclose([r[2] for r in rows], g["scan_sector_E0"], atol=1e-10, rtol=0)
+    assert np.array_equal([r[1] for r in rows], g["scan_sector_dim"])
+    assert sum(r[1] for r in rows) == int(g["scan_dimension_sum"]) == 1 << 10
+    # the lowest sector energy is the full-basis ground energy
+    Hf = ref.dense_h(10, None, np.zeros(10), xy['delta'], pairs, exchange=ex)
+    assert abs(np.linalg.eigvalsh(Hf)[0] - E0) < 1e-10
+
+
+def test_sector_ground_corr_matches_reference():
+    from energy_level_b200 import configs
+    g = load("exchange")
+    xy = configs.xy_chain(10)
+    pairs = [(p['i'], p['j'], p['V']) for p in xy['calib']['pairs']]
+    ex = [(p['i'], p['j'], p['J'], 0.0) for p in xy['calib']['pairs']]
+    codes = ref.number_sector_basis(10, 5)
+    assert np.array_equal(codes, g["gs5_sector_idx"])
+    w, V = np.linalg.eigh(ref.dense_h(10, codes, np.zeros(10), xy['delta'], pairs, exchange=ex))
+    assert abs(w[0] - float(g["gs5_E0"])) < 1e-10
+    p = np.abs(V[:, 0]) ** 2
+    bits = ref.basis_bits(10, codes)
+    assert np.allclose(bits @ p, g["gs5_n_atom"], atol=1e-9)
+    assert np.allclose(ref.corr_matrix(bits, p), g["gs5_corr"], atol=1e-9)
