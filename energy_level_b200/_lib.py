@@ -69,6 +69,8 @@ PROTOTYPES = {
     "el_observables": (C.c_int, [_vp, _vp, C.c_int, _vp, _dp, _dp]),
     "el_lanczos_tridiag": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, C.c_int, _dp, _dp,
                                      C.POINTER(C.c_int), _dp, _dp, C.POINTER(C.c_int)]),
+    "el_spin_observables": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _dp, _dp, _dp, _dp, _dp]),
+    "el_pauli_expect": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_char_p, _dp]),
     "el_observables_noalloc": (C.c_int, [_vp, _vp, C.c_int, _vp, _dp, _dp]),
     "el_adjoint_pulse": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _vp, _vp, _vp,
                                    C.c_double, _dp, _dp, _dp, _vp]),

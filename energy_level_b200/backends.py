@@ -51,7 +51,7 @@ TIME_BACKENDS = {
                              options=(('memory_budget_mb', 'memory_budget_mb'), ('dtype', 'dtype'),
                                       ('device', 'device')),
                              segments=True, projected=True, gamma=False, return_state=True,
-                             algorithm='chebyshev'),
+                             pauli='full', algorithm='chebyshev'),
 }
 
 
@@ -80,7 +80,7 @@ def validate_time_capabilities(name, *, segments=None, plan=None, gamma=None, re
     """Refuse what b200-cheb does not implement, with ConfigConflict keys
     (backends.py:182-230 semantics)."""
     b = TIME_BACKENDS[normalize_time_backend(name)]
-    if pauli_strings:
+    if pauli_strings and not b.pauli:
         raise ConfigConflict('%s 不提供 Pauli 串观测' % name, keys=('manybody.pauli_strings',))
     if segments and not b.segments:
         raise ConfigConflict('%s 尚不支持 drive_segments' % name, keys=('manybody.drive_segments',))

@@ -124,6 +124,60 @@ def observables(ham: Hamiltonian, psi):
     return ns, float(nrm.value)
 
 
+def spin_observables(ham: Hamiltonian, psi, pairs=()):
+    """Device spin observables of a state (el_spin_observables).
+
+    Returns dict(n, norm, sm, nn, xy): <n_i>, squared norm, <sigma-_i>
+    (complex) per site, and for each (i, j) of ``pairs`` <n_i n_j> and
+    <sigma+_i sigma-_j> (complex)."""
+    torch = _torch()
+    dt = {torch.float32: _lib.EL_F32, torch.float64: _lib.EL_F64,
+          torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}[psi.dtype]
+    psi = psi.contiguous()
+    n = ham.n
+    pr = np.asarray(list(pairs), dtype=np.int32).reshape(-1, 2)
+    pi = np.ascontiguousarray(pr[:, 0])
+    pj = np.ascontiguousarray(pr[:, 1])
+    k = len(pr)
+    ns = np.zeros(n)
+    sm = np.zeros(2 * n)
+    nn = np.zeros(max(k, 1))
+    xy = np.zeros(2 * max(k, 1))
+    nrm = C.c_double()
+    ham.ctx.call('el_spin_observables', ham.handle, C.c_int(dt), C.c_void_p(psi.data_ptr()), C.c_int(k),
+                 C.c_void_p(pi.ctypes.data) if k else None, C.c_void_p(pj.ctypes.data) if k else None,
+                 _lib.dptr(ns), C.byref(nrm), _lib.dptr(sm), _lib.dptr(nn) if k else None,
+                 _lib.dptr(xy) if k else None)
+    return dict(n=ns, norm=float(nrm.value), sm=sm[0::2] + 1j * sm[1::2],
+                nn=nn[:k], xy=xy[0:2 * k:2] + 1j * xy[1:2 * k:2])
+
+
+def pauli_expect(ham: Hamiltonian, psi, specs):
+    """<psi|P|psi> (complex) of each Pauli string in ``specs``
+    ([{'label', 'terms': [(site, axis), ...]}], axes 'x'/'y'/'z'), on the device
+    (el_pauli_expect)."""
+    torch = _torch()
+    dt = {torch.float32: _lib.EL_F32, torch.float64: _lib.EL_F64,
+          torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}[psi.dtype]
+    specs = list(specs or [])
+    if not specs:
+        return np.zeros(0, complex)
+    psi = psi.contiguous()
+    offs, sites, axes = [0], [], []
+    for sp in specs:
+        for site, ax in sp['terms']:
+            sites.append(int(site))
+            axes.append(str(ax))
+        offs.append(len(sites))
+    offs = np.ascontiguousarray(offs, dtype=np.int32)
+    sites = np.ascontiguousarray(sites, dtype=np.int32)
+    out = np.zeros(2 * len(specs))
+    ham.ctx.call('el_pauli_expect', ham.handle, C.c_int(dt), C.c_void_p(psi.data_ptr()), C.c_int(len(specs)),
+                 C.c_void_p(offs.ctypes.data), C.c_void_p(sites.ctypes.data),
+                 ''.join(axes).encode('ascii'), _lib.dptr(out))
+    return out[0::2] + 1j * out[1::2]
+
+
 def observables_noalloc(ham: Hamiltonian, psi):
     """observables() through el_observables_noalloc: no device allocation,
     static scratch shared per device (at most 40 sites; calls on one device

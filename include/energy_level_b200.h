@@ -260,6 +260,28 @@ int el_adjoint_pulse(el_ctx *ctx, el_ham *ham, int dtype, int K, const double *t
  * the bits @ |psi|^2 reduction of engine_ed.py:259-263 (_reduce). */
 int el_observables(el_ctx *ctx, el_ham *ham, int dtype, const void *psi,
                    double *n_site_host, double *norm_host);
+/* Spin observables of a device state psi (dtype EL_*): norm, <n_i> and
+ * <sigma-_i> (complex, re/im interleaved in sigma_minus[2n]) for every site,
+ * and for each of n_pairs site pairs (pi[p], pj[p]), i != j in any order,
+ * <n_i n_j> (nn[p]) and <sigma+_i sigma-_j> (complex, xy[2p], xy[2p+1]).  On
+ * a restricted basis flip targets outside it drop out.  Any output pointer
+ * may be NULL; n_pairs may be 0.  FP64 sums in a fixed order.  Replaces
+ * observables.py:117-205 spin_observables / spin_observables_basis and the
+ * <n_i n_j> of observables.py:40-47 corr_matrix, evaluated per output time in
+ * engine_ed.py:259-281. */
+int el_spin_observables(el_ctx *ctx, el_ham *ham, int dtype, const void *psi,
+                        int n_pairs, const int32_t *pi, const int32_t *pj,
+                        double *n_site, double *norm, double *sigma_minus,
+                        double *nn, double *xy);
+/* Expectations <psi|P_q|psi> of n_strings Pauli strings (complex, re/im
+ * interleaved in out_host[2 n_strings]).  String q is the product over
+ * k in [offsets[q], offsets[q+1]) of sigma^{axes[k]} on site sites[k]
+ * (axes 'x', 'y', 'z'; distinct sites; standard Pauli matrices in the
+ * (|g>, |r>) basis).  On a restricted basis, targets outside it drop out.
+ * Replaces observables.py:486-622 PauliPlan.expect (full and basis kinds). */
+int el_pauli_expect(el_ctx *ctx, el_ham *ham, int dtype, const void *psi, int n_strings,
+                    const int32_t *offsets, const int32_t *sites, const char *axes,
+                    double *out_host);
 /* el_observables without any allocation.  This entry point has no
  * counterpart in the reference; it exists for callers that must not allocate
  * device memory once they are running, e.g. an evolution driver measuring

@@ -327,6 +327,95 @@ def corr_matrix(bits, p):
     return (bits * p) @ bits.T - np.outer(ni, ni)
 
 
+def spin_observables(n, codes, psi):
+    """sx, sy, sz, sp, sm, phase per site and xy[i, j] = <sigma+_i sigma-_j>
+    on the full (codes=None) or a restricted basis (observables.py:117-205;
+    flip targets outside a restricted basis drop out)."""
+    n = int(n)
+    v = np.asarray(psi, complex).reshape(-1)
+    codes = np.arange(1 << n, dtype=np.int64) if codes is None else np.asarray(codes, np.int64)
+    pos = {int(c): k for k, c in enumerate(codes)}
+    p = np.abs(v) ** 2
+    bits = basis_bits(n, codes).astype(bool)
+    sz = np.zeros(n)
+    sm = np.zeros(n, complex)
+    for i in range(n):
+        m = 1 << (n - 1 - i)
+        sz[i] = p[~bits[i]].sum() - p[bits[i]].sum()
+        for k in np.flatnonzero(~bits[i]):
+            t = pos.get(int(codes[k]) | m)
+            if t is not None:
+                sm[i] += np.conj(v[k]) * v[t]
+    xy = np.zeros((n, n), complex)
+    for i in range(n):
+        mi = 1 << (n - 1 - i)
+        xy[i, i] = p[bits[i]].sum()
+        for j in range(n):
+            if j == i:
+                continue
+            mj = 1 << (n - 1 - j)
+            for k in np.flatnonzero(~bits[i] & bits[j]):
+                t = pos.get((int(codes[k]) | mi) ^ mj)
+                if t is not None:
+                    xy[i, j] += np.conj(v[t]) * v[k]
+    phase = np.angle(sm)
+    phase[np.abs(sm) < 1e-14] = np.nan
+    return dict(sx=2 * sm.real, sy=2 * sm.imag, sz=sz, sp=np.conj(sm), sm=sm, phase=phase, xy_corr=xy)
+
+
+def pauli_expect(n, codes, psi, terms):
+    """<psi|P|psi> for P = prod sigma^{axis} on distinct sites, standard
+    Pauli matrices in the (|g>, |r>) basis; on a restricted basis targets
+    outside it drop out (observables.py:546-622 PauliPlan, basis form)."""
+    n = int(n)
+    v = np.asarray(psi, complex).reshape(-1)
+    codes = np.arange(1 << n, dtype=np.int64) if codes is None else np.asarray(codes, np.int64)
+    pos = {int(c): k for k, c in enumerate(codes)}
+    t = codes.copy()
+    ph = np.ones(len(codes), complex)
+    for site, axis in terms:
+        m = np.int64(1) << (n - 1 - int(site))
+        bit = (codes & m) != 0
+        if axis == 'z':
+            ph *= np.where(bit, -1.0, 1.0)
+        elif axis == 'y':
+            ph *= np.where(bit, -1j, 1j)
+        if axis != 'z':
+            t = t ^ m
+    total = 0j
+    for k in range(len(codes)):
+        q = pos.get(int(t[k]))
+        if q is not None:
+            total += np.conj(v[q]) * ph[k] * v[k]
+    return total
+
+
+def entropy_cut(n, codes, psi, cut, max_entries=1 << 20):
+    """Bipartite von Neumann entropy (nat) between the first `cut` sites and
+    the rest: full basis as observables.py:50-80 entropy_at_cut, restricted
+    basis on the occupied Schmidt rows/columns as observables.py:89-114
+    entropy_in_basis (None beyond max_entries)."""
+    n, cut = int(n), int(cut)
+    v = np.asarray(psi, complex).reshape(-1)
+    if codes is None:
+        sv = np.linalg.svd(v.reshape(1 << cut, 1 << (n - cut)), compute_uv=False)
+        w = sv ** 2
+        w = w[w > 1e-15]
+        return float(-np.sum(w * np.log(w))) if w.size else 0.0
+    codes = np.asarray(codes, np.int64)
+    _, li = np.unique(codes >> (n - cut), return_inverse=True)
+    _, ri = np.unique(codes & ((1 << (n - cut)) - 1), return_inverse=True)
+    shape = (int(li.max()) + 1, int(ri.max()) + 1)
+    if shape[0] * shape[1] > max_entries:
+        return None
+    M = np.zeros(shape, complex)
+    M[li, ri] = v
+    w = np.linalg.svd(M, compute_uv=False) ** 2
+    w = w / w.sum()
+    w = w[w > 0]
+    return float(-np.sum(w * np.log(w)))
+
+
 # ------------------------------------------------------------ sector scan
 
 def sector_scan(n, delta, pairs, exchange, sectors=None):

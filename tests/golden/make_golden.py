@@ -336,6 +336,86 @@ def exchange_fixture(ref_root: str) -> None:
     print("exchange fixture written to", HERE)
 
 
+def observables_fixture(ref_root: str) -> None:
+    """Spin observables and entropies: observables.spin_observables /
+    spin_observables_basis (observables.py:117-205), entropy_at_cut /
+    entropy_in_basis (observables.py:50-114), corr_matrix (:40-47), and two
+    evolutions with every observable on (engine_ed.py:153-372): a full-basis
+    XY + drive quench with segments and a projected blockade ramp."""
+    sys.path.insert(0, ref_root)
+    from src.core.manybody import observables as robs                   # observables.py
+    from src.core.manybody import engine_ed as red                      # engine_ed.py
+    from src.core.manybody import basis as rbasis                       # basis.py
+    from src.core.manybody import hamiltonian_plan as rplan             # hamiltonian_plan.py
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from energy_level_b200 import configs
+    rng = np.random.default_rng(20261205)
+    out = {}
+    # single states
+    n = 7
+    psi = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    psi /= np.linalg.norm(psi)
+    ob = robs.spin_observables(psi, n)
+    out["full_psi"] = psi
+    for k in ("sx", "sy", "sz", "sp", "sm", "xy_corr", "phase"):
+        out["full_" + k] = np.asarray(ob[k])
+    out["full_S3"] = np.float64(robs.entropy_at_cut(psi, n, 3))
+    nb = 10
+    states = np.asarray(rbasis.independent_states(nb, configs.chain_edges(nb)), np.int64)
+    q = rng.normal(size=states.size) + 1j * rng.normal(size=states.size)
+    q /= np.linalg.norm(q)
+    ob = robs.spin_observables_basis(q, states, nb)
+    out["basis_psi"] = q
+    out["basis_states"] = states
+    for k in ("sx", "sy", "sz", "sp", "sm", "xy_corr", "phase"):
+        out["basis_" + k] = np.asarray(ob[k])
+    out["basis_S5"] = np.float64(robs.entropy_in_basis(q, states, nb, 5))
+    bits = np.asarray([((states >> (nb - 1 - i)) & 1) for i in range(nb)], float)
+    out["basis_corr"] = robs.corr_matrix(bits, np.abs(q) ** 2)
+
+    # evolution 1: full basis, XY exchange + drive, three segments
+    n = 6
+    xy = configs.xy_chain(n, seed=21)
+    segs = [{"t0": 0.0, "Om": np.full(n, 0.8), "delta": xy["delta"]},
+            {"t0": 150.0, "Om": np.full(n, 1.2), "delta": xy["delta"] - 0.5},
+            {"t0": 300.0, "Om": np.full(n, 0.4), "delta": xy["delta"] + 0.3}]
+    t = np.linspace(0.0, 400.0, 6)
+    r = red.evolve_manybody(xy["calib"], psi0="rg" * (n // 2), t_grid=t, segments=segs, terms=["I1", "I2"],
+                            record_psi=True, link_pairs=[(0, 1), (2, 4)])
+    out["ev1_n"] = np.int64(n)
+    out["ev1_t"] = t
+    out["ev1_seg_t0"] = np.asarray([sg["t0"] for sg in segs])
+    out["ev1_seg_om"] = np.asarray([sg["Om"] for sg in segs])
+    out["ev1_seg_de"] = np.asarray([sg["delta"] for sg in segs])
+    for k in ("pops_atom", "S", "corr", "norms", "pops", "basis_probabilities", "psi_amp"):
+        out["ev1_" + k] = np.asarray(r[k])
+    for k in ("sx", "sy", "sz", "sp", "sm", "phase", "xy_corr", "link_corr"):
+        out["ev1_obs_" + k] = np.asarray(r["observables"][k])
+
+    # evolution 2: projected blockade chain, two segments
+    n = 10
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+    segs = [{"t0": 0.0, "Om": np.full(n, 2.0), "delta": np.full(n, 3.0)},
+            {"t0": 100.0, "Om": np.full(n, 1.5), "delta": np.full(n, -2.0)}]
+    plan = rplan.build_plan(calib, Om=np.full(n, 2.0), delta=np.zeros(n), terms=["I1"],
+                            constraint={"kind": "blockade", "edges": configs.chain_edges(n)})
+    t = np.linspace(0.0, 200.0, 5)
+    r = red.evolve_manybody(calib, psi0="g" * n, t_grid=t, segments=segs, plan=plan, terms=["I1"],
+                            record_psi=True)
+    out["ev2_n"] = np.int64(n)
+    out["ev2_t"] = t
+    out["ev2_seg_t0"] = np.asarray([sg["t0"] for sg in segs])
+    out["ev2_seg_om"] = np.asarray([sg["Om"] for sg in segs])
+    out["ev2_seg_de"] = np.asarray([sg["delta"] for sg in segs])
+    out["ev2_states"] = np.asarray(r["basis_states"], np.int64)
+    for k in ("pops_atom", "S", "corr", "norms", "pops", "basis_probabilities", "psi_amp"):
+        out["ev2_" + k] = np.asarray(r[k])
+    for k in ("sx", "sy", "sz", "sp", "sm", "phase", "xy_corr"):
+        out["ev2_obs_" + k] = np.asarray(r["observables"][k])
+    np.savez_compressed(os.path.join(HERE, "observables.npz"), **out)
+    print("observables fixture written to", HERE)
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     which = sys.argv[2] if len(sys.argv) > 2 else "all"
@@ -345,8 +425,11 @@ if __name__ == "__main__":
         ramp_fixture(root)
     elif which == "exchange":
         exchange_fixture(root)
+    elif which == "observables":
+        observables_fixture(root)
     else:
         main(root)
         spectrum_fixture(root)
         ramp_fixture(root)
         exchange_fixture(root)
+        observables_fixture(root)

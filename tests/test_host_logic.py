@@ -28,8 +28,9 @@ def test_capability_refusals_are_config_conflicts():
     with pytest.raises(model.ConfigConflict) as e:
         backends.validate_time_capabilities("b200-cheb", gamma=[0.1, 0.0])
     assert e.value.keys == ("manybody.gamma_mhz",)
-    with pytest.raises(model.ConfigConflict):
-        backends.validate_time_capabilities("b200-cheb", pauli_strings=[{"label": "x"}])
+    # Pauli strings are evaluated on the device ('full' capability, as the ed engine)
+    backends.validate_time_capabilities("b200-cheb", pauli_strings=[{"label": "x"}])
+    assert backends.TIME_BACKENDS["b200-cheb"].pauli == "full"
     with pytest.raises(ValueError):
         backends.validate_time_capabilities("b200-cheb", psi0="ground")
     backends.validate_time_capabilities("b200-cheb", segments=[{"t0": 0}], plan={"projected": True})

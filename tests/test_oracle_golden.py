@@ -202,3 +202,24 @@ def test_sector_ground_corr_matches_reference():
     bits = ref.basis_bits(10, codes)
     assert np.allclose(bits @ p, g["gs5_n_atom"], atol=1e-9)
     assert np.allclose(ref.corr_matrix(bits, p), g["gs5_corr"], atol=1e-9)
+
+
+@pytest.mark.parametrize("which", ["full", "basis"])
+def test_spin_observables_match_reference(which):
+    g = load("observables")
+    if which == "full":
+        n, codes, psi = 7, None, g["full_psi"]
+    else:
+        n, codes, psi = 10, g["basis_states"], g["basis_psi"]
+    ob = ref.spin_observables(n, codes, psi)
+    for k in ("sx", "sy", "sz", "sp", "sm", "xy_corr"):
+        assert np.allclose(ob[k], g["%s_%s" % (which, k)], atol=1e-12, rtol=0), k
+    assert np.allclose(ob["phase"], g[which + "_phase"], atol=1e-12, rtol=0, equal_nan=True)
+
+
+def test_entropies_and_corr_match_reference():
+    g = load("observables")
+    assert abs(ref.entropy_cut(7, None, g["full_psi"], 3) - float(g["full_S3"])) < 1e-12
+    assert abs(ref.entropy_cut(10, g["basis_states"], g["basis_psi"], 5) - float(g["basis_S5"])) < 1e-12
+    bits = ref.basis_bits(10, g["basis_states"])
+    assert np.allclose(ref.corr_matrix(bits, np.abs(g["basis_psi"]) ** 2), g["basis_corr"], atol=1e-13)
