@@ -354,9 +354,9 @@ def run_native(args):
 # ------------------------------------------------- further workloads (C1, C3-C5, H.v)
 
 WORKLOADS = ("kpm_dos_square25", "hv_chain31", "lanczos_chain12", "ramp_chain31", "batch512",
-             "adjoint_ring20")
+             "adjoint_ring20", "scan_xy20")
 DEFAULT_STEPS = {"kpm_dos_square25": 5, "hv_chain31": 200, "lanczos_chain12": 50, "ramp_chain31": 3,
-                 "batch512": 10, "adjoint_ring20": 5}
+                 "batch512": 10, "adjoint_ring20": 5, "scan_xy20": 3}
 
 
 class Harness:
@@ -692,9 +692,19 @@ def native_ramp31(h, args):
     b0 = h.ctx.copied_bytes
     te = time.perf_counter()
     res = evolve_manybody(cfg["calib"], psi0=cfg["psi0"], t_grid=cfg["t_grid"], segments=cfg["segments"],
-                          plan=plan, dtype="complex64", want_corr=False, want_entropy=False)
+                          plan=plan, dtype="complex64")
     e2e_s = time.perf_counter() - te
     b1 = h.ctx.copied_bytes
+    # the device observables alone on the final state: per output time (sites)
+    # and at the last time (all 465 pairs for corr and xy_corr)
+    all_pairs = [(i, j) for i in range(31) for j in range(i + 1, 31)]
+    obs_ms = {}
+    for tag, prs in (("sites", []), ("sites_and_465_pairs", all_pairs)):
+        solvers.spin_observables(ham32, psi32, prs)
+        t0 = time.perf_counter()
+        for _ in range(5):
+            solvers.spin_observables(ham32, psi32, prs)
+        obs_ms[tag] = (time.perf_counter() - t0) / 5 * 1e3
     cpu = None
     if h.rank == 0 and h.world == 1 and not args.no_cpu:
         cpu = cpu_ramp_sample(basis.dim)
@@ -710,6 +720,7 @@ def native_ramp31(h, args):
         "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
         "plain_fp64": {"solves_per_s": psteps / el64, "form": "complex128, tol 1e-13"},
         "chosen_vs_plain": (steps / el) / (psteps / el64),
+        "observables_ms": obs_ms,
         "error_vs_fp64": {"infidelity": 1.0 - fid, "norm_deviation": abs(norm32 - 1.0),
                           "max_abs_n_i": float(np.max(np.abs(n32 - n64))),
                           "max_abs_n_i_normalised": float(np.max(np.abs(n32 / norm32 ** 2 - n64 / norm64 ** 2))),
@@ -941,8 +952,123 @@ def cpu_adjoint_sample(cfg):
                       "per FD gradient" % (K, len(tau))}
 
 
+# --- sector scan: dipolar XY chain, every fixed-excitation sector
+
+SCAN_N = 20
+
+
+def native_scan_xy20(h, args):
+    """scan_ground_sectors on a 20-site dipolar XY chain (J on all 190 pairs,
+    weak V, random fields; 21 sectors, sum of dimensions 2^20)."""
+    torch = h.torch
+    import ctypes as C
+    from energy_level_b200 import _lib, configs, model, solvers
+    from energy_level_b200.sector_scan import scan_ground_sectors
+    n = SCAN_N
+    xy = configs.xy_chain(n, seed=7 + h.rank)
+    hams = []
+    for k in range(n + 1):
+        _, b, ham, _ = model.build(xy["calib"], xy["Om"], xy["delta"], terms=["I1", "I2"],
+                                   constraint={"kind": "charge", "k": k}, ctx=h.ctx)
+        hams.append((b, ham))
+
+    def scan():
+        best = None
+        for b, ham in hams:
+            r = solvers.lanczos_ground(ham, dtype="float64", seed=0, max_iter=48, max_restarts=8,
+                                       tol=1e-9, nev=min(2, b.dim))
+            e = float(r["evals"][0])
+            best = e if best is None else min(best, e)
+        return best
+
+    for _ in range(args.warmup):
+        scan()
+    steps = args.steps
+    el, launches, clocks = h.timed(scan, steps)
+    E0 = scan()
+    # H.v of the largest sector (k = 10, dim 184,756) alone: the dominant kernel
+    b10, h10 = hams[n // 2]
+    dim = b10.dim
+    x = torch.randn(dim, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    f = lambda: h.ctx.call("el_hv", h10.handle, C.c_int(_lib.EL_F64), C.c_int(1), C.c_void_p(x.data_ptr()),
+                           C.c_void_p(y.data_ptr()))
+    for _ in range(args.warmup):
+        f()
+    nh = 50
+    th, _, _ = h.timed(f, nh)
+    th /= nh
+    # end to end: the public call from the host calib
+    reps = max(1, min(steps, 3))
+    b0 = h.ctx.copied_bytes
+    te = time.perf_counter()
+    for _ in range(reps):
+        r = scan_ground_sectors(xy["calib"], delta=xy["delta"], Om=np.zeros(n), terms=["I1", "I2"],
+                                device="cuda:%d" % h.local)
+    e2e_s = (time.perf_counter() - te) / reps
+    b1 = h.ctx.copied_bytes
+    cpu = None
+    if h.rank == 0 and h.world == 1 and not args.no_cpu:
+        cpu = cpu_scan_sample()
+    line = base_line(args, h.world, "scan_xy20", h.world * steps / el, "scans/s", steps, el, "f64",
+                     {"n_sites": n, "sectors": n + 1, "dimension_sum": 1 << n, "largest_sector": dim,
+                      "exchange_pairs": n * (n - 1) // 2,
+                      "form": "per sector: fixed-popcount basis + device Lanczos (m 48, tol 1e-9, FP64)",
+                      "l2": "every sector fits in L2 (largest H.v working set 4.4 MB); latency-bound"})
+    line.update({
+        "roofline": roofline(dim * (2 * 8 + 8), th, kernel="k_apply<double> generic kernel with 190 exchange "
+                             "pairs, fixed-popcount sector (L2-resident: HBM peak is not the bound)"),
+        "e2e": {"value": h.world / e2e_s, "unit": "scans/s",
+                "h2d_bytes_per_step": (b1[0] - b0[0]) // reps, "d2h_bytes_per_step": (b1[1] - b0[1]) // reps},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+        "check": {"E0": E0, "E0_e2e": float(r["E0"]), "sector": int(r["sector"]), "converged": bool(r["converged"])},
+        "hv_largest_sector_us": th * 1e6,
+    })
+    return line
+
+
+def _scan_cpu(n, seed=7):
+    """Oracle scan: per sector CSR (oracle channel list) + ARPACK eigsh(k=2,'SA')."""
+    import scipy.sparse.linalg as spla
+    from energy_level_b200 import configs
+    from oracle import ref
+    xy = configs.xy_chain(n, seed=seed)
+    pairs = [(p["i"], p["j"], p["V"]) for p in xy["calib"]["pairs"]]
+    ex = [(p["i"], p["j"], p["J"], 0.0) for p in xy["calib"]["pairs"]]
+    nnz = 0
+    best = None
+    for k in range(n + 1):
+        codes = ref.number_sector_basis(n, k)
+        H = ref.sparse_h(n, codes, np.zeros(n), xy["delta"], pairs, exchange=ex)
+        nnz += H.nnz
+        if H.shape[0] <= 64:
+            e = float(np.linalg.eigvalsh(H.toarray())[0])
+        else:
+            v0 = np.random.default_rng(0).normal(size=H.shape[0])
+            e = float(spla.eigsh(H, k=2, which="SA", v0=v0, tol=1e-10, return_eigenvectors=False).min())
+        best = e if best is None else min(best, e)
+    return best, nnz
+
+
+def cpu_scan_sample(n_sample=16):
+    """Full oracle scan of a 16-site chain, scaled to 20 sites by the total
+    number of stored H entries."""
+    from math import comb
+    t0 = time.perf_counter()
+    _, nnz_s = _scan_cpu(n_sample)
+    dt = time.perf_counter() - t0
+    # stored entries at 20 sites: per row the diagonal and one entry for each
+    # of the k (n - k) exchange hops inside the sector
+    n = SCAN_N
+    nnz_full = sum(comb(n, k) * (1 + k * (n - k)) for k in range(n + 1))
+    scale = nnz_full / nnz_s
+    return {"value": 1.0 / (dt * scale), "unit": "scans/s", "cores": _threads(), "kind": "port",
+            "sample": "full oracle scan (CSR + ARPACK per sector) of a %d-site XY chain, %.2f s, scaled to "
+                      "%d sites by stored H entries (x%.1f)" % (n_sample, dt, n, scale)}
+
+
 NATIVE = {"hv_chain31": native_hv, "lanczos_chain12": native_lanczos12, "ramp_chain31": native_ramp31,
-          "batch512": native_batch512, "adjoint_ring20": native_adjoint20}
+          "batch512": native_batch512, "adjoint_ring20": native_adjoint20, "scan_xy20": native_scan_xy20}
 
 
 def run_native_workload(args):
@@ -974,6 +1100,9 @@ def run_reference_workload(args):
     elif w == "batch512":
         cb = cpu_batch_sample(configs.batch512())
         v, unit = cb["value"], "solves/s"
+    elif w == "scan_xy20":
+        cb = cpu_scan_sample()
+        v, unit = cb["value"], "scans/s"
     else:
         cb = cpu_adjoint_sample(configs.ring20())
         v, unit = cb["value"], "grads/s"
