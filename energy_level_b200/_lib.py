@@ -50,6 +50,8 @@ PROTOTYPES = {
     "el_basis_destroy": (C.c_int, [_vp]),
     "el_ham_create": (C.c_int, [_vp, _vp, _dp, _dp, _dp, C.c_int, _vp, _vp, _dp, C.POINTER(_vp)]),
     "el_ham_set_drive": (C.c_int, [_vp, _vp, _dp, _dp, _dp]),
+    "el_ham_set_loss": (C.c_int, [_vp, _vp, _dp]),
+    "el_taylor_step": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, _ip]),
     "el_ham_set_exchange": (C.c_int, [_vp, _vp, C.c_int, _vp, _vp, _dp, _dp, _dp, _dp]),
     "el_ham_diag": (C.c_int, [_vp, _vp, C.c_int, _vp]),
     "el_ham_destroy": (C.c_int, [_vp]),

@@ -50,7 +50,7 @@ TIME_BACKENDS = {
                              aliases=('b200', 'b200-ed', 'chebyshev-gpu'),
                              options=(('memory_budget_mb', 'memory_budget_mb'), ('dtype', 'dtype'),
                                       ('device', 'device')),
-                             segments=True, projected=True, gamma=False, return_state=True,
+                             segments=True, projected=True, gamma=True, return_state=True,
                              pauli='full', algorithm='chebyshev'),
 }
 
@@ -86,7 +86,7 @@ def validate_time_capabilities(name, *, segments=None, plan=None, gamma=None, re
         raise ConfigConflict('%s 尚不支持 drive_segments' % name, keys=('manybody.drive_segments',))
     if plan and plan.get('projected') and not b.projected:
         raise ConfigConflict('%s 尚不支持 projected HamiltonianPlan' % name, keys=('manybody.constraint',))
-    if gamma is not None and np.any(np.asarray(gamma) != 0):
+    if gamma is not None and np.any(np.asarray(gamma) != 0) and not b.gamma:
         raise ConfigConflict('%s 仅支持 gamma=0' % name, keys=('manybody.gamma_mhz',))
     if charge_sector is not None:
         raise ConfigConflict('%s 尚不支持实时 charge_sector' % name, keys=('manybody.charge_sector',))

@@ -182,6 +182,7 @@ class Hamiltonian:
         self.omega = om
         self.delta = de
         self.pairs = list(zip(pi.tolist(), pj.tolist(), V.tolist()))
+        self.gamma = np.zeros(n)
         self.exchange = []
         if exchange:
             self.set_exchange(exchange)
@@ -199,11 +200,25 @@ class Hamiltonian:
                       *[_lib.dptr(a) if k else None for a in amp])
         self.exchange = ex
 
+    def set_loss(self, gamma):
+        """Loss rates per site (gamma_mhz): non-Hermitian diagonal
+        -0.5 i gamma 1e-3 / CONV per excited site; None or zeros clear it."""
+        g = np.zeros(self.n) if gamma is None else np.asarray(gamma, float).reshape(-1)
+        if g.shape != (self.n,) or not np.isfinite(g).all():
+            raise ValueError('gamma 须为有限、长度为 N 的数组')
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        self.ctx.call('el_ham_set_loss', self.handle, _lib.dptr(g))
+        self.gamma = g
+
+    @property
+    def lossy(self) -> bool:
+        return bool(np.any(getattr(self, 'gamma', np.zeros(1)) != 0))
+
     @property
     def complex_drive(self) -> bool:
-        """H is complex: a complex Omega, J or A."""
-        return bool(np.any(self.omega.imag != 0)) or any(e[2].imag != 0 or e[3].imag != 0
-                                                         for e in getattr(self, 'exchange', ()))
+        """H is complex: a complex Omega, J or A, or a loss diagonal."""
+        return bool(np.any(self.omega.imag != 0)) or self.lossy or any(
+            e[2].imag != 0 or e[3].imag != 0 for e in getattr(self, 'exchange', ()))
 
     def set_drive(self, omega, delta):
         om = np.asarray(omega, complex).reshape(-1)

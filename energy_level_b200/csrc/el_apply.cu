@@ -27,6 +27,8 @@ struct HamArgs {
   S up_im[EL_MAX_SITES];  // (into a row whose bit k is 0: conj(Omega)/2)
   const ExPair *px;       // exchange channels (generic kernel only)
   int npx;
+  int lossy;              // loss diagonal present (generic kernel only)
+  S loss[EL_MAX_SITES];   // imaginary diagonal per set bit: -gamma/2 (evolution units)
 };
 
 // Amplitude <row|H|row ^ (bit bi | bit bj)> of exchange pair e for a row whose
@@ -111,10 +113,13 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev B, HamArgs<S> H, KArgs K
     const int64_t v = t & (K.nvec - 1);
     const uint64_t code = el::unrank_row(B, row);
     const V xr = V::load(K.x, t);
-    S hre = 0, him = 0, dsum = 0;
+    S hre = 0, him = 0, dsum = 0, dimg = 0;
     for (int k = 0; k < B.n; ++k) {
       const bool set = (code >> k) & 1ULL;
-      if (set) dsum += H.delta[k];
+      if (set) {
+        dsum += H.delta[k];
+        if constexpr (C) dimg += H.loss[k];
+      }
       const S are = H.up_re[k];
       const S aim = C ? (set ? H.up_im[k] : -H.up_im[k]) : S(0);
       if (are == S(0) && aim == S(0)) continue;
@@ -146,8 +151,12 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev B, HamArgs<S> H, KArgs K
     }
     if (!K.skip_diag) {
       dsum += H.diagV[row];
-      if constexpr (C) { hre += dsum * xr.re; him += dsum * xr.im; }
-      else { hre += dsum * xr.v; }
+      if constexpr (C) {
+        hre += dsum * xr.re - dimg * xr.im;
+        him += dsum * xr.im + dimg * xr.re;
+      } else {
+        hre += dsum * xr.v;
+      }
     }
     V yv;
     if constexpr (C) {
@@ -731,10 +740,12 @@ HamArgs<S> ham_args(const el_ham *h, const S *diagV) {
   A.diagV = diagV;
   A.px = h->d_px;
   A.npx = (int)h->px.size();
+  A.lossy = h->lossy ? 1 : 0;
   for (int k = 0; k < h->n; ++k) {
     A.delta[k] = (S)h->delta[k];
     A.up_re[k] = (S)(0.5 * h->om_re[k]);
     A.up_im[k] = (S)(0.5 * h->om_im[k]);
+    A.loss[k] = (S)h->loss[k];
   }
   return A;
 }
@@ -786,15 +797,15 @@ __global__ void k_full_diag(BasisDev B, HamArgs<double> H, S *out) {
 // Gershgorin interval: min_r (d_r - R_r), max_r (d_r + R_r).
 __global__ void k_gershgorin(BasisDev B, HamArgs<double> H, double *partials,
                              unsigned int *counter, double *out) {
-  __shared__ double lo_s[256], hi_s[256];
+  __shared__ double lo_s[256], hi_s[256], nm_s[256];
   __shared__ bool last;
-  double lo = 1e300, hi = -1e300;
+  double lo = 1e300, hi = -1e300, nm = 0.0;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < B.dim;
        r += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t code = el::unrank_row(B, r);
-    double d = H.diagV[r], R = 0.0;
+    double d = H.diagV[r], R = 0.0, di = 0.0;
     for (int k = 0; k < B.n; ++k) {
-      if ((code >> k) & 1ULL) d += H.delta[k];
+      if ((code >> k) & 1ULL) { d += H.delta[k]; di += H.loss[k]; }
       const double amp = sqrt(H.up_re[k] * H.up_re[k] + H.up_im[k] * H.up_im[k]);
       if (amp == 0.0) continue;
       if (el::flip_target(B, code, r, k) >= 0) R += amp;
@@ -808,33 +819,39 @@ __global__ void k_gershgorin(BasisDev B, HamArgs<double> H, double *partials,
     }
     lo = fmin(lo, d - R);
     hi = fmax(hi, d + R);
+    nm = fmax(nm, sqrt(d * d + di * di) + R);
   }
   lo_s[threadIdx.x] = lo;
   hi_s[threadIdx.x] = hi;
+  nm_s[threadIdx.x] = nm;
   __syncthreads();
   for (int s = 128; s > 0; s >>= 1) {
     if (threadIdx.x < s) {
       lo_s[threadIdx.x] = fmin(lo_s[threadIdx.x], lo_s[threadIdx.x + s]);
       hi_s[threadIdx.x] = fmax(hi_s[threadIdx.x], hi_s[threadIdx.x + s]);
+      nm_s[threadIdx.x] = fmax(nm_s[threadIdx.x], nm_s[threadIdx.x + s]);
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = lo_s[0];
-    partials[2 * blockIdx.x + 1] = hi_s[0];
+    partials[3 * blockIdx.x] = lo_s[0];
+    partials[3 * blockIdx.x + 1] = hi_s[0];
+    partials[3 * blockIdx.x + 2] = nm_s[0];
     __threadfence();
     last = (atomicAdd(counter, 1u) == gridDim.x - 1);
   }
   __syncthreads();
   if (last && threadIdx.x == 0) {
     __threadfence();
-    double a = 1e300, b = -1e300;
+    double a = 1e300, b = -1e300, c = 0.0;
     for (unsigned i = 0; i < gridDim.x; ++i) {
-      a = fmin(a, __ldcg(&partials[2 * i]));
-      b = fmax(b, __ldcg(&partials[2 * i + 1]));
+      a = fmin(a, __ldcg(&partials[3 * i]));
+      b = fmax(b, __ldcg(&partials[3 * i + 1]));
+      c = fmax(c, __ldcg(&partials[3 * i + 2]));
     }
     out[0] = a;
     out[1] = b;
+    out[2] = c;
     *counter = 0u;
   }
 }
@@ -1071,7 +1088,7 @@ namespace {
 // (dot products only for one vector) when every vector pointer is aligned for
 // its row-segment loads.
 bool row_kernel_ok(const el_ham *h, const ApplyArgs &A) {
-  if (!h->px.empty()) return false;   // exchange channels: generic kernel
+  if (!h->px.empty() || h->lossy) return false;   // exchange channels or loss: generic kernel
   const int lay = h->basis->layout;
   if (lay != EL_LAYOUT_FULL && lay != EL_LAYOUT_CHAIN && lay != EL_LAYOUT_RING) return false;
   if (A.nvec > 8) return false;
@@ -1294,18 +1311,19 @@ int launch_full_diag(el_ctx *ctx, el_ham *h, int dtype, void *out) {
   return EL_OK;
 }
 
-int gershgorin(el_ctx *ctx, el_ham *h, double *lo, double *hi) {
+int gershgorin(el_ctx *ctx, el_ham *h, double *lo, double *hi, double *norm1) {
   BasisDev B = basis_dev(h->basis);
   HamArgs<double> H = ham_args<double>(h, h->d_diagV64);
   const int grid = grid_for(B.dim, 256);
-  int rc = ensure_partials(ctx, (size_t)grid * 2);
+  int rc = ensure_partials(ctx, (size_t)grid * 3);
   if (rc) return rc;
   k_gershgorin<<<grid, 256, 0, ctx->stream>>>(B, H, ctx->d_partials, ctx->d_counter, ctx->d_scalars);
   EL_LAUNCH_CHECK(ctx);
-  EL_CUDA_TRY(ctx, el::copy(ctx, ctx->h_scalars, ctx->d_scalars, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  EL_CUDA_TRY(ctx, el::copy(ctx, ctx->h_scalars, ctx->d_scalars, 3 * sizeof(double), cudaMemcpyDeviceToHost));
   EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   *lo = ctx->h_scalars[0];
   *hi = ctx->h_scalars[1];
+  if (norm1) *norm1 = ctx->h_scalars[2];
   return EL_OK;
 }
 
@@ -1465,6 +1483,7 @@ int el_ham_create(el_ctx *ctx, el_basis *basis, const double *omega_re,
   memset(h->om_re, 0, sizeof h->om_re);
   memset(h->om_im, 0, sizeof h->om_im);
   memset(h->delta, 0, sizeof h->delta);
+  memset(h->loss, 0, sizeof h->loss);
   h->Vbits.assign((size_t)n * n, 0.0);
   for (int p = 0; p < n_pairs; ++p) {
     const int i = pi[p], j = pj[p];
@@ -1502,7 +1521,25 @@ int el_ham_set_drive(el_ctx *ctx, el_ham *h, const double *omega_re,
     if (oim != 0.0) cplx = true;
   }
   h->drive_complex = cplx;
-  h->complex_drive = h->drive_complex || h->px_complex;
+  h->complex_drive = h->drive_complex || h->px_complex || h->lossy;
+  return EL_OK;
+}
+
+int el_ham_set_loss(el_ctx *ctx, el_ham *h, const double *gamma) {
+  if (!ctx || !h) return EL_EINVAL;
+  const int n = h->n;
+  // channels.py:69-76: diagonal (delta_i - 0.5 i gamma_i 1e-3 / CONV) n_i
+  const double conv = 2.0 * 3.14159265358979323846 * 1e-3;
+  bool any = false;
+  double loss[EL_MAX_SITES] = {0.0};
+  for (int i = 0; gamma && i < n; ++i) {
+    if (!std::isfinite(gamma[i])) return fail(ctx, EL_EINVAL, "gamma must be finite");
+    loss[n - 1 - i] = -0.5 * gamma[i] * 1e-3 / conv;
+    if (gamma[i] != 0.0) any = true;
+  }
+  memcpy(h->loss, loss, sizeof loss);
+  h->lossy = any;
+  h->complex_drive = h->drive_complex || h->px_complex || h->lossy;
   return EL_OK;
 }
 
@@ -1548,7 +1585,7 @@ int el_ham_set_exchange(el_ctx *ctx, el_ham *h, int n_pairs, const int32_t *pi,
   h->d_px = d;
   h->px.swap(px);
   h->px_complex = cplx;
-  h->complex_drive = h->drive_complex || h->px_complex;
+  h->complex_drive = h->drive_complex || h->px_complex || h->lossy;
   return EL_OK;
 }
 

@@ -91,6 +91,7 @@ extern "C" int el_cheb_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
   if (dtype != EL_C64 && dtype != EL_C128) return fail(ctx, EL_EINVAL, "evolution needs EL_C64 or EL_C128");
   if (!std::isfinite(tau_ns) || tau_ns < 0) return fail(ctx, EL_EINVAL, "tau must be finite and >= 0");
   if (!(tol > 0) || tol >= 1) return fail(ctx, EL_EINVAL, "tol must be in (0, 1)");
+  if (h->lossy) return fail(ctx, EL_EINVAL, "the Chebyshev step needs a Hermitian H; use el_taylor_step with gamma != 0");
   if (n_terms) *n_terms = 0;
   if (tau_ns == 0.0) return EL_OK;
   if (el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
@@ -131,5 +132,75 @@ extern "C" int el_cheb_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
   }
   EL_CUDA_TRY(ctx, el::copy(ctx, psi, acc, vb, cudaMemcpyDeviceToDevice));
   if (n_terms) *n_terms = M + 1;
+  return EL_OK;
+}
+
+// ------------------------------------------------------------------- Taylor
+// Non-Hermitian H (loss diagonal -i gamma/2): psi <- exp(A) psi with
+// A = -i CONV tau H, the operation of expm_multiply in engine_ed.py:125,145
+// for gamma != 0.  With the bound ||H|| <= max_r (|d_r| + sum_offdiag |H_rs|)
+// (row and column sums agree: the off-diagonal part is Hermitian), exp(A) is
+// applied as s substeps exp(A/s) with ||A/s|| <= theta, each a Taylor
+// polynomial of degree m, the smallest m whose remainder bound
+// sum_{j>m} theta_s^j / j! is below tol / s (theta_s = ||A|| / s).  With
+// u_0 = psi, u_j = (CONV tau / (s j)) H u_{j-1}, the terms are (-i)^j u_j:
+// one fused launch per term (real scale on H x, complex weight on acc).
+extern "C" int el_taylor_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
+                              double tau_ns, double tol, int *n_terms) {
+  if (!ctx || !h || !psi) return EL_EINVAL;
+  if (dtype != EL_C64 && dtype != EL_C128) return fail(ctx, EL_EINVAL, "evolution needs EL_C64 or EL_C128");
+  if (!std::isfinite(tau_ns) || tau_ns < 0) return fail(ctx, EL_EINVAL, "tau must be finite and >= 0");
+  if (!(tol > 0) || tol >= 1) return fail(ctx, EL_EINVAL, "tol must be in (0, 1)");
+  if (n_terms) *n_terms = 0;
+  if (tau_ns == 0.0) return EL_OK;
+  if (el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int64_t dim = h->basis->dim;
+  const size_t vb = (size_t)dim * el::dtype_size(dtype);
+  double lo, hi, nrm;
+  int rc = el::gershgorin(ctx, h, &lo, &hi, &nrm);
+  if (rc) return rc;
+  const double x = CONV * tau_ns * nrm;
+  const double theta = (dtype == EL_C128) ? 2.0 : 1.0;
+  const int s = std::max(1, (int)std::ceil(x / theta));
+  const double ths = x / s;
+  // smallest m with sum_{j > m} ths^j / j! <= tol / s
+  int m = 1;
+  for (; m < 120; ++m) {
+    double term = 1.0, rem = 0.0;
+    for (int j = 1; j <= m + 80; ++j) {
+      term *= ths / j;
+      if (j > m) rem += term;
+    }
+    if (rem <= tol / s) break;
+  }
+  char *buf = (char *)el::workspace(ctx, 13, 3 * vb);
+  if (!buf) return EL_ENOMEM;
+  void *ta = buf, *tb = buf + vb, *acc = buf + 2 * vb;
+  const double scale = CONV * tau_ns / s;
+  for (int step = 0; step < s; ++step) {
+    if (el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
+    EL_CUDA_TRY(ctx, el::copy(ctx, acc, psi, vb, cudaMemcpyDeviceToDevice));
+    const void *xc = psi;
+    void *y = ta;
+    for (int j = 1; j <= m; ++j) {
+      ApplyArgs A;
+      memset(&A, 0, sizeof A);
+      A.dtype = dtype; A.nvec = 1; A.x = xc; A.y = (j < m) ? y : nullptr; A.acc = acc;
+      A.a = scale / j;
+      switch (j & 3) {  // (-i)^j
+        case 0: A.w_re = 1; break;
+        case 1: A.w_im = -1; break;
+        case 2: A.w_re = -1; break;
+        default: A.w_im = 1; break;
+      }
+      rc = el::launch_apply(ctx, h, A);
+      if (rc) return rc;
+      xc = y;
+      y = (y == ta) ? tb : ta;
+    }
+    EL_CUDA_TRY(ctx, el::copy(ctx, psi, acc, vb, cudaMemcpyDeviceToDevice));
+  }
+  if (n_terms) *n_terms = s * m;
   return EL_OK;
 }

@@ -105,7 +105,10 @@ struct el_ham {
   ExPair *d_px = nullptr;
   bool drive_complex = false;     // Omega has an imaginary part
   bool px_complex = false;        // some J or A has an imaginary part
-  bool complex_drive = false;     // H is complex: drive_complex || px_complex
+  // loss: imaginary diagonal -gamma_i/2 (in the evolution's units) per bit
+  double loss[EL_MAX_SITES];
+  bool lossy = false;             // some gamma != 0: H is not Hermitian
+  bool complex_drive = false;     // H is complex: drive_complex || px_complex || lossy
 };
 
 // ---------------------------------------------------------------- helpers
@@ -305,7 +308,9 @@ int launch_apply(el_ctx *ctx, el_ham *h, const ApplyArgs &A);
 int launch_diag_v(el_ctx *ctx, el_ham *h);
 int launch_full_diag(el_ctx *ctx, el_ham *h, int dtype, void *out);
 // Gershgorin interval of H over the basis (host results).
-int gershgorin(el_ctx *ctx, el_ham *h, double *lo, double *hi);
+// norm1 (optional): max over rows of |d_r| + sum |offdiag| (a bound on the
+// 1-norm and the 2-norm of H, also when H has a loss diagonal).
+int gershgorin(el_ctx *ctx, el_ham *h, double *lo, double *hi, double *norm1 = nullptr);
 // y[i] = alpha*x[i] + beta*y[i] and optional ||y||^2 (dots[0]); real or complex
 int launch_axpby(el_ctx *ctx, int dtype, int64_t len, double a_re, double a_im,
                  const void *x, double b_re, double b_im, void *y,

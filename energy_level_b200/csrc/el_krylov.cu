@@ -47,6 +47,7 @@ extern "C" int el_bounds(el_ctx *ctx, el_ham *h, int max_iter, double tol,
                          uint64_t seed, double *emin, double *emax) {
   if (!ctx || !h || !emin || !emax) return EL_EINVAL;
   if (max_iter < 2) return fail(ctx, EL_EINVAL, "max_iter must be >= 2");
+  if (h->lossy) return fail(ctx, EL_EINVAL, "spectral bounds need a Hermitian H (gamma = 0)");
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   const int64_t dim = h->basis->dim;
   const int dtype = h->complex_drive ? EL_C128 : EL_F64;
@@ -229,6 +230,7 @@ extern "C" int el_lanczos_ground(el_ctx *ctx, el_ham *h, int dtype, const void *
   if (!el::dtype_size(dtype)) return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
   if (h->complex_drive && !is_cplx(dtype)) return fail(ctx, EL_EINVAL, "complex Omega, J or A needs a complex dtype");
   if (nev < 1 || nev > 2) return fail(ctx, EL_EINVAL, "nev must be 1 or 2");
+  if (h->lossy) return fail(ctx, EL_EINVAL, "ground states need a Hermitian H (gamma = 0)");
   if (max_iter < 2 || max_restarts < 0) return fail(ctx, EL_EINVAL, "max_iter must be >= 2, max_restarts >= 0");
   if (!(tol > 0) || !std::isfinite(tol)) return fail(ctx, EL_EINVAL, "tol must be positive and finite");
   if (reorth < 0 || reorth > 2) return fail(ctx, EL_EINVAL, "reorth must be 0, 1 or 2");
@@ -447,6 +449,7 @@ extern "C" int el_lanczos_tridiag(el_ctx *ctx, el_ham *h, int dtype, const void 
   if (!el::dtype_size(dtype)) return fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
   if (h->complex_drive && !is_cplx(dtype)) return fail(ctx, EL_EINVAL, "complex Omega, J or A needs a complex dtype");
   if (n_krylov < 1) return fail(ctx, EL_EINVAL, "n_krylov must be positive");
+  if (h->lossy) return fail(ctx, EL_EINVAL, "the Lanczos tridiagonalisation needs a Hermitian H (gamma = 0)");
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   const int64_t dim = h->basis->dim;
   const size_t vb = (size_t)dim * el::dtype_size(dtype);

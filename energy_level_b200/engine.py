@@ -151,7 +151,9 @@ def evolve_manybody(calib, psi0=None, t_grid=None, Om=None, delta=None, gamma=No
         terms = plan.get('terms') if terms is None else terms
     t = time_grid(t_grid)
     check_cancel(progress_arr)
-    ctx, basis, ham, perm = model.build(calib, Om, delta, gamma, terms, plan=plan, device=device)
+    ctx, basis, ham, perm = model.build(calib, Om, delta, gamma, terms, plan=plan, device=device,
+                                        allow_loss=True)
+    hermitian = not ham.lossy
     dim = basis.dim
     if max_dim is not None and dim > int(max_dim):
         raise ValueError('多体 ED 有效维度 %d 超上限 %d；请调整系统或后端' % (dim, int(max_dim)))
@@ -240,7 +242,8 @@ def evolve_manybody(calib, psi0=None, t_grid=None, Om=None, delta=None, gamma=No
                 ham.set_drive(om, de)
                 current = key
             if b > a:
-                terms_used += solvers.cheb_step(ham, psi, b - a, tol=tol)
+                step = solvers.cheb_step if hermitian else solvers.taylor_step
+                terms_used += step(ham, psi, b - a, tol=tol)
                 pieces += 1
         reduce(k)
         progress_arr[0] = (k + 1) / n_t
@@ -260,7 +263,8 @@ def evolve_manybody(calib, psi0=None, t_grid=None, Om=None, delta=None, gamma=No
         if want_observables and want_xy_corr:
             xy_last = XY
     loss = 1.0 - norms
-    backend = 'b200-cheb-plan-%s' % plan['constraint']['kind'] if projected else 'b200-cheb'
+    backend = ('b200-cheb-plan-%s' % plan['constraint']['kind'] if projected else
+               'b200-cheb' if hermitian else 'b200-cheb-nonhermitian')
     capped = joint is None or projected
     if not capped:
         pops = joint
@@ -289,11 +293,11 @@ def evolve_manybody(calib, psi0=None, t_grid=None, Om=None, delta=None, gamma=No
         basis_probabilities=joint, basis_states=(codes if projected else None),
         basis=dict(kind='projected' if projected else 'full', bit_order='site0-msb',
                    n_atoms=n, dim=dim, full_dim=1 << n),
-        error_report=dict(backend=backend, solver='chebyshev', dim=dim, n_atoms=n, n_t=n_t,
-                          hermitian=True, used_sectors=False, full_pops=(not capped),
+        error_report=dict(backend=backend, solver='chebyshev' if hermitian else 'taylor', dim=dim,
+                          n_atoms=n, n_t=n_t, hermitian=hermitian, used_sectors=False, full_pops=(not capped),
                           projected=bool(projected), entropy_cut=(cut if want_entropy else None),
                           entropy_note=S_note,
-                          max_norm_dev=float(np.max(np.abs(norms - 1.0))),
+                          max_norm_dev=float(np.max(np.abs(norms - 1.0))) if hermitian else 0.0,
                           chebyshev_terms=int(terms_used), pieces=int(pieces), tol=tol, dtype=dtype),
         diag=({'dim': dim, 'n_atoms': n, 'backend': backend, 'launches': ctx.launches} if diag else None),
         observables=obs)

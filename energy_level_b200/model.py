@@ -38,11 +38,13 @@ def active_terms(calib):
     return out
 
 
-def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None, exchange=None):
+def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None, exchange=None, allow_loss=False):
     """Validate and flatten a calib to (n, Om complex[n], delta[n], pairs).
 
     ``exchange``: a list that receives the (i, j, J, A) exchange channels of
-    the terms in use; None refuses a nonzero J or A with ConfigConflict."""
+    the terms in use; None refuses a nonzero J or A with ConfigConflict.
+    ``allow_loss``: accept gamma != 0 (the caller sets the loss diagonal);
+    otherwise it is refused with ConfigConflict."""
     atoms = (calib or {}).get('atoms') or []
     n = len(atoms)
     if n == 0:
@@ -52,7 +54,7 @@ def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None, exchange=No
     gamma = np.zeros(n) if gamma is None else np.asarray(gamma, float).reshape(-1)
     if any(x.shape != (n,) or not np.isfinite(x).all() for x in (Om, delta, gamma)):
         raise ValueError('Om/delta/gamma 须为有限、长度为 N 的数组')
-    if np.any(gamma != 0):
+    if np.any(gamma != 0) and not allow_loss:
         raise ConfigConflict('b200 backends need a Hermitian H (gamma = 0)', keys=('manybody.gamma_mhz',))
     use = set(active_terms(calib) if terms is None else terms)
     pairs = []
@@ -146,10 +148,13 @@ def check_number_conserving(calib, Om=None, terms=None):
 
 
 def build(calib, Om=None, delta=None, gamma=None, terms=None, plan=None, basis_indices=None,
-          constraint=None, device=0, ctx=None, max_states=None):
-    """(ctx, basis, hamiltonian, permutation) for a reference-style model."""
+          constraint=None, device=0, ctx=None, max_states=None, allow_loss=False):
+    """(ctx, basis, hamiltonian, permutation) for a reference-style model.
+    ``allow_loss``: the caller propagates in time and accepts gamma != 0 (a
+    non-Hermitian loss diagonal, channels.py:69-76)."""
     exchange = []
-    n, Om, delta, pairs = model_arrays(calib, Om, delta, gamma, terms, exchange=exchange)
+    n, Om, delta, pairs = model_arrays(calib, Om, delta, gamma, terms, exchange=exchange,
+                                       allow_loss=allow_loss)
     dev = device
     if isinstance(dev, str):
         if dev.startswith('cpu'):
@@ -159,4 +164,6 @@ def build(calib, Om=None, delta=None, gamma=None, terms=None, plan=None, basis_i
     b, perm = basis_for(ctx, n, plan=plan, basis_indices=basis_indices, constraint=constraint,
                         max_states=max_states)
     h = Hamiltonian(ctx, b, Om, delta, pairs, exchange=exchange)
+    if gamma is not None and np.any(np.asarray(gamma, float) != 0):
+        h.set_loss(gamma)
     return ctx, b, h, perm

@@ -124,6 +124,21 @@ def observables(ham: Hamiltonian, psi):
     return ns, float(nrm.value)
 
 
+def taylor_step(ham: Hamiltonian, psi, tau_ns, tol=1e-13):
+    """psi <- exp(-i CONV H tau) psi for any H (loss diagonal included):
+    scaled Taylor polynomial (el_taylor_step); returns the H applications."""
+    torch = _torch()
+    dt = {torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}.get(psi.dtype)
+    if dt is None:
+        raise ValueError('psi must be complex64 or complex128')
+    if not psi.is_contiguous():
+        raise ValueError('psi must be contiguous')
+    nt = C.c_int()
+    ham.ctx.call('el_taylor_step', ham.handle, C.c_int(dt), C.c_void_p(psi.data_ptr()), C.c_double(float(tau_ns)),
+                 C.c_double(float(tol)), C.byref(nt))
+    return int(nt.value)
+
+
 def spin_observables(ham: Hamiltonian, psi, pairs=()):
     """Device spin observables of a state (el_spin_observables).
 

@@ -129,6 +129,13 @@ int el_ham_create(el_ctx *ctx, el_basis *basis, const double *omega_re,
  * engine_ed.py:141-144. */
 int el_ham_set_drive(el_ctx *ctx, el_ham *ham, const double *omega_re,
                      const double *omega_im, const double *delta);
+/* Set (replace) the loss rates gamma[i] (per site, as the reference's
+ * gamma_mhz; NULL clears them): the diagonal gains -0.5 i gamma_i 1e-3 / CONV
+ * per excited site i (channels.py:69-76).  H is then non-Hermitian and
+ * complex: products need complex dtypes, ground states, bounds, KPM, the
+ * Chebyshev step and the adjoint refuse it, and evolution uses
+ * el_taylor_step. */
+int el_ham_set_loss(el_ctx *ctx, el_ham *ham, const double *gamma);
 /* Set (replace) the two-site exchange channels of ham: for each pair p the
  * sites (pi[p], pj[p]), J = J_re + i J_im (I2: <g_i r_j|H|r_i g_j> = conj(J),
  * <r_i g_j|H|g_i r_j> = J) and A = A_re + i A_im (I3: <r_i r_j|H|g_i g_j> = A,
@@ -240,6 +247,13 @@ int el_batch_destroy(el_batch *batch);
  * Replaces the expm_multiply step of engine_ed.py:125 and engine_ed.py:145. */
 int el_cheb_step(el_ctx *ctx, el_ham *ham, int dtype, void *psi,
                  double tau_ns, double tol, int *n_terms);
+/* psi <- exp(-i CONV tau H) psi for any H, including a loss diagonal (gamma
+ * != 0, non-Hermitian): s substeps of a degree-m Taylor polynomial chosen
+ * from the bound ||H|| <= max_r (|d_r| + sum_s |H_rs|) so that the remainder
+ * bound is below tol per step; *n_terms = s * m H applications.  Replaces
+ * expm_multiply (engine_ed.py:125,145) on the non-Hermitian path. */
+int el_taylor_step(el_ctx *ctx, el_ham *ham, int dtype, void *psi, double tau_ns,
+                   double tol, int *n_terms);
 /* Pulse gradient by the adjoint of the Chebyshev propagator.  K steps; step k
  * lasts tau[k] ns with Omega_i = omega_k[k] * omega_shape[i] and
  * delta_i = -delta_k[k] * delta_shape[i] (shapes NULL = 1), V from `ham`.

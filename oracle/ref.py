@@ -97,6 +97,13 @@ def diagonal(n, codes, delta, pairs):
     return d
 
 
+def loss_diagonal(n, codes, gamma):
+    """Imaginary diagonal -0.5 i sum gamma_i 1e-3 / CONV n_i (channels.py:69-76)."""
+    bits = basis_bits(n, codes).astype(np.float64)
+    g = np.asarray(gamma, float)
+    return -0.5j * (g * 1e-3 / CONV) @ bits
+
+
 def channel_list(n, omega, exchange=None):
     """(selector, mask, amp) channels as channel_spec builds them
     (channels.py:114-131): per site with Omega != 0 a g->r channel with
@@ -146,12 +153,13 @@ def _channel_entries(n, codes, full, channels):
         yield order[pos[ok]], src[ok], amp
 
 
-def _is_complex(omega, exchange):
+def _is_complex(omega, exchange, gamma=None):
     return bool(np.any(np.asarray(omega).imag != 0)) or any(
-        complex(e[2]).imag != 0 or complex(e[3]).imag != 0 for e in (exchange or ()))
+        complex(e[2]).imag != 0 or complex(e[3]).imag != 0 for e in (exchange or ())) or (
+        gamma is not None and bool(np.any(np.asarray(gamma) != 0)))
 
 
-def hv(n, codes, omega, delta, pairs, x, exchange=None):
+def hv(n, codes, omega, delta, pairs, x, exchange=None, gamma=None):
     """y = H x on the full (codes=None) or restricted basis.
 
     Follows ChannelKernel.matvec (channels.py:210-221): the diagonal, then
@@ -163,14 +171,16 @@ def hv(n, codes, omega, delta, pairs, x, exchange=None):
     vec = x.ndim == 1
     X = x.reshape(len(codes), -1)
     d = diagonal(n, codes, delta, pairs)
-    cplx = np.iscomplexobj(X) or _is_complex(omega, exchange)
+    cplx = np.iscomplexobj(X) or _is_complex(omega, exchange, gamma)
+    if gamma is not None:
+        d = d + loss_diagonal(n, codes, gamma)
     Y = (d[:, None] * X).astype(complex if cplx else X.dtype)
     for loc, src, amp in _channel_entries(n, codes, full, channel_list(n, omega, exchange)):
         np.add.at(Y, loc, (amp if cplx else amp.real) * X[src])
     return Y.reshape(x.shape) if vec else Y
 
 
-def sparse_h(n, codes, omega, delta, pairs, exchange=None):
+def sparse_h(n, codes, omega, delta, pairs, exchange=None, gamma=None):
     """CSR H from the same channel list as hv (the reference assembles its CSR
     in assemble.py:277-393 build_H_sparse; used here for the larger CPU
     baseline samples, where a dense matrix does not fit)."""
@@ -180,7 +190,9 @@ def sparse_h(n, codes, omega, delta, pairs, exchange=None):
     codes = np.arange(1 << n, dtype=np.int64) if full else np.asarray(codes, np.int64)
     dim = len(codes)
     d = diagonal(n, codes, delta, pairs)
-    cplx = _is_complex(omega, exchange)
+    cplx = _is_complex(omega, exchange, gamma)
+    if gamma is not None:
+        d = d + loss_diagonal(n, codes, gamma)
     rows, cols, vals = [np.arange(dim)], [np.arange(dim)], [d.astype(complex if cplx else float)]
     for loc, src, amp in _channel_entries(n, codes, full, channel_list(n, omega, exchange)):
         rows.append(loc)
@@ -190,11 +202,11 @@ def sparse_h(n, codes, omega, delta, pairs, exchange=None):
                          shape=(dim, dim))
 
 
-def dense_h(n, codes, omega, delta, pairs, exchange=None):
+def dense_h(n, codes, omega, delta, pairs, exchange=None, gamma=None):
     """Dense H by applying hv to unit vectors (small systems only)."""
     dim = (1 << n) if codes is None else len(codes)
-    E = np.eye(dim, dtype=complex if _is_complex(omega, exchange) else float)
-    return hv(n, codes, omega, delta, pairs, E, exchange=exchange)
+    E = np.eye(dim, dtype=complex if _is_complex(omega, exchange, gamma) else float)
+    return hv(n, codes, omega, delta, pairs, E, exchange=exchange, gamma=gamma)
 
 
 # ------------------------------------------------------------------- KPM
@@ -292,7 +304,7 @@ def segment_drive(t, segments, n):
     return om * np.exp(1j * ph), de
 
 
-def evolve_segments(n, codes, pairs, segments, psi0, t_grid, exchange=None):
+def evolve_segments(n, codes, pairs, segments, psi0, t_grid, exchange=None, gamma=None):
     """Piecewise-constant exact propagation (engine_ed.py:130-147): for each
     output interval and each drive piece, psi <- expm_multiply(-i CONV dt H)."""
     import scipy.sparse as sp
@@ -306,8 +318,9 @@ def evolve_segments(n, codes, pairs, segments, psi0, t_grid, exchange=None):
             om, de = segment_drive(0.5 * (a + b), segments, n)
             key = (tuple(om), tuple(de))
             if key not in cache:
-                cache[key] = (sp.csr_matrix(dense_h(n, codes, om, de, pairs, exchange=exchange))
-                              if len(psi) <= 4096 else sparse_h(n, codes, om, de, pairs, exchange=exchange))
+                cache[key] = (sp.csr_matrix(dense_h(n, codes, om, de, pairs, exchange=exchange, gamma=gamma))
+                              if len(psi) <= 4096
+                              else sparse_h(n, codes, om, de, pairs, exchange=exchange, gamma=gamma))
             psi = expm_multiply((-1j * CONV * (b - a)) * cache[key], psi)
         out.append(psi.copy())
     return out

@@ -416,6 +416,70 @@ def observables_fixture(ref_root: str) -> None:
     print("observables fixture written to", HERE)
 
 
+def loss_fixture(ref_root: str) -> None:
+    """Loss rates gamma (non-Hermitian diagonal, channels.py:69-76):
+    hamiltonian_linear_operator with gamma on a full basis and on a blockade
+    chain, and evolve_manybody (engine_ed.py:153-372) with gamma: full basis
+    with XY exchange and three segments, projected chain with a static drive
+    (the expm_multiply path of engine_ed.py:117-127)."""
+    sys.path.insert(0, ref_root)
+    from src.core.manybody import matrix_free as rmf                    # matrix_free.py
+    from src.core.manybody import engine_ed as red                      # engine_ed.py
+    from src.core.manybody import basis as rbasis                       # basis.py
+    from src.core.manybody import hamiltonian_plan as rplan             # hamiltonian_plan.py
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from energy_level_b200 import configs
+    rng = np.random.default_rng(20261206)
+    out = {}
+    for name, n, edges in (("full7", 7, None), ("chain10", 10, configs.chain_edges(10))):
+        calib = configs.calib_from_positions(configs.chain_positions(n))
+        om = rng.uniform(0.5, 2.0, n)
+        de = rng.uniform(-2.0, 2.0, n)
+        ga = rng.uniform(0.0, 5.0, n)
+        idx = None if edges is None else np.asarray(rbasis.independent_states(n, edges), np.int64)
+        op = rmf.hamiltonian_linear_operator(calib, Om=om, delta=de, gamma=ga, terms=["I1"], basis_indices=idx)
+        x = rng.normal(size=op.shape[0]) + 1j * rng.normal(size=op.shape[0])
+        out["hv_" + name + "_x"] = x
+        out["hv_" + name + "_y"] = op @ x
+        out["hv_" + name + "_om"] = om
+        out["hv_" + name + "_de"] = de
+        out["hv_" + name + "_ga"] = ga
+    # evolution 1: full basis, XY + drive, three segments, loss
+    n = 6
+    xy = configs.xy_chain(n, seed=31)
+    ga = np.linspace(2.0, 8.0, n)
+    segs = [{"t0": 0.0, "Om": np.full(n, 0.9), "delta": xy["delta"]},
+            {"t0": 120.0, "Om": np.full(n, 1.4), "delta": xy["delta"] - 0.4},
+            {"t0": 260.0, "Om": np.full(n, 0.5), "delta": xy["delta"] + 0.2}]
+    t = np.linspace(0.0, 400.0, 6)
+    r = red.evolve_manybody(xy["calib"], psi0="rg" * (n // 2), t_grid=t, segments=segs, gamma=ga,
+                            terms=["I1", "I2"], record_psi=True)
+    out["ev1_t"] = t
+    out["ev1_ga"] = ga
+    out["ev1_seg_t0"] = np.asarray([sg["t0"] for sg in segs])
+    out["ev1_seg_om"] = np.asarray([sg["Om"] for sg in segs])
+    out["ev1_seg_de"] = np.asarray([sg["delta"] for sg in segs])
+    for k in ("pops_atom", "norms", "loss", "S", "corr", "psi_amp"):
+        out["ev1_" + k] = np.asarray(r[k])
+    out["ev1_backend"] = np.asarray(r["backend"])
+    # evolution 2: projected blockade chain, static drive, loss
+    n = 9
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+    plan = rplan.build_plan(calib, Om=np.full(n, 2.0), delta=np.full(n, -1.0), terms=["I1"],
+                            constraint={"kind": "blockade", "edges": configs.chain_edges(n)})
+    ga = np.full(n, 3.0)
+    t = np.linspace(0.0, 300.0, 4)
+    r = red.evolve_manybody(calib, psi0="g" * n, t_grid=t, Om=np.full(n, 2.0), delta=np.full(n, -1.0),
+                            gamma=ga, plan=plan, terms=["I1"], record_psi=True)
+    out["ev2_t"] = t
+    out["ev2_ga"] = ga
+    out["ev2_states"] = np.asarray(r["basis_states"], np.int64)
+    for k in ("pops_atom", "norms", "loss", "S", "corr", "psi_amp"):
+        out["ev2_" + k] = np.asarray(r[k])
+    np.savez_compressed(os.path.join(HERE, "loss.npz"), **out)
+    print("loss fixture written to", HERE)
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     which = sys.argv[2] if len(sys.argv) > 2 else "all"
@@ -427,9 +491,12 @@ if __name__ == "__main__":
         exchange_fixture(root)
     elif which == "observables":
         observables_fixture(root)
+    elif which == "loss":
+        loss_fixture(root)
     else:
         main(root)
         spectrum_fixture(root)
         ramp_fixture(root)
         exchange_fixture(root)
         observables_fixture(root)
+        loss_fixture(root)

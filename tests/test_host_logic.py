@@ -20,14 +20,16 @@ def test_backend_names_and_capabilities():
         backends.normalize_equilibrium_backend("b200-kpm", "gs")
     assert backends.normalize_time_backend("chebyshev-gpu") == "b200-cheb"
     b = backends.TIME_BACKENDS["b200-cheb"]
-    assert b.segments and b.projected and b.return_state and not b.gamma
+    assert b.segments and b.projected and b.return_state and b.gamma
     assert backends.engine_entries()[("b200-cheb", "many")] == ("energy_level_b200.engine", "evolve_manybody")
 
 
 def test_capability_refusals_are_config_conflicts():
+    # loss rates run on the non-Hermitian Taylor path
+    backends.validate_time_capabilities("b200-cheb", gamma=[0.1, 0.0])
     with pytest.raises(model.ConfigConflict) as e:
-        backends.validate_time_capabilities("b200-cheb", gamma=[0.1, 0.0])
-    assert e.value.keys == ("manybody.gamma_mhz",)
+        backends.validate_time_capabilities("b200-cheb", charge_sector=2)
+    assert e.value.keys == ("manybody.charge_sector",)
     # Pauli strings are evaluated on the device ('full' capability, as the ed engine)
     backends.validate_time_capabilities("b200-cheb", pauli_strings=[{"label": "x"}])
     assert backends.TIME_BACKENDS["b200-cheb"].pauli == "full"

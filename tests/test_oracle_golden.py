@@ -223,3 +223,33 @@ def test_entropies_and_corr_match_reference():
     assert abs(ref.entropy_cut(10, g["basis_states"], g["basis_psi"], 5) - float(g["basis_S5"])) < 1e-12
     bits = ref.basis_bits(10, g["basis_states"])
     assert np.allclose(ref.corr_matrix(bits, np.abs(g["basis_psi"]) ** 2), g["basis_corr"], atol=1e-13)
+
+
+@pytest.mark.parametrize("name", ["full7", "chain10"])
+def test_loss_hv_matches_reference(name):
+    from energy_level_b200 import configs
+    g = load("loss")
+    n = 7 if name == "full7" else 10
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+    pairs = [(p["i"], p["j"], p["V"]) for p in calib["pairs"]]
+    codes = None if name == "full7" else ref.independent_states(n, configs.chain_edges(n), None)
+    p = "hv_" + name + "_"
+    y = ref.hv(n, codes, g[p + "om"], g[p + "de"], pairs, g[p + "x"], gamma=g[p + "ga"])
+    assert np.max(np.abs(y - g[p + "y"])) < 1e-12 * max(1.0, np.abs(g[p + "y"]).max())
+
+
+def test_loss_evolution_oracle_matches_reference():
+    from energy_level_b200 import configs
+    g = load("loss")
+    n = 6
+    xy = configs.xy_chain(n, seed=31)
+    pairs = [(p["i"], p["j"], p["V"]) for p in xy["calib"]["pairs"]]
+    ex = [(p["i"], p["j"], p["J"], 0.0) for p in xy["calib"]["pairs"]]
+    segs = [{"t0": float(t0), "Om": om, "delta": de}
+            for t0, om, de in zip(g["ev1_seg_t0"], g["ev1_seg_om"], g["ev1_seg_de"])]
+    psi0 = np.zeros(1 << n, complex)
+    psi0[int("10" * 3, 2)] = 1.0
+    out = ref.evolve_segments(n, None, pairs, segs, psi0, g["ev1_t"], exchange=ex, gamma=g["ev1_ga"])
+    norms = np.asarray([np.vdot(v, v).real for v in out])
+    assert np.allclose(norms, g["ev1_norms"], atol=1e-10, rtol=0)
+    assert np.abs(out[-1] - g["ev1_psi_amp"]).max() < 1e-10
