@@ -221,3 +221,14 @@ def test_batched_refuses_exchange(ctx):
             "edges": configs.chain_edges(8)}
     with pytest.raises(ConfigConflict):
         batched.batched_ground_states([inst])
+
+
+def test_sector_scan_workers_give_identical_rows(ctx):
+    """One worker or four (separate contexts and streams): the same results."""
+    from energy_level_b200.sector_scan import scan_ground_sectors
+    xy = configs.xy_chain(12, seed=2)
+    r1 = scan_ground_sectors(xy["calib"], delta=xy["delta"], Om=np.zeros(12), terms=["I1", "I2"], workers=1)
+    r4 = scan_ground_sectors(xy["calib"], delta=xy["delta"], Om=np.zeros(12), terms=["I1", "I2"], workers=4)
+    assert [r["E0"] for r in r1["per_sector"]] == [r["E0"] for r in r4["per_sector"]]
+    assert [r["gap"] for r in r1["per_sector"]] == [r["gap"] for r in r4["per_sector"]]
+    assert r1["sector"] == r4["sector"] and r1["converged"] and r4["converged"]
