@@ -196,6 +196,137 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev B, HamArgs<S> H, KArgs K
   if (K.want) reduce4(K, q0, q1, q2, q3);
 }
 
+// --------------------------------------------- hop kernel (exchange channels)
+// H with exchange channels on a FULL or TABLE (fixed-excitation, general
+// restricted) basis of at most 32 sites: the generic kernel's per-element
+// work, but the J channels are visited as hops -- every (set bit a, clear bit
+// b) pair of the row, k (n - k) of them, with the amplitude from a table in
+// shared memory -- instead of testing every site pair, codes and table ranks
+// are 32-bit, and only the pairs with a nonzero A are scanned.
+__device__ __forceinline__ int rank32(const BasisDev &B, uint32_t c) {
+  if (B.layout == EL_LAYOUT_FULL) return (int)c;
+  const uint32_t p = c >> B.L, sfx = c & ((1u << B.L) - 1u);
+  const int64_t off = B.pre_off[p];
+  if (off < 0) return -1;
+  const int32_t rr = B.suf_rank[((uint32_t)B.pre_cls[p] << B.L) + sfx];
+  return rr < 0 ? -1 : (int)off + rr;
+}
+
+template <typename S, bool C>
+__global__ void __launch_bounds__(256) k_apply_hop(BasisDev B, HamArgs<S> H, KArgs K, const double *hop,
+                                                   const ExPair *pxA, int npxA) {
+  typedef Val<S, C> V;
+  extern __shared__ __align__(16) unsigned char hop_smem[];
+  const int n = B.n;
+  S *hre_t = reinterpret_cast<S *>(hop_smem);
+  S *him_t = hre_t + n * n;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+    hre_t[i] = (S)hop[i];
+    if constexpr (C) him_t[i] = (S)hop[n * n + i];
+  }
+  __syncthreads();
+  const uint32_t full = (n >= 32) ? 0xffffffffu : ((1u << n) - 1u);
+  const int64_t total = B.dim * K.nvec;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const int64_t row = t >> K.lognv;
+    const int64_t v = t & (K.nvec - 1);
+    const uint32_t code = (B.layout == EL_LAYOUT_FULL) ? (uint32_t)row : (uint32_t)B.codes[row];
+    const V xr = V::load(K.x, t);
+    S hre = 0, him = 0, dsum = 0, dimg = 0;
+    for (uint32_t m = code; m; m &= m - 1) {
+      const int k = __ffs(m) - 1;
+      dsum += H.delta[k];
+      if constexpr (C) dimg += H.loss[k];
+    }
+    // sigma^x channels (bits with a nonzero Omega)
+    for (int k = 0; k < n; ++k) {
+      const bool set = (code >> k) & 1u;
+      const S are = H.up_re[k];
+      const S aim = C ? (set ? H.up_im[k] : -H.up_im[k]) : S(0);
+      if (are == S(0) && aim == S(0)) continue;
+      const int tg = rank32(B, code ^ (1u << k));
+      if (tg < 0) continue;
+      const V xs = V::load(K.x, ((int64_t)tg << K.lognv) + v);
+      if constexpr (C) { hre += are * xs.re - aim * xs.im; him += are * xs.im + aim * xs.re; }
+      else { hre += are * xs.v; }
+    }
+    // J channels: move one excitation from a set bit a to a clear bit b
+    for (uint32_t ma = code; ma; ma &= ma - 1) {
+      const int a = __ffs(ma) - 1;
+      const S *hr = hre_t + a * n;
+      const S *hi = him_t + a * n;
+      for (uint32_t mb = ~code & full; mb; mb &= mb - 1) {
+        const int b = __ffs(mb) - 1;
+        const S are = hr[b];
+        const S aim = C ? hi[b] : S(0);
+        if (are == S(0) && aim == S(0)) continue;
+        const int tg = rank32(B, code ^ (1u << a) ^ (1u << b));
+        if (tg < 0) continue;
+        const V xs = V::load(K.x, ((int64_t)tg << K.lognv) + v);
+        if constexpr (C) { hre += are * xs.re - aim * xs.im; him += are * xs.im + aim * xs.re; }
+        else { hre += are * xs.v; }
+      }
+    }
+    // A channels: create or remove both excitations
+    for (int p = 0; p < npxA; ++p) {
+      const ExPair e = pxA[p];
+      const bool si = (code >> e.bi) & 1u, sj = (code >> e.bj) & 1u;
+      if (si != sj) continue;
+      const S are = (S)e.are;
+      const S aim = C ? (S)(si ? e.aim : -e.aim) : S(0);
+      const int tg = rank32(B, code ^ (1u << e.bi) ^ (1u << e.bj));
+      if (tg < 0) continue;
+      const V xs = V::load(K.x, ((int64_t)tg << K.lognv) + v);
+      if constexpr (C) { hre += are * xs.re - aim * xs.im; him += are * xs.im + aim * xs.re; }
+      else { hre += are * xs.v; }
+    }
+    if (!K.skip_diag) {
+      dsum += H.diagV[row];
+      if constexpr (C) {
+        hre += dsum * xr.re - dimg * xr.im;
+        him += dsum * xr.im + dimg * xr.re;
+      } else {
+        hre += dsum * xr.v;
+      }
+    }
+    V yv;
+    if constexpr (C) {
+      yv.re = (S)K.a * hre + (S)K.b * xr.re;
+      yv.im = (S)K.a * him + (S)K.b * xr.im;
+      if (K.z) { const V zv = V::load(K.z, t); yv.re += (S)K.c * zv.re; yv.im += (S)K.c * zv.im; }
+      if (K.acc) {
+        V av = V::load(K.acc, t);
+        av.re += (S)K.w_re * yv.re - (S)K.w_im * yv.im;
+        av.im += (S)K.w_re * yv.im + (S)K.w_im * yv.re;
+        av.store(K.acc, t);
+      }
+    } else {
+      yv.v = (S)K.a * hre + (S)K.b * xr.v;
+      if (K.z) { const V zv = V::load(K.z, t); yv.v += (S)K.c * zv.v; }
+      if (K.acc) { V av = V::load(K.acc, t); av.v += (S)K.w_re * yv.v; av.store(K.acc, t); }
+    }
+    if (K.y) yv.store(K.y, t);
+    if (K.want) {
+      if constexpr (C) {
+        const double xre = xr.re, xim = xr.im, yre = yv.re, yim = yv.im;
+        q0 += xre * xre + xim * xim;
+        q1 += xre * yre + xim * yim;
+        q2 += xre * yim - xim * yre;
+        q3 += yre * yre + yim * yim;
+      } else {
+        const double xd = xr.v, yd = yv.v;
+        q0 += xd * xd;
+        q1 += xd * yd;
+        q3 += yd * yd;
+        if (K.probe) q2 += yd * (double)V::load(K.probe, t).v;
+      }
+    }
+  }
+  if (K.want) reduce4(K, q0, q1, q2, q3);
+}
+
 // ------------------------------------------------- row kernel (FULL/CHAIN/RING)
 // One thread per row and all NV vectors of that row (NV <= 8): the code of a
 // row is recovered once and every flip gather moves the row's whole NV-vector
@@ -1245,6 +1376,19 @@ int launch_apply(el_ctx *ctx, el_ham *h, const ApplyArgs &A) {
     if (rc) return rc;
   }
   if (row_kernel_ok(h, A)) return launch_apply_row(ctx, h, A, B, K);
+  if (!h->px.empty() && (B.layout == EL_LAYOUT_FULL || B.layout == EL_LAYOUT_TABLE) && B.n <= 32 &&
+      B.dim < ((int64_t)1 << 31)) {
+    const size_t sm = (size_t)B.n * B.n * (single ? sizeof(float) : sizeof(double)) * 2;
+    switch (A.dtype) {
+      case EL_F32: k_apply_hop<float, false><<<grid, 256, sm, ctx->stream>>>(B, ham_args<float>(h, h->d_diagV32), K, h->d_hop, h->d_pxA, h->npxA); break;
+      case EL_F64: k_apply_hop<double, false><<<grid, 256, sm, ctx->stream>>>(B, ham_args<double>(h, h->d_diagV64), K, h->d_hop, h->d_pxA, h->npxA); break;
+      case EL_C64: k_apply_hop<float, true><<<grid, 256, sm, ctx->stream>>>(B, ham_args<float>(h, h->d_diagV32), K, h->d_hop, h->d_pxA, h->npxA); break;
+      case EL_C128: k_apply_hop<double, true><<<grid, 256, sm, ctx->stream>>>(B, ham_args<double>(h, h->d_diagV64), K, h->d_hop, h->d_pxA, h->npxA); break;
+      default: return fail(ctx, EL_EINVAL, "unknown dtype %d", A.dtype);
+    }
+    EL_LAUNCH_CHECK(ctx);
+    return EL_OK;
+  }
   switch (A.dtype) {
     case EL_F32:
       k_apply<float, false><<<grid, 256, 0, ctx->stream>>>(B, ham_args<float>(h, h->d_diagV32), K);
@@ -1569,20 +1713,47 @@ int el_ham_set_exchange(el_ctx *ctx, el_ham *h, int n_pairs, const int32_t *pi,
     if (e.jim != 0.0 || e.aim != 0.0) cplx = true;
     px.push_back(e);
   }
-  ExPair *d = nullptr;
-  if (!px.empty()) {
-    cudaError_t e = cudaMalloc(&d, px.size() * sizeof(ExPair));
-    if (e != cudaSuccess) return el::fail(ctx, EL_ENOMEM, "cannot allocate exchange pairs (%s)", cudaGetErrorString(e));
-    e = el::copy(ctx, d, px.data(), px.size() * sizeof(ExPair), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) { cudaFree(d); return el::cuda_fail(ctx, e, "exchange pairs"); }
+  // hop table of the J channels and the list of A pairs
+  std::vector<double> hop(2 * (size_t)n * n, 0.0);
+  std::vector<ExPair> pxA;
+  for (const ExPair &e : px) {
+    // row (i, j) = (r, g): bit bi set, bj clear -> J; row (g, r) -> conj(J)
+    hop[(size_t)e.bi * n + e.bj] += e.jre;
+    hop[(size_t)n * n + (size_t)e.bi * n + e.bj] += e.jim;
+    hop[(size_t)e.bj * n + e.bi] += e.jre;
+    hop[(size_t)n * n + (size_t)e.bj * n + e.bi] -= e.jim;
+    if (e.are != 0.0 || e.aim != 0.0) pxA.push_back(e);
   }
-  // the previous list may still be read by work queued on the stream
-  if (h->d_px) {
+  ExPair *d = nullptr, *dA = nullptr;
+  double *dh = nullptr;
+  auto upload = [&](void **dst, const void *src, size_t bytes) -> cudaError_t {
+    cudaError_t e = cudaMalloc(dst, bytes);
+    if (e != cudaSuccess) return e;
+    e = el::copy(ctx, *dst, src, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e;
+  };
+  if (!px.empty()) {
+    cudaError_t e = upload((void **)&d, px.data(), px.size() * sizeof(ExPair));
+    if (e == cudaSuccess) e = upload((void **)&dh, hop.data(), hop.size() * sizeof(double));
+    if (e == cudaSuccess && !pxA.empty()) e = upload((void **)&dA, pxA.data(), pxA.size() * sizeof(ExPair));
+    if (e != cudaSuccess) {
+      cudaFree(d); cudaFree(dh); cudaFree(dA);
+      cudaGetLastError();
+      return el::fail(ctx, EL_ENOMEM, "cannot store exchange channels (%s)", cudaGetErrorString(e));
+    }
+  }
+  // the previous lists may still be read by work queued on the stream
+  if (h->d_px || h->d_hop || h->d_pxA) {
     EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     cudaFree(h->d_px);
+    cudaFree(h->d_hop);
+    cudaFree(h->d_pxA);
   }
   h->d_px = d;
+  h->d_hop = dh;
+  h->d_pxA = dA;
+  h->npxA = (int)pxA.size();
   h->px.swap(px);
   h->px_complex = cplx;
   h->complex_drive = h->drive_complex || h->px_complex || h->lossy;
@@ -1601,6 +1772,8 @@ int el_ham_destroy(el_ham *h) {
   if (h->d_diagV64) cudaFree(h->d_diagV64);
   if (h->d_diagV32) cudaFree(h->d_diagV32);
   if (h->d_px) cudaFree(h->d_px);
+  if (h->d_hop) cudaFree(h->d_hop);
+  if (h->d_pxA) cudaFree(h->d_pxA);
   delete h;
   return EL_OK;
 }

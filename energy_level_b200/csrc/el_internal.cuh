@@ -103,6 +103,13 @@ struct el_ham {
   // exchange channels (I2 J, I3 A); empty for the Omega/delta/V model
   std::vector<ExPair> px;
   ExPair *d_px = nullptr;
+  // the same channels for the hop kernel: J as a table hop[a][b] (bit
+  // positions, a row with bit a = r and bit b = g gains hop[a][b] x[row with
+  // the excitation moved from a to b]; re/im, n*n each) and the pairs with a
+  // nonzero A in their own list
+  double *d_hop = nullptr;     // [2][n*n]
+  ExPair *d_pxA = nullptr;
+  int npxA = 0;
   bool drive_complex = false;     // Omega has an imaginary part
   bool px_complex = false;        // some J or A has an imaginary part
   // loss: imaginary diagonal -gamma_i/2 (in the evolution's units) per bit
