@@ -701,10 +701,12 @@ def native_ramp31(h, args):
     obs_ms = {}
     for tag, prs in (("sites", []), ("sites_and_465_pairs", all_pairs)):
         solvers.spin_observables(ham32, psi32, prs)
+        torch.cuda.nvtx.range_push("observables_" + tag)  # ncu --nvtx-include selects these launches
         t0 = time.perf_counter()
         for _ in range(5):
             solvers.spin_observables(ham32, psi32, prs)
         obs_ms[tag] = (time.perf_counter() - t0) / 5 * 1e3
+        torch.cuda.nvtx.range_pop()
     cpu = None
     if h.rank == 0 and h.world == 1 and not args.no_cpu:
         cpu = cpu_ramp_sample(basis.dim)
@@ -989,7 +991,9 @@ def native_scan_xy20(h, args):
     for _ in range(args.warmup):
         f()
     nh = 50
+    torch.cuda.nvtx.range_push("scan_hv_largest")      # ncu --nvtx-include selects these launches
     th, _, _ = h.timed(f, nh)
+    torch.cuda.nvtx.range_pop()
     th /= nh
     # the workers' contexts launch the scan's kernels (the harness context none)
     l0 = sum(c.launches for c in scan_obj.ctxs)

@@ -101,7 +101,17 @@ __global__ void __launch_bounds__(256, 2) k_obs_items(BasisDev B, const S *__res
       const bool sj = (code >> bj) & 1ULL;
       if (si && sj) acc[q][0] += p;
       if (!si && sj) {
-        const int64_t t = el::rank_any(B, code ^ ((1ULL << bi) | (1ULL << bj)));
+        // on chain / ring sectors: clear bit j (which keeps the state in the
+        // sector), then set bit i -- two O(1) single flips instead of a
+        // re-rank; other layouts rank the target directly (on a
+        // fixed-excitation sector the intermediate state is outside it)
+        int64_t t;
+        if (B.layout == EL_LAYOUT_CHAIN || B.layout == EL_LAYOUT_RING) {
+          const int64_t t1 = el::flip_target(B, code, r, bj);
+          t = (t1 >= 0) ? el::flip_target(B, code ^ (1ULL << bj), t1, bi) : -1;
+        } else {
+          t = el::rank_any(B, code ^ ((1ULL << bi) | (1ULL << bj)));
+        }
         if (t >= 0) {
           double wr, wi;
           load_amp<S, C>(psi, t, wr, wi);

@@ -176,3 +176,28 @@ def test_evolution_pauli_strings_and_loops(ctx):
     with pytest.raises(ValueError):
         evolve_manybody(xy["calib"], "rg" * 3, t, Om=np.full(n, 0.7), terms=["I1", "I2"],
                         link_pairs=[(0, 9)])
+
+
+@pytest.mark.parametrize("kind", ["charge", "ring"])
+def test_spin_observables_other_layouts_match_oracle(ctx, kind):
+    """Fixed-excitation (table-ranked) and ring sectors against the oracle."""
+    import torch
+    from energy_level_b200 import solvers
+    from energy_level_b200.core import Basis, Hamiltonian
+    n = 10
+    if kind == "charge":
+        b = Basis(ctx, n, kind="charge", k=4)
+        codes = ref.number_sector_basis(n, 4)
+    else:
+        b = Basis(ctx, n, kind="blockade", edges=configs.ring_edges(n))
+        codes = ref.independent_states(n, configs.ring_edges(n), None)
+    h = Hamiltonian(ctx, b, np.zeros(n), np.zeros(n), [])
+    rng = np.random.default_rng(8)
+    v = rng.normal(size=b.dim) + 1j * rng.normal(size=b.dim)
+    v /= np.linalg.norm(v)
+    want = ref.spin_observables(n, codes, v)
+    pairs = [(i, j) for i in range(n) for j in range(n) if i != j]
+    ob = solvers.spin_observables(h, torch.as_tensor(v, dtype=torch.complex128, device=ctx.device), pairs)
+    assert np.abs(ob["sm"] - want["sm"]).max() < 1e-12
+    _, XY = _matrices(ob, n, pairs)
+    assert np.abs(XY - want["xy_corr"]).max() < 1e-12
