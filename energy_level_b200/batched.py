@@ -77,6 +77,17 @@ class BatchedGroundStates:
         self.ctx.call('el_batch_run', self.handle, C.c_int(int(threads or t)),
                       C.c_int(int(ctas_per_sm or c)), C.c_uint64(int(seed)))
 
+    def run_coop(self, seed=0, check_every=8, reorth_passes=2):
+        """Each instance with the whole GPU: one cooperative launch per
+        instance, Krylov slices in shared memory, full reorthogonalisation
+        every step (el_batch_run_coop); for a few instances of a few
+        thousand rows.  reorth_passes: Gram-Schmidt passes per step; one
+        pass forms beta from |w|^2 - |c|^2, which loses accuracy when beta
+        is small against |H v| (near an invariant subspace), so two is the
+        safe default."""
+        self.ctx.call('el_batch_run_coop', self.handle, C.c_int(int(reorth_passes)), C.c_int(int(check_every)),
+                      C.c_uint64(int(seed)))
+
     def results(self):
         e0 = np.zeros(self.count)
         gap = np.zeros(self.count)
@@ -133,12 +144,34 @@ class BatchedGroundStates:
             pass
 
 
-def batched_ground_states(instances, dtype='float32', max_iter=200, tol=None, device=0, tune=False):
+COOP_MAX_INSTANCES = 8
+
+
+def batched_ground_states(instances, dtype='float32', max_iter=200, tol=None, device=0, tune=False,
+                          mode='auto'):
+    """Ground energies and gaps of many instances.  mode 'batch': one
+    persistent launch, one CTA per instance; 'coop': one cooperative launch
+    per instance over many CTAs; 'auto': 'coop' for a few instances
+    (<= COOP_MAX_INSTANCES) that fit it, else 'batch'."""
+    if mode not in ('auto', 'batch', 'coop'):
+        raise ValueError("mode must be 'auto', 'batch' or 'coop'")
     b = BatchedGroundStates(instances, dtype=dtype, max_iter=max_iter, tol=tol, device=device)
-    if tune:
-        b.autotune()
-    b.run()
-    out = b.results()
-    out['config'] = b.config
-    b.close()
+    used = 'batch'
+    try:
+        if mode == 'coop' or (mode == 'auto' and b.count <= COOP_MAX_INSTANCES):
+            try:
+                b.run_coop(check_every=16)
+                used = 'coop'
+            except ValueError:
+                if mode == 'coop':
+                    raise
+        if used == 'batch':
+            if tune:
+                b.autotune()
+            b.run()
+        out = b.results()
+        out['config'] = b.config if used == 'batch' else 'coop'
+        out['mode'] = used
+    finally:
+        b.close()
     return out

@@ -451,6 +451,286 @@ __global__ void __launch_bounds__(NT) k_lanczos_batch(const BatchArgs A) {
   }
 }
 
+// ------------------------------------------------ one instance, whole GPU
+// Cooperative Lanczos for one instance that is too small to fill the GPU
+// with vectors but too slow on one SM: the rows are split over G CTAs (NT
+// rows each, one row per thread) and every CTA keeps its slice of the
+// Krylov basis in shared memory, so the full reorthogonalisation (classical
+// Gram-Schmidt, twice, every step) touches only shared memory; the
+// coefficients are summed across CTAs through small global arrays.  A step
+// needs two grid barriers per projection sum (partials, then the sums, each
+// formed by one CTA) -- the last one also carries |w|^2 before it, so that
+// |w_final|^2 = |w|^2 - |c|^2 costs no further barrier -- and one to publish
+// the next vector, whose entries the sigma^x flips of every CTA read: five
+// with two Gram-Schmidt passes, three with one.  Every sum is
+// formed once, in a fixed order, and read by all CTAs, so every CTA holds
+// the same alpha/beta bits and takes the same decisions.  The grid barrier is a
+// monotonic arrival counter polled by one thread per CTA with a bounded
+// number of polls; a timeout sets the error flag, after which no barrier
+// waits again and the kernel runs out its bounded loop.
+struct CoopArgs {
+  int p, m, nctas, check_every, passes, pad2;
+  double tol, eps;
+  const Inst *inst;
+  const double *diag;
+  void *vpub;                   // [dim] the current Lanczos vector, published
+  double *part;                 // [2][nctas][MAXIT + 2] per-CTA partial sums
+  double *tot;                  // [2][MAXIT + 2] the sums, each formed by one CTA
+  unsigned *bar;                // arrival counter, zero at launch
+  int *err;
+  uint64_t seed;
+  double *e0, *e1, *res, *gap;
+  int *iters, *conv;
+};
+
+__device__ __forceinline__ void grid_barrier(const CoopArgs &G, unsigned &gen) {
+  __syncthreads();
+  gen += (unsigned)G.nctas;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(G.bar, 1u);
+    if (!*(volatile int *)G.err) {
+      int polls = 0;
+      while (*(volatile unsigned *)G.bar < gen) {
+        if (++polls > (1 << 22)) { atomicExch(G.err, 1); break; }
+        if (*(volatile int *)G.err) break;
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Dynamic shared memory of the cooperative kernel: the Krylov slice
+// [m + 1][NT + 1] then two inverse-iteration buffers.
+__host__ __device__ inline size_t coop_slice_bytes(int m, int nt, int es) {
+  return (((size_t)(m + 1) * (nt + 1) * es) + 15) / 16 * 16;
+}
+constexpr size_t COOP_WORK_BYTES = 2 * (6 * MAXIT + 8) * sizeof(double);
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_lanczos_coop(const CoopArgs G) {
+  extern __shared__ __align__(16) unsigned char coop_smem[];
+  T *Vs = reinterpret_cast<T *>(coop_smem);           // [m + 1][NT + 1]
+  constexpr int PITCH = NT + 1;
+  __shared__ Inst I;
+  __shared__ uint64_t fib[MAXN + 3];
+  __shared__ double red[NT / 32 > 0 ? NT / 32 : 1];
+  __shared__ double al[MAXIT], be[MAXIT];
+  __shared__ double cs[MAXIT + 2];
+  __shared__ T wsm[NT];
+  __shared__ double s_th[2], s_res[2];
+  __shared__ double prev_th[2], prev_dth[2];
+  __shared__ int have_prev, s_next;
+  __shared__ int s_done, s_err;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    fib[0] = 0; fib[1] = 1;
+    for (int i = 2; i < MAXN + 3; ++i) fib[i] = fib[i - 1] + fib[i - 2];
+    I = G.inst[G.p];
+    s_err = 0;
+    have_prev = 0;
+    s_next = 16;
+    s_th[0] = s_th[1] = 0.0; s_res[0] = s_res[1] = 1e300; s_done = 0;
+  }
+  __syncthreads();
+  const int64_t dim = I.dim;
+  const int64_t row = (int64_t)blockIdx.x * NT + tid;
+  const bool valid = row < dim;
+  const double *D = G.diag + I.off;
+  T *vpub = reinterpret_cast<T *>(G.vpub);
+  const int m = (int)min((int64_t)G.m, dim);
+  // inverse-iteration buffers of lanes 0 and 1 follow the slice in dynamic memory
+  double *work = reinterpret_cast<double *>(coop_smem + coop_slice_bytes(m, NT, (int)sizeof(T)));
+  unsigned gen = 0;
+  int slot = 0;
+  auto part = [&](int sl, int c, int k) -> double * {
+    return G.part + ((size_t)sl * G.nctas + c) * (MAXIT + 2) + k;
+  };
+  // partials part(slot, *, k), k < nk, written -> cs[k] = their sum in
+  // every CTA.  CTA c forms the sums k = c, c + G, ... (one warp per sum,
+  // lanes over CTAs, fixed tree) into tot, then every CTA reads tot: two
+  // barriers, O(nk) loads per CTA instead of O(nk x G)
+  auto reduce_all = [&](int nk) {
+    grid_barrier(G, gen);
+    const int lane = tid & 31, warp = tid >> 5;
+    double *tt = G.tot + (size_t)slot * (MAXIT + 2);
+    for (int k = blockIdx.x + warp * G.nctas; k < nk; k += G.nctas * (NT / 32)) {
+      double v = 0.0;
+      for (int cc = lane; cc < G.nctas; cc += 32) v += __ldcg(part(slot, cc, k));
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) tt[k] = v;
+    }
+    grid_barrier(G, gen);
+    for (int k = tid; k < nk; k += NT) cs[k] = __ldcg(&tt[k]);
+    slot ^= 1;
+    __syncthreads();
+  };
+  // sum over CTAs of a block-reduced scalar
+  auto grid_scalar = [&](double v) -> double {
+    v = block_sum<NT>(v, red);
+    if (tid == 0) *part(slot, blockIdx.x, 0) = v;
+    reduce_all(1);
+    return cs[0];
+  };
+  // start vector: counter-based Gaussian (same stream as the batched kernel)
+  double x0 = 0.0;
+  if (valid) {
+    const uint64_t h1 = el::counter_hash(G.seed + G.p, 0x77, (uint64_t)row);
+    const uint64_t h2 = el::counter_hash(G.seed + G.p, 0x99, (uint64_t)row);
+    const double u1 = ((h1 >> 11) + 1.0) * (1.0 / 9007199254740993.0);
+    const double u2 = (h2 >> 11) * (1.0 / 9007199254740992.0);
+    x0 = (double)(T)(sqrt(-2.0 * log(u1)) * cospi(2.0 * u2));
+  }
+  const double n0 = grid_scalar(x0 * x0);
+  {
+    const T v = (T)(x0 / sqrt(n0));
+    Vs[tid] = valid ? v : (T)0;
+    if (valid) vpub[row] = v;
+  }
+  grid_barrier(G, gen);
+  int steps = 0;
+  double bnext = 0.0, anorm = 0.0;
+  for (int j = 0; j < m; ++j) {
+    // a barrier timed out somewhere: stop (the flag is read once per CTA)
+    if (tid == 0) s_err = *(volatile int *)G.err;
+    __syncthreads();
+    if (s_err) break;
+    // w = H v_j (flip partners read from the published vector)
+    double w = 0.0;
+    if (valid) {
+      const uint64_t code = unrank_b(I, fib, row);
+      w = D[row] * (double)Vs[(size_t)j * PITCH + tid];
+      for (int k = 0; k < I.n; ++k) {
+        const double amp = I.om[k];
+        if (amp == 0.0) continue;
+        const int64_t t = flip_b(I, fib, code, row, k);
+        if (t >= 0) w += amp * (double)__ldcg(&vpub[t]);
+      }
+    }
+    // classical Gram-Schmidt against v_0..v_j, G.passes times; alpha = sum
+    // of the v_j coefficients.  The last pass also sums |w|^2 (slot j + 1).
+    double alpha = 0.0, b2 = 0.0;
+    for (int pass = 0; pass < G.passes; ++pass) {
+      const int last_pass = (pass == G.passes - 1);
+      wsm[tid] = (T)w;
+      __syncthreads();
+      for (int k = tid; k <= j; k += NT) {
+        const T *vk = Vs + (size_t)k * PITCH;
+        double c0 = 0.0, c1 = 0.0;
+        int r = 0;
+        for (; r + 1 < NT; r += 2) {
+          c0 += (double)vk[r] * (double)wsm[r];
+          c1 += (double)vk[r + 1] * (double)wsm[r + 1];
+        }
+        for (; r < NT; ++r) c0 += (double)vk[r] * (double)wsm[r];
+        *part(slot, blockIdx.x, k) = c0 + c1;
+      }
+      if (last_pass) {
+        const double ww = block_sum<NT>(valid ? w * w : 0.0, red);
+        if (tid == 0) *part(slot, blockIdx.x, j + 1) = ww;
+      }
+      reduce_all(j + 1 + last_pass);
+      alpha += cs[j];
+      if (last_pass) {
+        double cc2 = 0.0;
+        for (int k = 0; k <= j; ++k) cc2 += cs[k] * cs[k];
+        b2 = cs[j + 1] - cc2;
+      }
+      if (valid) {
+        double acc0 = w, acc1 = 0.0;
+        int k = 0;
+        for (; k + 1 <= j; k += 2) {
+          acc0 -= cs[k] * (double)Vs[(size_t)k * PITCH + tid];
+          acc1 -= cs[k + 1] * (double)Vs[(size_t)(k + 1) * PITCH + tid];
+        }
+        for (; k <= j; ++k) acc0 -= cs[k] * (double)Vs[(size_t)k * PITCH + tid];
+        w = (double)(T)(acc0 + acc1);
+      }
+      __syncthreads();
+    }
+    bnext = sqrt(fmax(b2, 0.0));
+    anorm = fmax(anorm, fabs(alpha) + bnext);
+    if (tid == 0) { al[j] = alpha; be[j] = bnext; }
+    __syncthreads();
+    steps = j + 1;
+    const int next_check = s_next;
+    const bool invariant = !(bnext > 1e-12 * fmax(1.0, anorm));
+    // Ritz values and residual estimates at step next_check (and at the
+    // end).  By Cauchy interlacing the q-th Ritz value never rises as the
+    // tridiagonal grows, so the previous value bounds it from above; a
+    // Sturm count confirms a narrow lower bound below it (else the
+    // Gershgorin bound is used), which saves most multisection rounds.  The
+    // two residual estimates (inverse iteration) run on lanes 0 and 1.
+    const bool check = invariant || (j + 1 == m) || (steps >= next_check);
+    if (check && tid < 32) {
+      const int mm = steps;
+      double glo = 1e300, ghi = -1e300;
+      for (int i = 0; i < mm; ++i) {
+        const double rr = (i > 0 ? fabs(be[i - 1]) : 0.0) + (i + 1 < mm ? fabs(be[i]) : 0.0);
+        glo = fmin(glo, al[i] - rr);
+        ghi = fmax(ghi, al[i] + rr);
+      }
+      const double scale = fmax(1.0, fmax(fabs(glo), fabs(ghi)));
+      glo -= 1e-9 * scale;
+      ghi += 1e-9 * scale;
+      const int ne = mm >= 2 ? 2 : 1;
+      double th[2] = {0.0, 0.0};
+      for (int q = 0; q < ne; ++q) {
+        double lo = glo, hi = ghi;
+        if (have_prev) {
+          hi = fmin(ghi, prev_th[q] + 1e-12 * scale);
+          const double d = fmax(16.0 * prev_dth[q], 1e-10 * scale);
+          const double cand = hi - d;
+          if (cand > glo && sturm(al, be, mm, cand) <= q) lo = cand;
+        }
+        th[q] = warp_eig(al, be, mm, q, lo, hi);
+      }
+      if (tid < ne) {
+        const double r = bnext * last_component(al, be, mm, th[tid], work + (size_t)tid * (6 * MAXIT + 8));
+        s_res[tid] = r;
+        s_th[tid] = th[tid];
+      }
+      __syncwarp();
+      if (tid == 0) {
+        bool ok = (ne == 2);
+        double worst = 0.0;
+        for (int q = 0; q < ne; ++q) {
+          const double lim = G.tol * fmax(1.0, fabs(s_th[q]));
+          ok = ok && (s_res[q] <= lim);
+          worst = fmax(worst, s_res[q] / lim);
+        }
+        s_done = (ok || invariant || j + 1 == m) ? 1 : 0;
+        // far from converged: look again later
+        s_next = mm + (worst > 1e3 ? 4 : 1) * G.check_every;
+      }
+      if (tid < ne) {
+        prev_dth[tid] = have_prev ? fmax(prev_th[tid] - th[tid], 0.0) : fabs(ghi - glo);
+        prev_th[tid] = th[tid];
+      }
+      if (tid == 0) have_prev = 1;
+    }
+    __syncthreads();
+    if (s_done) break;
+    // v_{j+1} = w / beta, into the shared slice and the published vector
+    const T vn = (T)(w / bnext);
+    Vs[(size_t)(j + 1) * PITCH + tid] = valid ? vn : (T)0;
+    if (valid) vpub[row] = vn;
+    grid_barrier(G, gen);
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    const int p = G.p;
+    G.e0[p] = s_th[0];
+    G.e1[p] = s_th[1];
+    G.gap[p] = s_th[1] - s_th[0];
+    G.res[p] = fmax(s_res[0], s_res[1]);
+    G.iters[p] = steps;
+    G.conv[p] = (!*(volatile int *)G.err && s_res[0] <= G.tol * fmax(1.0, fabs(s_th[0])) &&
+                 s_res[1] <= G.tol * fmax(1.0, fabs(s_th[1]))) ? 1 : 0;
+  }
+}
+
 // diagonal of every instance: V part + delta part, concatenated
 __global__ void k_batch_diag(int count, const Inst *inst, const double *Vmats, const double *deltas,
                              double *diag) {
@@ -500,6 +780,12 @@ struct el_batch_impl {
   void *ws = nullptr;
   size_t ws_bytes = 0;
   int device = 0;
+  std::vector<int64_t> dims;        // per processing position
+  // cooperative solver workspace
+  void *c_vpub = nullptr;
+  double *c_part = nullptr;
+  unsigned *c_sync = nullptr;       // [0] arrival counter, [1] error flag
+  int c_nctas = 0;
 };
 
 }  // namespace
@@ -567,6 +853,7 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
       Vm[(size_t)p * MAXN * MAXN + qb * MAXN + qa] += V[q];
     }
     off += dims[i];
+    b->dims.push_back(dims[i]);
     b->dim_max = std::max(b->dim_max, dims[i]);
   }
   b->total_rows = off;
@@ -638,6 +925,89 @@ int el_batch_run(el_ctx *ctx, el_batch *b, int threads, int ctas_per_sm, uint64_
   return EL_OK;
 }
 
+int el_batch_run_coop(el_ctx *ctx, el_batch *b, int reorth_passes, int check_every, uint64_t seed) {
+  if (!ctx || !b) return EL_EINVAL;
+  if (check_every < 1) return fail(ctx, EL_EINVAL, "check_every must be >= 1");
+  if (reorth_passes < 1 || reorth_passes > 2) return fail(ctx, EL_EINVAL, "reorth_passes must be 1 or 2");
+  EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const size_t es = b->dtype == EL_F32 ? 4 : 8;
+  const int m = b->max_iter;
+  // threads (= rows) per CTA: the smallest power of two >= 32 that keeps
+  // the grid within 64 CTAs, then the Krylov slice must fit shared memory
+  // and the grid must be co-resident (one CTA per SM)
+  struct Plan { int nt, nctas; size_t smem; };
+  std::vector<Plan> plans(b->count);
+  int nctas_max = 0;
+  for (int p = 0; p < b->count; ++p) {
+    const int64_t dim = b->dims[p];
+    int nt = 32;
+    while (nt < 1024 && (dim + nt - 1) / nt > 64) nt <<= 1;
+    auto slice = [&](int t) { return coop_slice_bytes((int)std::min<int64_t>(m, dim), t, (int)es); };
+    // a slice too large for shared memory: more, narrower CTAs (up to one per SM)
+    while (slice(nt) > 160 * 1024 && nt > 32 && (dim + nt / 2 - 1) / (nt / 2) <= sms) nt >>= 1;
+    const int64_t g = (dim + nt - 1) / nt;
+    const size_t smem = slice(nt) + COOP_WORK_BYTES;
+    if (g > sms || slice(nt) > 160 * 1024)
+      return fail(ctx, EL_EINVAL, "instance of dimension %lld is too large for the cooperative solver "
+                  "(use el_batch_run)", (long long)dim);
+    plans[p] = {nt, (int)g, smem};
+    nctas_max = std::max(nctas_max, (int)g);
+  }
+  if (!b->c_vpub || nctas_max > b->c_nctas) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx->stream, &cs);
+    if (cs != cudaStreamCaptureStatusNone) return fail(ctx, EL_EINVAL, "run the batch once before capturing it");
+    EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(b->c_vpub); cudaFree(b->c_part); cudaFree(b->c_sync);
+    b->c_vpub = nullptr; b->c_part = nullptr; b->c_sync = nullptr; b->c_nctas = 0;
+    cudaError_t e = cudaMalloc(&b->c_vpub, (size_t)b->dim_max * es);
+    if (e == cudaSuccess) e = cudaMalloc(&b->c_part, ((size_t)2 * nctas_max + 2) * (MAXIT + 2) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->c_sync, 2 * sizeof(unsigned));
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, EL_ENOMEM, "cooperative workspace"); }
+    b->c_nctas = nctas_max;
+  }
+  for (int p = 0; p < b->count; ++p) {
+    const Plan &P = plans[p];
+    CoopArgs G;
+    memset(&G, 0, sizeof G);
+    G.p = p; G.m = m; G.nctas = P.nctas; G.check_every = check_every; G.passes = reorth_passes;
+    G.tol = b->tol; G.eps = b->dtype == EL_F32 ? 1.19e-7 : 2.22e-16;
+    G.inst = b->d_inst; G.diag = b->d_diag; G.vpub = b->c_vpub; G.part = b->c_part;
+    G.tot = b->c_part + (size_t)2 * P.nctas * (MAXIT + 2);
+    G.bar = b->c_sync; G.err = (int *)(b->c_sync + 1); G.seed = seed;
+    G.e0 = b->d_out; G.e1 = b->d_out + b->count; G.res = b->d_out + 2 * b->count; G.gap = b->d_out + 3 * b->count;
+    G.iters = b->d_iout; G.conv = b->d_iout + b->count;
+    EL_CUDA_TRY(ctx, cudaMemsetAsync(b->c_sync, 0, 2 * sizeof(unsigned), ctx->stream));
+    void *kargs[] = {(void *)&G};
+    const void *fn = nullptr;
+#define EL_CPICK(TT)                                                                   \
+    switch (P.nt) {                                                                    \
+      case 32: fn = (const void *)k_lanczos_coop<TT, 32>; break;                       \
+      case 64: fn = (const void *)k_lanczos_coop<TT, 64>; break;                       \
+      case 128: fn = (const void *)k_lanczos_coop<TT, 128>; break;                     \
+      case 256: fn = (const void *)k_lanczos_coop<TT, 256>; break;                     \
+      case 512: fn = (const void *)k_lanczos_coop<TT, 512>; break;                     \
+      default: fn = (const void *)k_lanczos_coop<TT, 1024>; break;                     \
+    }
+    if (b->dtype == EL_F32) { EL_CPICK(float) } else { EL_CPICK(double) }
+#undef EL_CPICK
+    EL_CUDA_TRY(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem));
+    int per_sm = 0;
+    EL_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, P.nt, P.smem));
+    if (per_sm * sms < P.nctas) return fail(ctx, EL_EINVAL, "cooperative grid of %d CTAs is not co-resident", P.nctas);
+    EL_CUDA_TRY(ctx, cudaLaunchCooperativeKernel(fn, dim3(P.nctas), dim3(P.nt), kargs, P.smem, ctx->stream));
+    ctx->launches++;
+  }
+  // a barrier that timed out leaves the flag set
+  unsigned hs[2] = {0, 0};
+  EL_CUDA_TRY(ctx, el::copy(ctx, hs, b->c_sync, sizeof hs, cudaMemcpyDeviceToHost));
+  EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (hs[1]) return fail(ctx, EL_ECUDA, "cooperative Lanczos: a grid barrier timed out");
+  return EL_OK;
+}
+
 int el_batch_results(el_ctx *ctx, el_batch *b, double *e0, double *gap, double *residual,
                      int32_t *iters, int32_t *converged) {
   if (!ctx || !b || !e0 || !gap) return EL_EINVAL;
@@ -667,6 +1037,9 @@ int el_batch_destroy(el_batch *b) {
   if (b->d_iout) cudaFree(b->d_iout);
   if (b->d_queue) cudaFree(b->d_queue);
   if (b->ws) cudaFree(b->ws);
+  if (b->c_vpub) cudaFree(b->c_vpub);
+  if (b->c_part) cudaFree(b->c_part);
+  if (b->c_sync) cudaFree(b->c_sync);
   delete b;
   return EL_OK;
 }

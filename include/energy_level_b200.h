@@ -234,6 +234,18 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
  * 1 or 2.  Asynchronous and capturable in a CUDA graph once a first run has
  * sized the workspace. */
 int el_batch_run(el_ctx *ctx, el_batch *batch, int threads, int ctas_per_sm, uint64_t seed);
+/* Solve the batch's instances one after another, each with the whole GPU:
+ * one cooperative launch per instance splits its rows over up to 64 CTAs
+ * (one row per thread) that keep their slices of the Krylov basis in shared
+ * memory and reorthogonalise fully every step (classical Gram-Schmidt,
+ * reorth_passes = 1 or 2 times), meeting at grid barriers (bounded waits: a timeout returns
+ * EL_ECUDA).  For instances too small to fill the GPU with vectors but slow
+ * on one SM (a full 2^12 basis: a few thousand rows); EL_EINVAL when an
+ * instance's slice does not fit shared memory.  The Ritz values and their
+ * residual estimates are evaluated every check_every steps (and at the
+ * last).  Same results layout as el_batch_run (read with el_batch_results). */
+int el_batch_run_coop(el_ctx *ctx, el_batch *batch, int reorth_passes, int check_every,
+                      uint64_t seed);
 /* Copy results (caller order): ground energy, gap E1 - E0, max residual
  * estimate, Lanczos steps, converged flag.  Synchronises the stream. */
 int el_batch_results(el_ctx *ctx, el_batch *batch, double *e0, double *gap, double *residual,

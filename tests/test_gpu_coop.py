@@ -1,0 +1,86 @@
+"""GPU parity of the cooperative single-instance Lanczos (el_batch_run_coop):
+every instance solved by one cooperative launch over up to 64 CTAs, against
+dense eigenvalues from the oracle and the reference's C1 ground energy."""
+import numpy as np
+import pytest
+
+from oracle import ref
+from energy_level_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+C1_E0 = -10.2963231346414      # 12-site chain, full basis (the reference's ground_state)
+
+
+def _dense(n, edges, om, de, calib):
+    codes = None if edges is None else ref.independent_states(n, edges, None)
+    pairs = [(p["i"], p["j"], p["V"]) for p in calib["pairs"]]
+    w = np.linalg.eigvalsh(ref.dense_h(n, codes, om, de, pairs))
+    return w[0], w[1] - w[0]
+
+
+@pytest.mark.parametrize("dtype,tol_e", [("float64", 1e-9), ("float32", 2e-6)])
+def test_coop_c1_matches_reference(ctx, dtype, tol_e):
+    from energy_level_b200.batched import BatchedGroundStates
+    cfg = configs.chain12()
+    inst = [dict(calib=cfg["calib"], Om=cfg["Om"], delta=cfg["delta"], edges=None)]
+    b = BatchedGroundStates(inst, dtype=dtype, max_iter=300, tol=1e-10 if dtype == "float64" else 1e-5)
+    b.run_coop()
+    r = b.results()
+    e0, gap = _dense(12, None, cfg["Om"], cfg["delta"], cfg["calib"])
+    assert abs(e0 - C1_E0) < 1e-9
+    assert r["converged"][0]
+    assert abs(r["E0"][0] - e0) < tol_e * max(1.0, abs(e0))
+    assert abs(r["gap"][0] - gap) < (1e-7 if dtype == "float64" else 1e-4)
+    # a second run gives the same bits (fixed-order reductions)
+    b.run_coop()
+    assert b.results()["E0"][0] == r["E0"][0]
+    b.close()
+
+
+def test_coop_several_instances_match_dense(ctx):
+    from energy_level_b200.batched import BatchedGroundStates
+    rng = np.random.default_rng(6)
+    insts, want = [], []
+    for k, (n, kind) in enumerate([(14, "chain"), (13, "ring"), (10, "full"), (16, "chain"), (9, "ring")]):
+        edges = None if kind == "full" else (configs.ring_edges(n) if kind == "ring" else configs.chain_edges(n))
+        calib = configs.calib_from_positions(configs.chain_positions(n, jitter=rng.uniform(-0.3, 0.3, n)))
+        om, de = np.full(n, 2.0), np.full(n, -2.0 * rng.uniform(0, 3))
+        insts.append(dict(calib=calib, Om=om, delta=de, edges=edges))
+        want.append(_dense(n, edges, om, de, calib))
+    want = np.array(want)
+    b = BatchedGroundStates(insts, dtype="float64", max_iter=300, tol=1e-10)
+    b.run_coop()
+    r = b.results()
+    assert r["converged"].all()
+    assert np.max(np.abs(r["E0"] - want[:, 0])) < 1e-8
+    assert np.max(np.abs(r["gap"] - want[:, 1])) < 1e-7
+    # the single-CTA persistent kernel agrees
+    b.run()
+    r2 = b.results()
+    assert np.max(np.abs(r2["E0"] - r["E0"])) < 1e-8
+    b.close()
+
+
+def test_coop_refuses_too_large_instance(ctx):
+    from energy_level_b200.batched import BatchedGroundStates
+    n = 28                          # chain sector of 832,040 rows: more than 64 x 1024
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+    b = BatchedGroundStates([dict(calib=calib, Om=np.full(n, 2.0), delta=np.zeros(n),
+                                  edges=configs.chain_edges(n))], dtype="float32", max_iter=50)
+    with pytest.raises(ValueError):
+        b.run_coop()
+    b.close()
+
+
+def test_coop_check_interval_and_passes_agree(ctx):
+    """The same C1 ground energy for other check intervals and one pass."""
+    from energy_level_b200.batched import BatchedGroundStates
+    cfg = configs.chain12()
+    inst = [dict(calib=cfg["calib"], Om=cfg["Om"], delta=cfg["delta"], edges=None)]
+    b = BatchedGroundStates(inst, dtype="float64", max_iter=300, tol=1e-10)
+    for ce, ps in ((8, 2), (16, 2), (8, 1)):
+        b.run_coop(check_every=ce, reorth_passes=ps)
+        r = b.results()
+        assert r["converged"][0] and abs(r["E0"][0] - C1_E0) < 1e-9, (ce, ps)
+    b.close()
