@@ -228,7 +228,8 @@ __global__ void __launch_bounds__(NT) k_lanczos_batch(const BatchArgs A) {
   __shared__ double work[8 * MAXIT + 8];   // [0, MAXIT): omega row; [2 MAXIT, 8 MAXIT): projection coefficients, then inverse iteration
   __shared__ int s_idx, s_flag, s_done, s_force, s_trig, nsel;
   __shared__ short sel[MAXIT + 2];         // vectors of the current reorthogonalisation
-  __shared__ double s_th[2], s_res[2];
+  __shared__ double s_th[2], s_res[2], s_pth[2], s_pdth[2];
+  __shared__ int s_have, s_next;
   const int tid = threadIdx.x;
   if (tid == 0) {
     fib[0] = 0; fib[1] = 1;
@@ -263,7 +264,10 @@ __global__ void __launch_bounds__(NT) k_lanczos_batch(const BatchArgs A) {
       const T sc = (T)(1.0 / sqrt(nrm));
       for (int64_t r = tid; r < dim; r += NT) Vb[r] *= sc;
     }
-    if (tid == 0) { wcur[0] = 1.0; s_force = 0; s_done = 0; s_th[0] = s_th[1] = 0.0; s_res[0] = s_res[1] = 1e300; }
+    if (tid == 0) {
+      wcur[0] = 1.0; s_force = 0; s_done = 0; s_th[0] = s_th[1] = 0.0; s_res[0] = s_res[1] = 1e300;
+      s_have = 0; s_next = 8;
+    }
     __syncthreads();
     double beta = 0.0, anorm = 0.0;
     int j = 0, steps = 0;
@@ -405,29 +409,47 @@ __global__ void __launch_bounds__(NT) k_lanczos_batch(const BatchArgs A) {
       __syncthreads();   // al/be/omega rows visible to warp 0 and everyone
       steps = j + 1;
       const bool invariant = !(bnext > 1e-12 * fmax(1.0, anorm));
-      const bool check = invariant || (j + 1 == m) || ((steps >= 2) && (steps % 8 == 0));
+      // Ritz check every 8 steps (every 32 while the residuals are far from
+      // tolerance); the multisection starts from the previous Ritz values,
+      // upper bounds by Cauchy interlacing, with a Sturm-confirmed narrow
+      // lower bound when one holds
+      const bool check = invariant || (j + 1 == m) || ((steps >= 2) && (steps >= s_next));
       if (check && tid < 32) {
         const int mm = steps;
-        double lo = 1e300, hi = -1e300;
+        double glo = 1e300, ghi = -1e300;
         for (int i = 0; i < mm; ++i) {
           const double rr = (i > 0 ? fabs(be[i - 1]) : 0.0) + (i + 1 < mm ? fabs(be[i]) : 0.0);
-          lo = fmin(lo, al[i] - rr);
-          hi = fmax(hi, al[i] + rr);
+          glo = fmin(glo, al[i] - rr);
+          ghi = fmax(ghi, al[i] + rr);
         }
-        lo -= 1e-9 * fmax(1.0, fabs(lo));
-        hi += 1e-9 * fmax(1.0, fabs(hi));
+        const double scale = fmax(1.0, fmax(fabs(glo), fabs(ghi)));
+        glo -= 1e-9 * scale;
+        ghi += 1e-9 * scale;
         const int ne = mm >= 2 ? 2 : 1;
+        double worst = 0.0;
         for (int q = 0; q < ne; ++q) {
+          double lo = glo, hi = ghi;
+          if (s_have) {
+            hi = fmin(ghi, s_pth[q] + 1e-12 * scale);
+            const double cand = hi - fmax(16.0 * s_pdth[q], 1e-10 * scale);
+            if (cand > glo && sturm(al, be, mm, cand) <= q) lo = cand;
+          }
           const double th = warp_eig(al, be, mm, q, lo, hi);
           if (tid == 0) {
+            s_pdth[q] = s_have ? fmax(s_pth[q] - th, 0.0) : fabs(ghi - glo);
+            s_pth[q] = th;
             s_th[q] = th;
             s_res[q] = bnext * last_component(al, be, mm, th, work + 2 * MAXIT);
+            worst = fmax(worst, s_res[q] / (A.tol * fmax(1.0, fabs(th))));
           }
+          __syncwarp();
         }
         if (tid == 0) {
           bool ok = (ne == 2);
           for (int q = 0; q < ne; ++q) ok = ok && (s_res[q] <= A.tol * fmax(1.0, fabs(s_th[q])));
           s_done = (ok || invariant || j + 1 == m) ? 1 : 0;
+          s_have = (ne == 2) ? 1 : 0;
+          s_next = mm + (worst > 1e3 ? 32 : 8);
         }
       }
       __syncthreads();
