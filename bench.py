@@ -719,6 +719,30 @@ def native_ramp31(h, args):
             solvers.spin_observables(ham32, psi32, prs)
         obs_ms[tag] = (time.perf_counter() - t0) / 5 * 1e3
         torch.cuda.nvtx.range_pop()
+    # loss rates (non-Hermitian, gamma = 1 per site): the first 30 segments
+    # by the scaled Taylor propagator, against the Hermitian Chebyshev step
+    segs30 = cfg["segments"][:30]
+    psi_l = torch.zeros(basis.dim, dtype=torch.complex64, device="cuda")
+    cnt = {}
+
+    def run_segments(step, key):
+        psi_l.zero_()
+        psi_l[0] = 1.0
+        tt = 0
+        for s_ in segs30:
+            ham32.set_drive(s_["Om"], s_["delta"])
+            tt += step(ham32, psi_l, 3000.0 / 300, tol=1e-7)
+        cnt[key] = tt
+    ham32.set_loss(np.full(31, 1.0))
+    run_segments(solvers.taylor_step, "taylor")
+    el_t, _, _ = h.timed(lambda: run_segments(solvers.taylor_step, "taylor"), 1)
+    norm_loss = float(psi_l.abs().pow(2).sum())
+    ham32.set_loss(None)
+    el_c, _, _ = h.timed(lambda: run_segments(solvers.cheb_step, "cheb"), 1)
+    loss_line = {"segments": 30, "gamma_per_site": 1.0, "dtype": "c64", "tol": 1e-7,
+                 "taylor_ms_per_segment": el_t / 30 * 1e3, "taylor_terms_per_segment": cnt["taylor"] / 30,
+                 "chebyshev_ms_per_segment": el_c / 30 * 1e3, "chebyshev_terms_per_segment": cnt["cheb"] / 30,
+                 "norm_after_30_segments": norm_loss}
     cpu = None
     if h.rank == 0 and h.world == 1 and not args.no_cpu:
         cpu = cpu_ramp_sample(basis.dim)
@@ -735,6 +759,7 @@ def native_ramp31(h, args):
         "plain_fp64": {"solves_per_s": psteps / el64, "form": "complex128, tol 1e-13"},
         "chosen_vs_plain": (steps / el) / (psteps / el64),
         "observables_ms": obs_ms,
+        "loss_propagation": loss_line,
         "error_vs_fp64": {"infidelity": 1.0 - fid, "norm_deviation": abs(norm32 - 1.0),
                           "max_abs_n_i": float(np.max(np.abs(n32 - n64))),
                           "max_abs_n_i_normalised": float(np.max(np.abs(n32 / norm32 ** 2 - n64 / norm64 ** 2))),

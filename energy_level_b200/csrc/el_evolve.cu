@@ -138,13 +138,16 @@ extern "C" int el_cheb_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
 // ------------------------------------------------------------------- Taylor
 // Non-Hermitian H (loss diagonal -i gamma/2): psi <- exp(A) psi with
 // A = -i CONV tau H, the operation of expm_multiply in engine_ed.py:125,145
-// for gamma != 0.  With the bound ||H|| <= max_r (|d_r| + sum_offdiag |H_rs|)
-// (row and column sums agree: the off-diagonal part is Hermitian), exp(A) is
-// applied as s substeps exp(A/s) with ||A/s|| <= theta, each a Taylor
-// polynomial of degree m, the smallest m whose remainder bound
-// sum_{j>m} theta_s^j / j! is below tol / s (theta_s = ||A|| / s).  With
-// u_0 = psi, u_j = (CONV tau / (s j)) H u_{j-1}, the terms are (-i)^j u_j:
-// one fused launch per term (real scale on H x, complex weight on acc).
+// for gamma != 0.  H is shifted by the centre c of its real Gershgorin
+// interval [lo, hi] (a global phase exp(-i CONV tau c) put back in the term
+// weights); then ||H - c|| <= (hi - lo)/2 + sum_k |loss_k| bounds the
+// 1- and 2-norm (row and column sums agree: the off-diagonal part is
+// Hermitian).  exp(A) is applied as s substeps exp(A/s) with
+// ||A/s|| <= theta, each a Taylor polynomial of degree m, the smallest m
+// whose remainder bound sum_{j>m} theta_s^j / j! is below tol / s.  With
+// u_0 = psi, u_j = (CONV tau / (s j)) (H - c) u_{j-1}, the terms are
+// e^{-i phi} (-i)^j u_j (phi = CONV tau c / s): one fused launch per term
+// (real scale and shift on H x, complex weight on acc).
 extern "C" int el_taylor_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
                               double tau_ns, double tol, int *n_terms) {
   if (!ctx || !h || !psi) return EL_EINVAL;
@@ -160,7 +163,11 @@ extern "C" int el_taylor_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
   double lo, hi, nrm;
   int rc = el::gershgorin(ctx, h, &lo, &hi, &nrm);
   if (rc) return rc;
-  const double x = CONV * tau_ns * nrm;
+  const double c = 0.5 * (lo + hi);
+  double lsum = 0.0;
+  for (int k = 0; k < h->n; ++k) lsum += std::fabs(h->loss[k]);
+  const double bound = std::min(nrm + std::fabs(c), 0.5 * (hi - lo) + lsum);
+  const double x = CONV * tau_ns * bound;
   const double theta = (dtype == EL_C128) ? 2.0 : 1.0;
   const int s = std::max(1, (int)std::ceil(x / theta));
   const double ths = x / s;
@@ -178,9 +185,11 @@ extern "C" int el_taylor_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
   if (!buf) return EL_ENOMEM;
   void *ta = buf, *tb = buf + vb, *acc = buf + 2 * vb;
   const double scale = CONV * tau_ns / s;
+  const double cph = std::cos(scale * c), sph = -std::sin(scale * c);   // e^{-i phi}
   for (int step = 0; step < s; ++step) {
     if (el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
-    EL_CUDA_TRY(ctx, el::copy(ctx, acc, psi, vb, cudaMemcpyDeviceToDevice));
+    rc = el::launch_axpby(ctx, dtype, dim, cph, sph, psi, 0, 0, acc, nullptr);   // acc = e^{-i phi} psi
+    if (rc) return rc;
     const void *xc = psi;
     void *y = ta;
     for (int j = 1; j <= m; ++j) {
@@ -188,12 +197,16 @@ extern "C" int el_taylor_step(el_ctx *ctx, el_ham *h, int dtype, void *psi,
       memset(&A, 0, sizeof A);
       A.dtype = dtype; A.nvec = 1; A.x = xc; A.y = (j < m) ? y : nullptr; A.acc = acc;
       A.a = scale / j;
+      A.b = -scale * c / j;
+      double wr = 0, wi = 0;
       switch (j & 3) {  // (-i)^j
-        case 0: A.w_re = 1; break;
-        case 1: A.w_im = -1; break;
-        case 2: A.w_re = -1; break;
-        default: A.w_im = 1; break;
+        case 0: wr = 1; break;
+        case 1: wi = -1; break;
+        case 2: wr = -1; break;
+        default: wi = 1; break;
       }
+      A.w_re = wr * cph - wi * sph;   // (-i)^j e^{-i phi}
+      A.w_im = wr * sph + wi * cph;
       rc = el::launch_apply(ctx, h, A);
       if (rc) return rc;
       xc = y;

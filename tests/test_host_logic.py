@@ -129,3 +129,43 @@ def test_kpm_thermal_from_exact_moments_matches_spectrum():
         p = np.exp(-b * (w - w.min()))
         E = float(p @ w / p.sum())
         assert abs(th["E"][i] - E) < 1e-5
+
+
+def test_exchange_parsing_and_number_conservation():
+    xy = configs.xy_chain(6)
+    ex = []
+    n, om, de, pairs = model.model_arrays(xy["calib"], xy["Om"], xy["delta"], terms=["I1", "I2"], exchange=ex)
+    assert n == 6 and len(pairs) == 15 and len(ex) == 15
+    assert all(e[3] == 0 for e in ex) and all(e[2] != 0 for e in ex)
+    # without an exchange list a nonzero J is refused, never dropped
+    with pytest.raises(model.ConfigConflict):
+        model.model_arrays(xy["calib"], xy["Om"], xy["delta"], terms=["I1", "I2"])
+    # I2 not among the terms: J is ignored as in channels.py
+    ex2 = []
+    model.model_arrays(xy["calib"], xy["Om"], xy["delta"], terms=["I1"], exchange=ex2)
+    assert ex2 == []
+    model.check_number_conserving(xy["calib"], np.zeros(6), ["I1", "I2"])
+    with pytest.raises(ValueError):
+        model.check_number_conserving(xy["calib"], np.full(6, 0.1), ["I1", "I2"])
+    cal = dict(xy["calib"], pairs=[dict(p, A=0.2) for p in xy["calib"]["pairs"]])
+    with pytest.raises(ValueError):
+        model.check_number_conserving(cal, np.zeros(6), ["I1", "I2", "I3"])
+    # loss rates: refused unless the caller propagates in time
+    with pytest.raises(model.ConfigConflict):
+        model.model_arrays(xy["calib"], xy["Om"], xy["delta"], gamma=np.full(6, 0.1), terms=["I1"])
+    model.model_arrays(xy["calib"], xy["Om"], xy["delta"], gamma=np.full(6, 0.1), terms=["I1"], allow_loss=True)
+
+
+def test_sector_scan_refuses_before_touching_the_device():
+    from energy_level_b200.sector_scan import SectorScan, scan_ground_sectors
+    xy = configs.xy_chain(6)
+    with pytest.raises(ValueError):
+        SectorScan(xy["calib"], xy["delta"], np.full(6, 0.1), terms=["I1", "I2"])
+    with pytest.raises(ValueError):
+        SectorScan(xy["calib"], xy["delta"], np.zeros(6), terms=["I1", "I2"], sectors=[0, 7])
+    with pytest.raises(ValueError):
+        SectorScan(xy["calib"], xy["delta"], np.zeros(6), gamma=np.full(6, 0.1))
+    with pytest.raises(ValueError):
+        scan_ground_sectors(xy["calib"], xy["delta"], np.zeros(6), terms=["I1", "I2"], backend="dmrg")
+    with pytest.raises(ValueError):
+        SectorScan({"atoms": [], "pairs": []})
