@@ -637,10 +637,15 @@ struct TileFlip {
   int32_t k;     // bit
 };
 
-template <typename S, bool C, int NV>
+// RA: the amplitudes are real (real Omega) although the vectors are
+// complex: two FMAs per complex entry instead of four.
+template <typename S, bool C, int NV, bool RA = false>
 __device__ __forceinline__ void acc_flip(S (&h)[NV * (C ? 2 : 1)], S are, S aim,
                                          const S (&xv)[NV * (C ? 2 : 1)]) {
-  if constexpr (C) {
+  if constexpr (C && RA) {
+#pragma unroll
+    for (int v = 0; v < 2 * NV; ++v) h[v] += are * xv[v];
+  } else if constexpr (C) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       h[2 * v] += are * xv[2 * v] - aim * xv[2 * v + 1];
@@ -652,7 +657,7 @@ __device__ __forceinline__ void acc_flip(S (&h)[NV * (C ? 2 : 1)], S are, S aim,
   }
 }
 
-template <typename S, bool C, int NV, bool WANT>
+template <typename S, bool C, int NV, bool WANT, bool RA>
 __global__ void __launch_bounds__(256) k_apply_chain_tile(BasisDev B, HamArgs<S> H, KArgs K, int L,
                                                           int64_t ntiles) {
   constexpr int W = NV * (C ? 2 : 1);
@@ -794,7 +799,7 @@ __global__ void __launch_bounds__(256) k_apply_chain_tile(BasisDev B, HamArgs<S>
           const S aim = set ? s_aim[k] : -s_aim[k];
           S xv[W];
           tile_ld<S, W>(xt, TS, pi, xv);
-          acc_flip<S, C, NV>(h, are, aim, xv);
+          acc_flip<S, C, NV, RA>(h, are, aim, xv);
         }
       }
       // high flips: contiguous partner rows in global memory, two in flight
@@ -804,8 +809,8 @@ __global__ void __launch_bounds__(256) k_apply_chain_tile(BasisDev B, HamArgs<S>
         const bool ob = (f + 1 < nh) && (i < hf[f + 1].len);
         if (oa) ld_row<S, W>(xp + (size_t)(base + i + hf[f].off) * W, xa);
         if (ob) ld_row<S, W>(xp + (size_t)(base + i + hf[f + 1].off) * W, xb);
-        if (oa) acc_flip<S, C, NV>(h, hf_re[f], hf_im[f], xa);
-        if (ob) acc_flip<S, C, NV>(h, hf_re[f + 1], hf_im[f + 1], xb);
+        if (oa) acc_flip<S, C, NV, RA>(h, hf_re[f], hf_im[f], xa);
+        if (ob) acc_flip<S, C, NV, RA>(h, hf_re[f + 1], hf_im[f + 1], xb);
       }
       const int64_t row = base + i;
       S xr[W];
@@ -1274,31 +1279,42 @@ int chain_tile_bits(int n, int row_bytes, int scalar_bytes) {
   return best;
 }
 
-template <typename S, bool C, int NV, bool WANT>
+template <typename S, bool C, int NV, bool WANT, bool RA>
 int launch_chain_tile_t(el_ctx *ctx, int L, int64_t ntiles, const BasisDev &B, const HamArgs<S> &H,
                         const KArgs &K) {
   constexpr int W = NV * (C ? 2 : 1);
   const size_t ts = (size_t)B.fib[L + 2];
   const size_t smem = ts * W * sizeof(S) + ts * 4 + ts * sizeof(S) + 16;
-  cudaFuncSetAttribute(k_apply_chain_tile<S, C, NV, WANT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_apply_chain_tile<S, C, NV, WANT, RA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smem);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sms * 8);
-  k_apply_chain_tile<S, C, NV, WANT><<<grid, 256, smem, ctx->stream>>>(B, H, K, L, ntiles);
+  k_apply_chain_tile<S, C, NV, WANT, RA><<<grid, 256, smem, ctx->stream>>>(B, H, K, L, ntiles);
   return EL_OK;
 }
 
+template <typename S, bool C, bool RA>
+int launch_chain_tile_r(el_ctx *ctx, int nvec, bool want, int L, int64_t ntiles, const BasisDev &B,
+                        const HamArgs<S> &H, const KArgs &K) {
+  if (want) return launch_chain_tile_t<S, C, 1, true, RA>(ctx, L, ntiles, B, H, K);
+  switch (nvec) {
+    case 1: return launch_chain_tile_t<S, C, 1, false, RA>(ctx, L, ntiles, B, H, K);
+    case 2: return launch_chain_tile_t<S, C, 2, false, RA>(ctx, L, ntiles, B, H, K);
+    case 4: return launch_chain_tile_t<S, C, 4, false, RA>(ctx, L, ntiles, B, H, K);
+    default: return launch_chain_tile_t<S, C, 8, false, RA>(ctx, L, ntiles, B, H, K);
+  }
+}
+
+// complex vectors with a real drive take the real-amplitude variant, except
+// for eight complex64 vectors per row, where it needs 119 registers instead
+// of 80 and loses the third CTA per SM
 template <typename S, bool C>
 int launch_chain_tile_v(el_ctx *ctx, int nvec, bool want, int L, int64_t ntiles, const BasisDev &B,
-                        const HamArgs<S> &H, const KArgs &K) {
-  if (want) return launch_chain_tile_t<S, C, 1, true>(ctx, L, ntiles, B, H, K);
-  switch (nvec) {
-    case 1: return launch_chain_tile_t<S, C, 1, false>(ctx, L, ntiles, B, H, K);
-    case 2: return launch_chain_tile_t<S, C, 2, false>(ctx, L, ntiles, B, H, K);
-    case 4: return launch_chain_tile_t<S, C, 4, false>(ctx, L, ntiles, B, H, K);
-    default: return launch_chain_tile_t<S, C, 8, false>(ctx, L, ntiles, B, H, K);
-  }
+                        const HamArgs<S> &H, const KArgs &K, bool real_amp) {
+  if (C && real_amp && (want || nvec <= 4 || sizeof(S) == 8))
+    return launch_chain_tile_r<S, C, true>(ctx, nvec, want, L, ntiles, B, H, K);
+  return launch_chain_tile_r<S, C, false>(ctx, nvec, want, L, ntiles, B, H, K);
 }
 
 int launch_apply_row(el_ctx *ctx, el_ham *h, const ApplyArgs &A, const BasisDev &B, KArgs K) {
@@ -1321,10 +1337,10 @@ int launch_apply_row(el_ctx *ctx, el_ham *h, const ApplyArgs &A, const BasisDev 
     if (L > 0) {
       const int64_t ntiles = (int64_t)B.fib[h->n - L + 2];
       switch (A.dtype) {
-        case EL_F32: launch_chain_tile_v<float, false>(ctx, A.nvec, want, L, ntiles, B, ham_args<float>(h, h->d_diagV32), K); break;
-        case EL_F64: launch_chain_tile_v<double, false>(ctx, A.nvec, want, L, ntiles, B, ham_args<double>(h, h->d_diagV64), K); break;
-        case EL_C64: launch_chain_tile_v<float, true>(ctx, A.nvec, want, L, ntiles, B, ham_args<float>(h, h->d_diagV32), K); break;
-        case EL_C128: launch_chain_tile_v<double, true>(ctx, A.nvec, want, L, ntiles, B, ham_args<double>(h, h->d_diagV64), K); break;
+        case EL_F32: launch_chain_tile_v<float, false>(ctx, A.nvec, want, L, ntiles, B, ham_args<float>(h, h->d_diagV32), K, false); break;
+        case EL_F64: launch_chain_tile_v<double, false>(ctx, A.nvec, want, L, ntiles, B, ham_args<double>(h, h->d_diagV64), K, false); break;
+        case EL_C64: launch_chain_tile_v<float, true>(ctx, A.nvec, want, L, ntiles, B, ham_args<float>(h, h->d_diagV32), K, !h->drive_complex); break;
+        case EL_C128: launch_chain_tile_v<double, true>(ctx, A.nvec, want, L, ntiles, B, ham_args<double>(h, h->d_diagV64), K, !h->drive_complex); break;
         default: return el::fail(ctx, EL_EINVAL, "unknown dtype %d", A.dtype);
       }
       EL_LAUNCH_CHECK(ctx);
