@@ -28,6 +28,7 @@ struct HamArgs {
   const ExPair *px;       // exchange channels (generic kernel only)
   int npx;
   int lossy;              // loss diagonal present (generic kernel only)
+  int real_amp;           // every sigma^x amplitude is real (row kernel: cheaper complex FMAs)
   S loss[EL_MAX_SITES];   // imaginary diagonal per set bit: -gamma/2 (evolution units)
 };
 
@@ -490,10 +491,15 @@ __global__ void __launch_bounds__(256) k_apply_row(BasisDev B, HamArgs<S> H, KAr
       for (int u = 0; u < U; ++u) {
         if (!ok[u]) continue;
         if constexpr (C) {
+          if (H.real_amp) {   // uniform: a real drive needs two FMAs per complex entry
 #pragma unroll
-          for (int v = 0; v < NV; ++v) {
-            h[2 * v] += ar[u] * xv[u][2 * v] - ai[u] * xv[u][2 * v + 1];
-            h[2 * v + 1] += ar[u] * xv[u][2 * v + 1] + ai[u] * xv[u][2 * v];
+            for (int v = 0; v < 2 * NV; ++v) h[v] += ar[u] * xv[u][v];
+          } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+              h[2 * v] += ar[u] * xv[u][2 * v] - ai[u] * xv[u][2 * v + 1];
+              h[2 * v + 1] += ar[u] * xv[u][2 * v + 1] + ai[u] * xv[u][2 * v];
+            }
           }
         } else {
 #pragma unroll
@@ -877,6 +883,7 @@ HamArgs<S> ham_args(const el_ham *h, const S *diagV) {
   A.px = h->d_px;
   A.npx = (int)h->px.size();
   A.lossy = h->lossy ? 1 : 0;
+  A.real_amp = h->drive_complex ? 0 : 1;
   for (int k = 0; k < h->n; ++k) {
     A.delta[k] = (S)h->delta[k];
     A.up_re[k] = (S)(0.5 * h->om_re[k]);
