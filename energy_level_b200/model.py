@@ -57,28 +57,50 @@ def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None, exchange=No
     if np.any(gamma != 0) and not allow_loss:
         raise ConfigConflict('b200 backends need a Hermitian H (gamma = 0)', keys=('manybody.gamma_mhz',))
     use = set(active_terms(calib) if terms is None else terms)
-    pairs = []
-    for p in (calib.get('pairs') or []):
-        i, j = int(p['i']), int(p['j'])
-        if not (0 <= i < n and 0 <= j < n) or i == j:
-            raise ValueError('pair (%d, %d) out of range' % (i, j))
-        amps = []
-        for key, term in (('J', 'I2'), ('A', 'I3')):
-            a = complex(p.get(key) or 0.0) if term in use else 0j
-            if not np.isfinite(a):
-                raise ValueError('pair (%d, %d): %s must be finite' % (i, j, key))
-            if a != 0 and exchange is None:
-                raise ConfigConflict('this b200 solver implements the Omega/delta/V model only '
-                                     '(%s channel %s != 0)' % (term, key), keys=('manybody.calib',))
-            amps.append(a)
-        if exchange is not None and (amps[0] != 0 or amps[1] != 0):
-            exchange.append((i, j, amps[0], amps[1]))
-        if 'I1' in use:
-            V = complex(p.get('V') or 0.0)
-            if V.imag != 0:
-                raise ValueError('V must be real')
-            if V.real != 0:
-                pairs.append((i, j, float(V.real)))
+    raw = calib.get('pairs') or []
+    m = len(raw)
+    if m == 0:
+        return n, Om, delta, []
+    # columns of the pair list; the checks below raise, for the first pair
+    # that fails any of them, the error that pair's own checks would raise
+    # first (range, J, A, V, in that order)
+    ii = np.fromiter((p['i'] for p in raw), dtype=np.int64, count=m)
+    jj = np.fromiter((p['j'] for p in raw), dtype=np.int64, count=m)
+    zero = np.zeros(m, complex)
+
+    def column(key):
+        try:       # real values (the common case) without building Python complex numbers
+            return np.fromiter((p.get(key) or 0.0 for p in raw), dtype=float, count=m).astype(complex)
+        except TypeError:
+            return np.array([p.get(key) or 0.0 for p in raw], dtype=complex)
+    V = column('V') if 'I1' in use else zero
+    J = column('J') if 'I2' in use else zero
+    A = column('A') if 'I3' in use else zero
+    checks = [
+        ((ii < 0) | (ii >= n) | (jj < 0) | (jj >= n) | (ii == jj),
+         lambda k: ValueError('pair (%d, %d) out of range' % (ii[k], jj[k]))),
+        (~np.isfinite(J), lambda k: ValueError('pair (%d, %d): J must be finite' % (ii[k], jj[k]))),
+        ((J != 0) if exchange is None else np.zeros(m, bool),
+         lambda k: ConfigConflict('this b200 solver implements the Omega/delta/V model only '
+                                  '(I2 channel J != 0)', keys=('manybody.calib',))),
+        (~np.isfinite(A), lambda k: ValueError('pair (%d, %d): A must be finite' % (ii[k], jj[k]))),
+        ((A != 0) if exchange is None else np.zeros(m, bool),
+         lambda k: ConfigConflict('this b200 solver implements the Omega/delta/V model only '
+                                  '(I3 channel A != 0)', keys=('manybody.calib',))),
+        (V.imag != 0, lambda k: ValueError('V must be real')),
+    ]
+    first = None
+    for order, (mask, err) in enumerate(checks):
+        if mask.any():
+            k = int(np.argmax(mask))
+            if first is None or (k, order) < first[:2]:
+                first = (k, order, err)
+    if first is not None:
+        raise first[2](first[0])
+    if exchange is not None:
+        for k in np.flatnonzero((J != 0) | (A != 0)):
+            exchange.append((int(ii[k]), int(jj[k]), complex(J[k]), complex(A[k])))
+    pairs = [(int(ii[k]), int(jj[k]), float(V[k].real)) for k in np.flatnonzero(V.real != 0)]
     return n, Om, delta, pairs
 
 
