@@ -1821,12 +1821,12 @@ int el_hv_host(el_ctx *ctx, el_ham *h, int dtype, int nvec, const void *x_host, 
   if (!es) return el::fail(ctx, EL_EINVAL, "unknown dtype %d", dtype);
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   const size_t bytes = (size_t)h->basis->dim * nvec * es;
-  void *dx = nullptr, *dy = nullptr;
-  EL_CUDA_TRY(ctx, cudaMalloc(&dx, bytes));
-  cudaError_t e = cudaMalloc(&dy, bytes);
+  // device copies in the context's cached workspace (kept between calls)
+  char *buf = (char *)el::workspace(ctx, 14, 2 * bytes);
+  if (!buf) return EL_ENOMEM;
+  void *dx = buf, *dy = buf + bytes;
+  cudaError_t e = el::copy(ctx, dx, x_host, bytes, cudaMemcpyHostToDevice);
   int rc = EL_OK;
-  if (e != cudaSuccess) { cudaFree(dx); return el::cuda_fail(ctx, e, "cudaMalloc"); }
-  e = el::copy(ctx, dx, x_host, bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     rc = el_hv(ctx, h, dtype, nvec, dx, dy);
     if (rc == EL_OK) {
@@ -1834,8 +1834,6 @@ int el_hv_host(el_ctx *ctx, el_ham *h, int dtype, int nvec, const void *x_host, 
       if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     }
   }
-  cudaFree(dx);
-  cudaFree(dy);
   if (rc) return rc;
   if (e != cudaSuccess) return el::cuda_fail(ctx, e, "el_hv_host");
   return EL_OK;

@@ -99,9 +99,17 @@ def state_vector(spec, n, codes=None):
         vecs = product_vectors(spec, n)
         if vecs is None:
             raise ValueError('ground 初态必须由求解器从当前 Hamiltonian 准备')
-        vec = np.ones(len(basis), complex)
-        for i, loc in enumerate(vecs):
-            vec *= loc[(basis >> (n - 1 - i)) & 1]
+        if all(np.count_nonzero(loc) == 1 for loc in vecs):
+            # every site in |g> or |r> (up to a phase): one basis code
+            bits = [int(np.flatnonzero(loc)[0]) for loc in vecs]
+            c0 = sum(b << (n - 1 - i) for i, b in enumerate(bits))
+            amp = complex(np.prod([loc[b] for loc, b in zip(vecs, bits)]))
+            vec = np.zeros(len(basis), complex)
+            vec[np.flatnonzero(basis == c0)] = amp
+        else:
+            vec = np.ones(len(basis), complex)
+            for i, loc in enumerate(vecs):
+                vec *= loc[(basis >> (n - 1 - i)) & 1]
     nrm = float(np.linalg.norm(vec))
     if not np.isfinite(nrm) or nrm <= 0:
         raise ValueError('多体初态零范数或不在受限子空间')
