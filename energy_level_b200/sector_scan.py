@@ -67,6 +67,9 @@ class SectorScan:
             if not 0 <= k <= n:
                 raise ValueError('sector 必须在 [0, N]')
         self.n, self.ks = n, ks
+        # the calib is parsed once; every sector gets its basis and H from it
+        exchange = []
+        _, om_arr, de_arr, vpairs = model.model_arrays(calib, Om, delta, gamma, terms, exchange=exchange)
         self.dev = _device_index(device)
         self.nw = max(1, min(int(workers), len(ks)))
         t_w = time.perf_counter()
@@ -93,8 +96,8 @@ class SectorScan:
                     if self.owner[k] != w:
                         continue
                     t0 = time.perf_counter()
-                    _, basis, ham, _ = model.build(calib, Om, delta, gamma, terms,
-                                                   constraint={'kind': 'charge', 'k': k}, ctx=self.ctxs[w])
+                    basis = model.Basis(self.ctxs[w], n, kind='charge', k=k)
+                    ham = model.Hamiltonian(self.ctxs[w], basis, om_arr, de_arr, vpairs, exchange=exchange)
                     if memory_budget_mb is not None and basis.dim * itemsize * (min(m, basis.dim) + 5) > \
                             float(memory_budget_mb) * 1024 ** 2:
                         raise MemoryError('GPU Krylov/transition 保守内存估算超过 memory_budget_mb')
