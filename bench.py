@@ -354,9 +354,9 @@ def run_native(args):
 # ------------------------------------------------- further workloads (C1, C3-C5, H.v)
 
 WORKLOADS = ("kpm_dos_square25", "hv_chain31", "lanczos_chain12", "ramp_chain31", "batch512",
-             "adjoint_ring20", "scan_xy20")
+             "adjoint_ring20", "scan_xy20", "spectrum_chain26")
 DEFAULT_STEPS = {"kpm_dos_square25": 5, "hv_chain31": 200, "lanczos_chain12": 50, "ramp_chain31": 3,
-                 "batch512": 10, "adjoint_ring20": 5, "scan_xy20": 3}
+                 "batch512": 10, "adjoint_ring20": 5, "scan_xy20": 3, "spectrum_chain26": 3}
 
 
 class Harness:
@@ -991,6 +991,92 @@ def cpu_adjoint_sample(cfg):
                       "per FD gradient" % (K, len(tau))}
 
 
+# --- f1: source-state spectrum, 26-site chain sector
+
+SPEC_N, SPEC_K = 26, 200
+
+
+def native_spectrum26(h, args):
+    """Source-state Lanczos spectrum (k = 200, full reorthogonalisation twice,
+    complex128) on the 26-site chain blockade sector (dim F(28) = 317,811)
+    from a seeded random source state."""
+    torch = h.torch
+    from energy_level_b200 import configs, spectrum
+    from energy_level_b200.core import Basis, Hamiltonian
+    n = SPEC_N
+    calib, pairs, om, de = chain_model(n, Om=2.0, Delta=1.0)
+    basis = Basis(h.ctx, n, "blockade", edges=configs.chain_edges(n))
+    ham = Hamiltonian(h.ctx, basis, om, de, pairs)
+    dim = basis.dim
+    rng = np.random.default_rng(11 + h.rank)
+    phi_h = rng.normal(size=dim) + 1j * rng.normal(size=dim)
+    phi_h /= np.linalg.norm(phi_h)
+    phi = torch.as_tensor(phi_h, dtype=torch.complex128, device="cuda")
+
+    def run(p):
+        return spectrum.source_spectrum(ham, p, n_krylov=SPEC_K, eta=0.1, memory_budget_mb=None,
+                                        dtype="complex128")
+    for _ in range(args.warmup):
+        run(phi)
+    steps = args.steps
+    el, launches, clocks = h.timed(lambda: run(phi), steps)
+    r = run(phi)
+    # end to end: the source state from the host each time
+    b0 = h.ctx.copied_bytes
+    te = time.perf_counter()
+    reps = max(1, min(steps, 3))
+    for _ in range(reps):
+        r2 = run(phi_h)
+    e2e_s = (time.perf_counter() - te) / reps
+    b1 = h.ctx.copied_bytes
+    k = int(r["krylov"]["n"])
+    # compulsory traffic: per step H.v (x, y, d) plus two Gram-Schmidt passes
+    # that read the stored basis twice (projections, then the update)
+    alg = sum(dim * (16 * 2 + 8) + 2 * 2 * (j + 1) * dim * 16 for j in range(k))
+    cpu = None
+    if h.rank == 0 and h.world == 1 and not args.no_cpu:
+        cpu = cpu_spectrum_sample()
+    line = base_line(args, h.world, "spectrum_chain26", h.world * steps / el, "spectra/s", steps, el, "c128",
+                     {"n_sites": n, "basis": "chain nearest-neighbour blockade sector", "dim": dim,
+                      "krylov": SPEC_K, "reorthogonalisation": "full, twice per step",
+                      "source": "seeded random complex state", "Om": 2.0, "Delta": 1.0,
+                      "l2": "Krylov basis 1.0 GB, larger than L2"})
+    line.update({
+        "roofline": roofline(alg, el / steps, kernel="whole spectrum (H.v + Gram-Schmidt gemv kernels), "
+                             "algorithmic bytes of the k steps / time per spectrum"),
+        # the host source state is copied in by the call (torch), the alphas/betas out by the library
+        "e2e": {"value": h.world / e2e_s, "unit": "spectra/s",
+                "h2d_bytes_per_step": phi_h.nbytes + (b1[0] - b0[0]) // reps,
+                "d2h_bytes_per_step": (b1[1] - b0[1]) // reps},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+        "check": {"krylov_n": k, "ortho_loss": r["krylov"]["ortho_loss"],
+                  "integral_ratio": r["error_report"]["integral_ratio"],
+                  "e2e_same_alphas": bool(np.array_equal(r["evals"], r2["evals"]))},
+    })
+    return line
+
+
+def cpu_spectrum_sample(n_sample=20):
+    """The reference's algorithm (oracle restatement of spectrum.lanczos: three
+    terms, full Gram-Schmidt twice) on a 20-site chain sector, scaled to 26
+    sites by the dimension (the work per step is proportional to it)."""
+    from energy_level_b200 import configs
+    from oracle import ref
+    codes = ref.independent_states(n_sample, configs.chain_edges(n_sample), None)
+    calib, pairs, om, de = chain_model(n_sample, Om=2.0, Delta=1.0)
+    H = ref.sparse_h(n_sample, codes, om, de, pairs)
+    rng = np.random.default_rng(11)
+    phi = rng.normal(size=len(codes)) + 1j * rng.normal(size=len(codes))
+    t0 = time.perf_counter()
+    ref.lanczos_tridiag(lambda v: H @ v, phi, SPEC_K, reorth=True)
+    dt = time.perf_counter() - t0
+    full_dim = 317811
+    scale = full_dim / len(codes)
+    return {"value": 1.0 / (dt * scale), "unit": "spectra/s", "cores": 1, "kind": "port",
+            "sample": "oracle Lanczos (k 200, full reorthogonalisation twice, numpy) on the 20-site chain "
+                      "sector (dim %d), %.2f s, scaled by the dimension to 317,811" % (len(codes), dt)}
+
+
 # --- sector scan: dipolar XY chain, every fixed-excitation sector
 
 SCAN_N = 20
@@ -1111,7 +1197,7 @@ def cpu_scan_sample(n_sample=16):
                       "%d sites by stored H entries (x%.1f)" % (n_sample, dt, n, scale)}
 
 
-NATIVE = {"hv_chain31": native_hv, "lanczos_chain12": native_lanczos12, "ramp_chain31": native_ramp31,
+NATIVE = {"spectrum_chain26": native_spectrum26, "hv_chain31": native_hv, "lanczos_chain12": native_lanczos12, "ramp_chain31": native_ramp31,
           "batch512": native_batch512, "adjoint_ring20": native_adjoint20, "scan_xy20": native_scan_xy20}
 
 
@@ -1147,6 +1233,9 @@ def run_reference_workload(args):
     elif w == "scan_xy20":
         cb = cpu_scan_sample()
         v, unit = cb["value"], "scans/s"
+    elif w == "spectrum_chain26":
+        cb = cpu_spectrum_sample()
+        v, unit = cb["value"], "spectra/s"
     else:
         cb = cpu_adjoint_sample(configs.ring20())
         v, unit = cb["value"], "grads/s"

@@ -1052,12 +1052,17 @@ __global__ void k_axpby(int64_t len, double a_re, double a_im, const S *x,
 }
 
 // partials[bx][j] (re, im) of <V_j, w> over the block's rows.
-constexpr int GJ = 8;
+constexpr int GJ = 16;
+// dots_j = <V_j, w> for a group of GJ columns per blockIdx.y: every thread
+// accumulates its rows in FP64 registers, warps reduce by shuffles (fixed
+// tree), then the block's warps in order; per-block partials are summed by
+// k_sum_partials in block order (deterministic).
 template <typename S, bool C>
-__global__ void k_gemv_t(int64_t len, int k, const S *V, int64_t ld, const S *w,
-                         double *partials) {
-  __shared__ double red[256][2 * GJ];
+__global__ void __launch_bounds__(256) k_gemv_t(int64_t len, int k, const S *V, int64_t ld, const S *w,
+                                                double *partials) {
+  __shared__ double red[8][2 * GJ];
   const int j0 = blockIdx.y * GJ;
+  const int nq = min(GJ, k - j0);
   double accr[GJ], acci[GJ];
 #pragma unroll
   for (int q = 0; q < GJ; ++q) { accr[q] = 0.0; acci[q] = 0.0; }
@@ -1067,7 +1072,7 @@ __global__ void k_gemv_t(int64_t len, int k, const S *V, int64_t ld, const S *w,
       const double wr = w[2 * i], wi = w[2 * i + 1];
 #pragma unroll
       for (int q = 0; q < GJ; ++q) {
-        if (j0 + q < k) {
+        if (q < nq) {
           const S *vj = V + (size_t)(j0 + q) * ld * 2;
           const double vr = vj[2 * i], vi = vj[2 * i + 1];
           accr[q] += vr * wr + vi * wi;
@@ -1078,20 +1083,25 @@ __global__ void k_gemv_t(int64_t len, int k, const S *V, int64_t ld, const S *w,
       const double wv = w[i];
 #pragma unroll
       for (int q = 0; q < GJ; ++q)
-        if (j0 + q < k) accr[q] += (double)V[(size_t)(j0 + q) * ld + i] * wv;
+        if (q < nq) accr[q] += (double)V[(size_t)(j0 + q) * ld + i] * wv;
     }
   }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int q = 0; q < GJ; ++q) { red[threadIdx.x][2 * q] = accr[q]; red[threadIdx.x][2 * q + 1] = acci[q]; }
-  __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
-    if (threadIdx.x < s)
-      for (int q = 0; q < 2 * GJ; ++q) red[threadIdx.x][q] += red[threadIdx.x + s][q];
-    __syncthreads();
+  for (int q = 0; q < GJ; ++q) {
+    double a = accr[q], b = acci[q];
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (C) b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) { red[warp][2 * q] = a; red[warp][2 * q + 1] = b; }
   }
+  __syncthreads();
   if (threadIdx.x < 2 * GJ) {
     const int q = threadIdx.x >> 1;
-    if (j0 + q < k) partials[((size_t)blockIdx.x * k + j0 + q) * 2 + (threadIdx.x & 1)] = red[0][threadIdx.x];
+    double sum = 0.0;
+    for (int wp = 0; wp < (int)(blockDim.x >> 5); ++wp) sum += red[wp][threadIdx.x];
+    if (q < nq) partials[((size_t)blockIdx.x * k + j0 + q) * 2 + (threadIdx.x & 1)] = sum;
   }
 }
 
@@ -1103,29 +1113,55 @@ __global__ void k_sum_partials(int nparts, int k, const double *partials, double
   }
 }
 
-// w -= sum_j coef_j V_j  (sub = true) or w = sum_j coef_j V_j (sub = false)
+// w -= sum_j coef_j V_j  (sub = true) or w = sum_j coef_j V_j (sub = false).
+// The coefficients are staged in shared memory (k <= GN_MAX, else read from
+// global memory); four partial sums per row keep four column loads in flight.
+constexpr int GN_MAX = 1024;
 template <typename S, bool C>
-__global__ void k_gemv_n(int64_t len, int k, const S *V, int64_t ld,
-                         const double *coef, S *w, bool sub) {
+__global__ void __launch_bounds__(256) k_gemv_n(int64_t len, int k, const S *V, int64_t ld,
+                                                const double *coef, S *w, bool sub) {
+  __shared__ double cs[2 * GN_MAX];
+  const bool staged = k <= GN_MAX;
+  if (staged)
+    for (int t = threadIdx.x; t < 2 * k; t += blockDim.x) cs[t] = coef[t];
+  __syncthreads();
+  const double *cf = staged ? cs : coef;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
        i += (int64_t)gridDim.x * blockDim.x) {
-    double sr = 0.0, si = 0.0;
-    for (int j = 0; j < k; ++j) {
-      const double cr = coef[2 * j], ci = coef[2 * j + 1];
+    double sr[4] = {0.0, 0.0, 0.0, 0.0}, si[4] = {0.0, 0.0, 0.0, 0.0};
+    int j = 0;
+    for (; j + 4 <= k; j += 4) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double cr = cf[2 * (j + u)], ci = cf[2 * (j + u) + 1];
+        if constexpr (C) {
+          const S *vj = V + (size_t)(j + u) * ld * 2;
+          const double vr = vj[2 * i], vi = vj[2 * i + 1];
+          sr[u] += cr * vr - ci * vi;
+          si[u] += cr * vi + ci * vr;
+        } else {
+          sr[u] += cr * (double)V[(size_t)(j + u) * ld + i];
+        }
+      }
+    }
+    for (; j < k; ++j) {
+      const double cr = cf[2 * j], ci = cf[2 * j + 1];
       if constexpr (C) {
         const S *vj = V + (size_t)j * ld * 2;
         const double vr = vj[2 * i], vi = vj[2 * i + 1];
-        sr += cr * vr - ci * vi;
-        si += cr * vi + ci * vr;
+        sr[0] += cr * vr - ci * vi;
+        si[0] += cr * vi + ci * vr;
       } else {
-        sr += cr * (double)V[(size_t)j * ld + i];
+        sr[0] += cr * (double)V[(size_t)j * ld + i];
       }
     }
+    const double tr = (sr[0] + sr[1]) + (sr[2] + sr[3]);
+    const double ti = (si[0] + si[1]) + (si[2] + si[3]);
     if constexpr (C) {
-      if (sub) { w[2 * i] = (S)((double)w[2 * i] - sr); w[2 * i + 1] = (S)((double)w[2 * i + 1] - si); }
-      else { w[2 * i] = (S)sr; w[2 * i + 1] = (S)si; }
+      if (sub) { w[2 * i] = (S)((double)w[2 * i] - tr); w[2 * i + 1] = (S)((double)w[2 * i + 1] - ti); }
+      else { w[2 * i] = (S)tr; w[2 * i + 1] = (S)ti; }
     } else {
-      w[i] = sub ? (S)((double)w[i] - sr) : (S)sr;
+      w[i] = sub ? (S)((double)w[i] - tr) : (S)tr;
     }
   }
 }
@@ -1515,9 +1551,15 @@ int launch_axpby(el_ctx *ctx, int dtype, int64_t len, double a_re, double a_im,
 int launch_gemv_t(el_ctx *ctx, int dtype, int64_t len, int k, const void *V,
                   int64_t ld, const void *w, double *dots_out) {
   if (k <= 0) return EL_OK;
+  // one CTA per SM and column group: each thread walks many rows, so the
+  // block reduction is paid once per many rows
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   int gx = grid_for(len, 256);
-  if (gx > 296) gx = 296;
-  dim3 grid(gx, (k + GJ - 1) / GJ);
+  const int ngroups = (k + GJ - 1) / GJ;
+  const int gcap = std::max(1, (2 * sms + ngroups - 1) / ngroups);   // about two CTAs per SM in total
+  if (gx > gcap) gx = gcap;
+  dim3 grid(gx, ngroups);
   int rc = ensure_partials(ctx, (size_t)gx * k * 2);
   if (rc) return rc;
   switch (dtype) {
