@@ -7,12 +7,14 @@ and time evolution through TIME_BACKENDS -> runspec._ENGINE_TABLE
 B200 backends in the same shapes:
 
     EQ_BACKENDS   'b200-lanczos': ('gs', 'spectrum', 'ramp')   'b200-kpm': ('thermal', 'dos')
-    TIME_BACKENDS 'b200-cheb': TimeBackend(segments, projected, return_state)
+    TIME_BACKENDS 'b200-cheb': TimeBackend(segments, projected, gamma, return_state,
+                                           pauli='full')
 
 ``solve_equilibrium`` accepts the reference's ``system`` dict and keyword
 arguments for these names and returns the same result keys as
-eq_route._solve_ground / _solve_thermal / _solve_dos.  ``install_into``
-registers the names into a reference backends module.
+eq_route._solve_ground / _solve_thermal / _solve_dos (and the spectrum and
+ramp routes).  ``install_into`` adds the names to a module shaped like the
+reference's backends.py (EQ_BACKENDS, TIME_BACKENDS, TimeBackend).
 """
 from __future__ import annotations
 
