@@ -44,18 +44,32 @@ struct AdjArgs {
   double *out;             // [2]: Re<G_O x, t>, Re<G_D x, t>
 };
 
+// One adjoint step over all rows: y = clam lam + alpha H x + beta x - z and
+// the two gradient dots.  ADJ_LANES adjacent lanes share a row and take the
+// sites k = lane, lane + ADJ_LANES, ...: the small bases that the pulse
+// gradient runs on (tens of thousands of rows) would otherwise leave most
+// SMs idle while each thread walks all n flips.  The row loop is uniform
+// over the block so that every lane reaches the shuffles.  The CTA that
+// finishes last sums the per-CTA partials with all its threads in a fixed
+// order (the result does not depend on which CTA is last).
+constexpr int ADJ_LANES = 4;
+
 template <typename S>
 __global__ void __launch_bounds__(256) k_adjoint_step(BasisDev B, AdjArgs<S> P) {
+  constexpr int G = ADJ_LANES;
   __shared__ double red[2][256];
   __shared__ bool last;
+  const int lane = (int)threadIdx.x & (G - 1);
+  const int64_t rpb = blockDim.x / G;
   double gO = 0.0, gD = 0.0;
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < B.dim;
-       r += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t base = (int64_t)blockIdx.x * rpb; base < B.dim; base += (int64_t)gridDim.x * rpb) {
+    const int64_t mine = base + threadIdx.x / G;
+    const bool active = mine < B.dim;           // the same for the G lanes of a row
+    const int64_t r = active ? mine : 0;        // lanes past the end work on row 0
     const uint64_t code = el::unrank_row(B, r);
-    const S xr = P.x[2 * r], xi = P.x[2 * r + 1];
-    S sre = 0, sim = 0, dsum = P.diagV[r], nb = 0;
-    for (int k = 0; k < B.n; ++k) {
-      if ((code >> k) & 1ULL) { dsum += P.delta[k]; nb += P.bsh[k]; }
+    S sre = 0, sim = 0, dpart = 0, nb = 0;
+    for (int k = lane; k < B.n; k += G) {
+      if ((code >> k) & 1ULL) { dpart += P.delta[k]; nb += P.bsh[k]; }
       const S amp = P.ahalf[k];
       if (amp == S(0)) continue;
       const int64_t tg = el::flip_target(B, code, r, k);
@@ -63,6 +77,16 @@ __global__ void __launch_bounds__(256) k_adjoint_step(BasisDev B, AdjArgs<S> P) 
       sre += amp * P.x[2 * tg];
       sim += amp * P.x[2 * tg + 1];
     }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) {
+      sre += __shfl_xor_sync(0xffffffffu, sre, off);
+      sim += __shfl_xor_sync(0xffffffffu, sim, off);
+      dpart += __shfl_xor_sync(0xffffffffu, dpart, off);
+      nb += __shfl_xor_sync(0xffffffffu, nb, off);
+    }
+    if (lane != 0 || !active) continue;
+    const S xr = P.x[2 * r], xi = P.x[2 * r + 1];
+    const S dsum = P.diagV[r] + dpart;
     // H x = dsum x + Omega S
     const S hre = dsum * xr + P.om * sre, him = dsum * xi + P.om * sim;
     S yre = P.alpha * hre + P.beta * xr, yim = P.alpha * him + P.beta * xi;
@@ -97,12 +121,26 @@ __global__ void __launch_bounds__(256) k_adjoint_step(BasisDev B, AdjArgs<S> P) 
     last = (atomicAdd(P.counter, 1u) == gridDim.x - 1);
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    double a = 0.0, b = 0.0;
-    for (unsigned i = 0; i < gridDim.x; ++i) { a += __ldcg(&P.partials[2 * i]); b += __ldcg(&P.partials[2 * i + 1]); }
-    P.out[0] = a;
-    P.out[1] = b;
+  if (!last) return;
+  __threadfence();
+  double a = 0.0, b = 0.0;
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+    a += __ldcg(&P.partials[2 * i]);
+    b += __ldcg(&P.partials[2 * i + 1]);
+  }
+  red[0][threadIdx.x] = a;
+  red[1][threadIdx.x] = b;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + s];
+      red[1][threadIdx.x] += red[1][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    P.out[0] = red[0][0];
+    P.out[1] = red[1][0];
     *P.counter = 0u;
   }
 }
@@ -214,7 +252,8 @@ int adjoint_impl(el_ctx *ctx, el_ham *h, int dtype, int K, const double *tau, co
   // ---- objective and lambda_K
   double F = 0.0;
   const int grid = el::grid_for(dim, 256);
-  rc = el::ensure_partials(ctx, (size_t)std::max(grid, 2) * 2);
+  const int agrid = el::grid_for(dim * ADJ_LANES, 256);
+  rc = el::ensure_partials(ctx, (size_t)std::max(std::max(grid, agrid), 2) * 2);
   if (rc) return rc;
   if (target) {
     rc = el::launch_gemv_t(ctx, dtype, dim, 1, target, dim, ckp(K), ctx->d_scalars);
@@ -289,7 +328,7 @@ int adjoint_impl(el_ctx *ctx, el_ham *h, int dtype, int K, const double *tau, co
       P.t = (const S *)term(m);
       P.y = (S *)U[m % 3];
       P.out = d_g + ((size_t)k * (Mmax + 1) + (m + 1)) * 2;
-      k_adjoint_step<S><<<grid, 256, 0, ctx->stream>>>(B, P);
+      k_adjoint_step<S><<<agrid, 256, 0, ctx->stream>>>(B, P);
       EL_LAUNCH_CHECK(ctx);
     }
     // lambda_{k-1} = u_0

@@ -338,6 +338,16 @@ __global__ void __launch_bounds__(256) k_apply_hop(BasisDev B, HamArgs<S> H, KAr
 // gathers before any of them is accumulated.  CT/RT are 32-bit when the
 // code has at most 32 bits and the basis fewer than 2^31 rows, which halves
 // the integer work of unranking and target arithmetic.
+//
+// G > 1 (single vector, small bases): G adjacent lanes of a warp share one
+// row and take the bits k = lane, lane + G, ...; their partial flip sums and
+// detunings meet in a butterfly of warp shuffles and the row's first lane
+// runs the epilogue.  A basis of a few ten thousand rows fills only part of
+// the 148 SMs with one thread per row, and each thread then waits for n
+// dependent rounds of gathers; G lanes per row cut that chain by G and give
+// the grid G times more warps.  The row loop is uniform over the block so
+// that every lane reaches the shuffles; lanes past the last row work on
+// row 0 and store nothing.
 
 template <typename S, int W>
 __device__ __forceinline__ void ld_row(const S *p, S (&v)[W]) {
@@ -429,8 +439,9 @@ __device__ __forceinline__ RT ring_rank_t(const BasisDev &B, CT c, int n) {
   return r;
 }
 
-template <typename S, bool C, int NV, int LAY, bool WANT, typename CT, typename RT>
+template <typename S, bool C, int NV, int LAY, bool WANT, typename CT, typename RT, int G>
 __global__ void __launch_bounds__(256) k_apply_row(BasisDev B, HamArgs<S> H, KArgs K) {
+  static_assert(G == 1 || (NV == 1 && 32 % G == 0), "lanes per row: G divides 32, one vector");
   constexpr int W = NV * (C ? 2 : 1);
   constexpr int U = 4;
   const int n = B.n;
@@ -438,8 +449,16 @@ __global__ void __launch_bounds__(256) k_apply_row(BasisDev B, HamArgs<S> H, KAr
   const S *__restrict__ xp = (const S *)K.x;
   double q0 = 0, q1 = 0, q2 = 0, q3 = 0;
   const RT dim = (RT)B.dim;
-  const RT stride = (RT)gridDim.x * blockDim.x;
-  for (RT row = (RT)blockIdx.x * blockDim.x + threadIdx.x; row < dim; row += stride) {
+  const int lane = (int)threadIdx.x & (G - 1);
+  const RT rpb = (RT)(blockDim.x / G);
+  const RT stride = (RT)gridDim.x * rpb;
+  for (RT base = (RT)blockIdx.x * rpb; base < dim; base += stride) {
+    const RT mine = base + (RT)(threadIdx.x / G);
+    const bool active = mine < dim;       // the same for the G lanes of a row
+    if constexpr (G == 1) {
+      if (!active) break;
+    }
+    const RT row = active ? mine : (RT)0;
     const CT code = unrank_fib<LAY, CT, RT>(B, row);
     CT allowed = full;
     if constexpr (LAY != EL_LAYOUT_FULL) {
@@ -452,13 +471,13 @@ __global__ void __launch_bounds__(256) k_apply_row(BasisDev B, HamArgs<S> H, KAr
 #pragma unroll
     for (int i = 0; i < W; ++i) h[i] = S(0);
     S dsum = S(0);
-    for (int k0 = 0; k0 < n; k0 += U) {
+    for (int j0 = 0; j0 * G < n; j0 += U) {
       S xv[U][W];
       S ar[U], ai[U];
       bool ok[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int k = k0 + u;
+        const int k = (j0 + u) * G + lane;
         ok[u] = false;
         ar[u] = S(0);
         ai[u] = S(0);
@@ -506,6 +525,15 @@ __global__ void __launch_bounds__(256) k_apply_row(BasisDev B, HamArgs<S> H, KAr
           for (int v = 0; v < NV; ++v) h[v] += ar[u] * xv[u][v];
         }
       }
+    }
+    if constexpr (G > 1) {
+#pragma unroll
+      for (int off = G / 2; off > 0; off >>= 1) {
+#pragma unroll
+        for (int i = 0; i < W; ++i) h[i] += __shfl_xor_sync(0xffffffffu, h[i], off);
+        dsum += __shfl_xor_sync(0xffffffffu, dsum, off);
+      }
+      if (lane != 0 || !active) continue;
     }
     S xr[W];
     ld_row<S, W>(xp + (size_t)row * W, xr);
@@ -1279,22 +1307,37 @@ bool row_kernel_ok(const el_ham *h, const ApplyArgs &A) {
   return true;
 }
 
-template <typename S, bool C, int NV, bool WANT, typename CT, typename RT>
+template <typename S, bool C, int NV, bool WANT, typename CT, typename RT, int G>
 void launch_row_ct(el_ctx *ctx, int lay, int grid, const BasisDev &B, const HamArgs<S> &H, const KArgs &K) {
   if (lay == EL_LAYOUT_FULL)
-    k_apply_row<S, C, NV, EL_LAYOUT_FULL, WANT, CT, RT><<<grid, 256, 0, ctx->stream>>>(B, H, K);
+    k_apply_row<S, C, NV, EL_LAYOUT_FULL, WANT, CT, RT, G><<<grid, 256, 0, ctx->stream>>>(B, H, K);
   else if (lay == EL_LAYOUT_CHAIN)
-    k_apply_row<S, C, NV, EL_LAYOUT_CHAIN, WANT, CT, RT><<<grid, 256, 0, ctx->stream>>>(B, H, K);
+    k_apply_row<S, C, NV, EL_LAYOUT_CHAIN, WANT, CT, RT, G><<<grid, 256, 0, ctx->stream>>>(B, H, K);
   else
-    k_apply_row<S, C, NV, EL_LAYOUT_RING, WANT, CT, RT><<<grid, 256, 0, ctx->stream>>>(B, H, K);
+    k_apply_row<S, C, NV, EL_LAYOUT_RING, WANT, CT, RT, G><<<grid, 256, 0, ctx->stream>>>(B, H, K);
+}
+
+// Rows below which a single-vector row kernel gives each row ROW_LANES lanes:
+// one thread per row would occupy fewer than two CTAs of 256 per SM.
+constexpr int64_t LANE_ROWS = 148 * 512;
+constexpr int ROW_LANES = 4;
+
+bool row_lanes(const BasisDev &B, int nvec) {
+  return nvec == 1 && B.n <= 32 && B.dim < LANE_ROWS;
 }
 
 template <typename S, bool C, int NV, bool WANT>
 void launch_row_lay(el_ctx *ctx, int lay, int grid, const BasisDev &B, const HamArgs<S> &H, const KArgs &K) {
+  if constexpr (NV == 1) {
+    if (row_lanes(B, NV)) {
+      launch_row_ct<S, C, NV, WANT, uint32_t, int32_t, ROW_LANES>(ctx, lay, grid, B, H, K);
+      return;
+    }
+  }
   if (B.n <= 32 && B.dim < ((int64_t)1 << 31))
-    launch_row_ct<S, C, NV, WANT, uint32_t, int32_t>(ctx, lay, grid, B, H, K);
+    launch_row_ct<S, C, NV, WANT, uint32_t, int32_t, 1>(ctx, lay, grid, B, H, K);
   else
-    launch_row_ct<S, C, NV, WANT, uint64_t, int64_t>(ctx, lay, grid, B, H, K);
+    launch_row_ct<S, C, NV, WANT, uint64_t, int64_t, 1>(ctx, lay, grid, B, H, K);
 }
 
 template <typename S, bool C>
@@ -1362,7 +1405,8 @@ int launch_chain_tile_v(el_ctx *ctx, int nvec, bool want, int L, int64_t ntiles,
 
 int launch_apply_row(el_ctx *ctx, el_ham *h, const ApplyArgs &A, const BasisDev &B, KArgs K) {
   const int lay = h->basis->layout;
-  const int grid = el::grid_for(h->basis->dim, 256);
+  const int64_t lanes = row_lanes(B, (int)A.nvec) ? ROW_LANES : 1;
+  const int grid = el::grid_for(h->basis->dim * lanes, 256);
   const bool want = K.want != 0;
   if (want) {
     K.nvec = 1;
