@@ -53,10 +53,12 @@ struct AdjArgs {
 // finishes last sums the per-CTA partials with all its threads in a fixed
 // order (the result does not depend on which CTA is last).
 constexpr int ADJ_LANES = 4;
+constexpr int ADJ_UNROLL = 4;   // gathers in flight per lane
 
 template <typename S>
-__global__ void __launch_bounds__(256) k_adjoint_step(BasisDev B, AdjArgs<S> P) {
+__global__ void __launch_bounds__(256, 4) k_adjoint_step(BasisDev B, AdjArgs<S> P) {
   constexpr int G = ADJ_LANES;
+  typedef typename el::VecT<S, true>::type V2;   // one complex entry, one load
   __shared__ double red[2][256];
   __shared__ bool last;
   const int lane = (int)threadIdx.x & (G - 1);
@@ -68,14 +70,33 @@ __global__ void __launch_bounds__(256) k_adjoint_step(BasisDev B, AdjArgs<S> P) 
     const int64_t r = active ? mine : 0;        // lanes past the end work on row 0
     const uint64_t code = el::unrank_row(B, r);
     S sre = 0, sim = 0, dpart = 0, nb = 0;
-    for (int k = lane; k < B.n; k += G) {
-      if ((code >> k) & 1ULL) { dpart += P.delta[k]; nb += P.bsh[k]; }
-      const S amp = P.ahalf[k];
-      if (amp == S(0)) continue;
-      const int64_t tg = el::flip_target(B, code, r, k);
-      if (tg < 0) continue;
-      sre += amp * P.x[2 * tg];
-      sim += amp * P.x[2 * tg + 1];
+    // a lane's sites k = (j0 + u) G + lane: all U gathers of a round are
+    // issued before any of them is accumulated
+    for (int j0 = 0; j0 * G < B.n; j0 += ADJ_UNROLL) {
+      S xa[ADJ_UNROLL], xb[ADJ_UNROLL], am[ADJ_UNROLL];
+#pragma unroll
+      for (int u = 0; u < ADJ_UNROLL; ++u) {
+        const int k = (j0 + u) * G + lane;
+        am[u] = S(0);
+        xa[u] = S(0);
+        xb[u] = S(0);
+        if (k < B.n) {
+          if ((code >> k) & 1ULL) { dpart += P.delta[k]; nb += P.bsh[k]; }
+          const S amp = P.ahalf[k];
+          const int64_t tg = amp == S(0) ? -1 : el::flip_target(B, code, r, k);
+          if (tg >= 0) {
+            const V2 v = reinterpret_cast<const V2 *>(P.x)[tg];
+            am[u] = amp;
+            xa[u] = v.x;
+            xb[u] = v.y;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < ADJ_UNROLL; ++u) {   // a skipped flip adds 0 * 0
+        sre += am[u] * xa[u];
+        sim += am[u] * xb[u];
+      }
     }
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) {

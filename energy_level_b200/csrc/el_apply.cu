@@ -334,8 +334,9 @@ __global__ void __launch_bounds__(256) k_apply_hop(BasisDev B, HamArgs<S> H, KAr
 // segment with 16-byte loads.  The bit loop runs over k = 0..n-1 in the same
 // order in every thread (warp-uniform k), so Fibonacci weights, amplitudes
 // and detunings are broadcast kernel-parameter reads; a flip that leaves the
-// basis only predicates its load off.  Four bits per round issue their
-// gathers before any of them is accumulated.  CT/RT are 32-bit when the
+// basis only predicates its load off.  Four bits per round (eight per lane
+// when G lanes share a row, below) issue their gathers before any of them
+// is accumulated.  CT/RT are 32-bit when the
 // code has at most 32 bits and the basis fewer than 2^31 rows, which halves
 // the integer work of unranking and target arithmetic.
 //
@@ -443,7 +444,7 @@ template <typename S, bool C, int NV, int LAY, bool WANT, typename CT, typename 
 __global__ void __launch_bounds__(256) k_apply_row(BasisDev B, HamArgs<S> H, KArgs K) {
   static_assert(G == 1 || (NV == 1 && 32 % G == 0), "lanes per row: G divides 32, one vector");
   constexpr int W = NV * (C ? 2 : 1);
-  constexpr int U = 4;
+  constexpr int U = G == 1 ? 4 : 8;   // with lanes, one round covers up to 8 G sites
   const int n = B.n;
   const CT full = (n >= (int)(8 * sizeof(CT))) ? ~(CT)0 : (((CT)1 << n) - 1);
   const S *__restrict__ xp = (const S *)K.x;
