@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _lib
 from .core import _torch, default_context
-from .model import model_arrays
+from .model import model_columns
 
 _TUNED = {}
 
@@ -35,32 +35,40 @@ def _layout(n, edges):
                      'or full bases')
 
 
+def pack_instances(instances):
+    """Host arrays of el_batch_create for a list of instances: [n int32,
+    layout int32, Omega float64 (concatenated), delta float64, pair offsets
+    int32 [count + 1], i int32, j int32, V float64] (one dummy entry where a
+    list is empty).  Raises the model's errors for an invalid instance."""
+    ns, lays, om, de, npair, pi, pj, V = [], [], [], [], [], [], [], []
+    for inst in instances:
+        n, o, d, (i, j, v) = model_columns(inst['calib'], inst.get('Om'), inst.get('delta'),
+                                           inst.get('gamma'), inst.get('terms'))
+        if np.any(o.imag != 0):
+            raise ValueError('batched solves need real Omega')
+        ns.append(n)
+        lays.append(_layout(n, inst.get('edges')))
+        om.append(o.real)
+        de.append(d)
+        pi.append(i); pj.append(j); V.append(v)
+        npair.append(len(v))
+    arr = lambda x, t: np.ascontiguousarray(np.asarray(x, dtype=t))
+    cat = lambda x, t, empty: arr(np.concatenate(x) if sum(map(len, x)) else [empty], t)
+    poff = np.concatenate([[0], np.cumsum(npair, dtype=np.int64)])
+    return [arr(ns, np.int32), arr(lays, np.int32), cat(om, np.float64, 0.0), cat(de, np.float64, 0.0),
+            arr(poff, np.int32), cat(pi, np.int32, 0), cat(pj, np.int32, 0), cat(V, np.float64, 0.0)]
+
+
 class BatchedGroundStates:
     def __init__(self, instances, dtype='float32', max_iter=200, tol=None, device=0, ctx=None):
         if dtype not in ('float32', 'float64'):
             raise ValueError('dtype 必须为 float32/float64')
         self.ctx = ctx or default_context(device)
-        ns, lays, om, de, poff, pi, pj, V = [], [], [], [], [0], [], [], []
-        for inst in instances:
-            n, o, d, pairs = model_arrays(inst['calib'], inst.get('Om'), inst.get('delta'),
-                                          inst.get('gamma'), inst.get('terms'))
-            if np.any(o.imag != 0):
-                raise ValueError('batched solves need real Omega')
-            ns.append(n)
-            lays.append(_layout(n, inst.get('edges')))
-            om.extend(o.real.tolist())
-            de.extend(d.tolist())
-            for i, j, v in pairs:
-                pi.append(i); pj.append(j); V.append(v)
-            poff.append(len(V))
-        self.count = len(ns)
-        self.n_sites = np.asarray(ns)
+        self._keep = pack_instances(instances)
+        self.count = len(self._keep[0])
+        self.n_sites = self._keep[0].astype(np.int64)
         self.dtype = dtype
         self.tol = float(tol if tol is not None else (1e-5 if dtype == 'float32' else 1e-10))
-        arr = lambda x, t: np.ascontiguousarray(np.asarray(x, dtype=t))
-        self._keep = [arr(ns, np.int32), arr(lays, np.int32), arr(om, np.float64), arr(de, np.float64),
-                      arr(poff, np.int32), arr(pi if pi else [0], np.int32), arr(pj if pj else [0], np.int32),
-                      arr(V if V else [0.0], np.float64)]
         k = self._keep
         h = C.c_void_p()
         self.ctx.call('el_batch_create', C.c_int(self.count), C.c_void_p(k[0].ctypes.data),

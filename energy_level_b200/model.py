@@ -45,6 +45,14 @@ def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None, exchange=No
     the terms in use; None refuses a nonzero J or A with ConfigConflict.
     ``allow_loss``: accept gamma != 0 (the caller sets the loss diagonal);
     otherwise it is refused with ConfigConflict."""
+    n, Om, delta, (pi, pj, V) = model_columns(calib, Om, delta, gamma, terms, exchange, allow_loss)
+    return n, Om, delta, list(zip(pi.tolist(), pj.tolist(), V.tolist()))
+
+
+def model_columns(calib, Om=None, delta=None, gamma=None, terms=None, exchange=None, allow_loss=False):
+    """model_arrays with the density pairs as columns: (n, Om, delta,
+    (i int32[m], j int32[m], V float64[m])) for the pairs with V != 0, in
+    calib order.  Same checks and errors as model_arrays."""
     atoms = (calib or {}).get('atoms') or []
     n = len(atoms)
     if n == 0:
@@ -56,26 +64,37 @@ def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None, exchange=No
         raise ValueError('Om/delta/gamma 须为有限、长度为 N 的数组')
     if np.any(gamma != 0) and not allow_loss:
         raise ConfigConflict('b200 backends need a Hermitian H (gamma = 0)', keys=('manybody.gamma_mhz',))
-    use = set(active_terms(calib) if terms is None else terms)
     raw = calib.get('pairs') or []
     m = len(raw)
+    none = (np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0))
     if m == 0:
-        return n, Om, delta, []
-    # columns of the pair list; the checks below raise, for the first pair
-    # that fails any of them, the error that pair's own checks would raise
-    # first (range, J, A, V, in that order)
-    ii = np.fromiter((p['i'] for p in raw), dtype=np.int64, count=m)
-    jj = np.fromiter((p['j'] for p in raw), dtype=np.int64, count=m)
-    zero = np.zeros(m, complex)
+        return n, Om, delta, none
 
     def column(key):
         try:       # real values (the common case) without building Python complex numbers
             return np.fromiter((p.get(key) or 0.0 for p in raw), dtype=float, count=m).astype(complex)
         except TypeError:
             return np.array([p.get(key) or 0.0 for p in raw], dtype=complex)
-    V = column('V') if 'I1' in use else zero
-    J = column('J') if 'I2' in use else zero
-    A = column('A') if 'I3' in use else zero
+    if terms is None:
+        terms = (calib or {}).get('terms')
+    if terms is None:
+        # the terms a calib carries (active_terms): a channel is on when any
+        # of its pair values has a nonzero magnitude
+        cols = {key: column(key) for key in ('V', 'J', 'A')}
+        use = {name for name, key in (('I1', 'V'), ('I2', 'J'), ('I3', 'A'))
+               if np.any(np.abs(cols[key]) > 0.0)}
+    else:
+        use = set(terms)
+        cols = {key: column(key) for name, key in (('I1', 'V'), ('I2', 'J'), ('I3', 'A')) if name in use}
+    # columns of the pair list; the checks below raise, for the first pair
+    # that fails any of them, the error that pair's own checks would raise
+    # first (range, J, A, V, in that order)
+    ii = np.fromiter((p['i'] for p in raw), dtype=np.int64, count=m)
+    jj = np.fromiter((p['j'] for p in raw), dtype=np.int64, count=m)
+    zero = np.zeros(m, complex)
+    V = cols['V'] if 'I1' in use else zero
+    J = cols['J'] if 'I2' in use else zero
+    A = cols['A'] if 'I3' in use else zero
     checks = [
         ((ii < 0) | (ii >= n) | (jj < 0) | (jj >= n) | (ii == jj),
          lambda k: ValueError('pair (%d, %d) out of range' % (ii[k], jj[k]))),
@@ -100,8 +119,9 @@ def model_arrays(calib, Om=None, delta=None, gamma=None, terms=None, exchange=No
     if exchange is not None:
         for k in np.flatnonzero((J != 0) | (A != 0)):
             exchange.append((int(ii[k]), int(jj[k]), complex(J[k]), complex(A[k])))
-    pairs = [(int(ii[k]), int(jj[k]), float(V[k].real)) for k in np.flatnonzero(V.real != 0)]
-    return n, Om, delta, pairs
+    keep = np.flatnonzero(V.real != 0)
+    return n, Om, delta, (ii[keep].astype(np.int32), jj[keep].astype(np.int32),
+                          np.ascontiguousarray(V.real[keep], dtype=np.float64))
 
 
 def _is_chain_or_ring(n, edges):

@@ -75,6 +75,31 @@ def test_model_refuses_unimplemented_channels():
         model.model_arrays({"atoms": [], "pairs": []})
 
 
+def test_model_columns_match_active_terms():
+    """Without ``terms`` the channels in use are the calib's own (its 'terms'
+    key, else every channel with a nonzero pair value), exactly as if
+    active_terms(calib) had been passed; the column form equals the tuples."""
+    calib = {k: v for k, v in configs.calib_from_positions(configs.chain_positions(5)).items()
+             if k != "terms"}
+    variants = [calib,
+                dict(calib, pairs=[dict(p, V=0.0) for p in calib["pairs"]]),
+                dict(calib, pairs=[dict(p, V=float("nan") if k == 0 else 0.0)
+                                   for k, p in enumerate(calib["pairs"])]),
+                dict(calib, pairs=[dict(p, J=0.0, A=None) for p in calib["pairs"]]),
+                dict(calib, terms=["I1"], pairs=[dict(p, J=0.5) for p in calib["pairs"]])]
+    for c in variants:
+        ex_a, ex_b = [], []
+        got = model.model_arrays(c, np.ones(5), np.zeros(5), exchange=ex_a)
+        want = model.model_arrays(c, np.ones(5), np.zeros(5), terms=model.active_terms(c), exchange=ex_b)
+        assert got[0] == want[0] and repr(got[3]) == repr(want[3]) and ex_a == ex_b
+        n, _, _, (pi, pj, V) = model.model_columns(c, np.ones(5), np.zeros(5), exchange=[])
+        assert repr(list(zip(pi.tolist(), pj.tolist(), V.tolist()))) == repr(got[3])
+        assert pi.dtype == np.int32 and V.dtype == np.float64
+    with pytest.raises(model.ConfigConflict):   # J in use without an exchange list
+        model.model_columns(dict(calib, pairs=[dict(p, J=0.5) for p in calib["pairs"]]),
+                            np.ones(5), np.zeros(5))
+
+
 def test_state_grammar_full_and_projected():
     n = 6
     codes = ref.independent_states(n, configs.chain_edges(n), None)
@@ -169,3 +194,33 @@ def test_sector_scan_refuses_before_touching_the_device():
         scan_ground_sectors(xy["calib"], xy["delta"], np.zeros(6), terms=["I1", "I2"], backend="dmrg")
     with pytest.raises(ValueError):
         SectorScan({"atoms": [], "pairs": []})
+
+
+def test_pack_instances_matches_calib_pairs():
+    """The batched solver's host arrays, against a direct walk over each
+    instance's calib: sizes, layouts, drive columns and the V pairs in calib
+    order with their offsets; an instance without pairs adds none."""
+    from energy_level_b200 import _lib, batched
+    insts = configs.batch512(count=24, seed=4)
+    lone = {"atoms": [{"id": 0, "pos": [0.0, 0.0, 0.0]}, {"id": 1, "pos": [9.0, 0.0, 0.0]}],
+            "pairs": [], "terms": ["I1"]}
+    insts.append(dict(calib=lone, Om=np.full(2, 2.0), delta=np.zeros(2), edges=None))
+    k = batched.pack_instances(insts)
+    assert [a.dtype for a in k] == [np.int32, np.int32, np.float64, np.float64,
+                                    np.int32, np.int32, np.int32, np.float64]
+    assert k[0].tolist() == [len(i["calib"]["atoms"]) for i in insts]
+    assert k[1].tolist() == [_lib.EL_LAYOUT_CHAIN] * 24 + [_lib.EL_LAYOUT_FULL]
+    assert np.array_equal(k[2], np.concatenate([np.asarray(i["Om"], float) for i in insts]))
+    assert np.array_equal(k[3], np.concatenate([np.asarray(i["delta"], float) for i in insts]))
+    offs, pi, pj, V = [0], [], [], []
+    for inst in insts:
+        for p in inst["calib"]["pairs"]:
+            if p.get("V"):
+                pi.append(p["i"]); pj.append(p["j"]); V.append(p["V"])
+        offs.append(len(V))
+    assert k[4].tolist() == offs and offs[-1] == offs[-2]
+    assert k[5].tolist() == pi and k[6].tolist() == pj and k[7].tolist() == V
+    empty = batched.pack_instances([dict(calib=lone, Om=np.ones(2), delta=np.zeros(2), edges=None)])
+    assert empty[4].tolist() == [0, 0] and empty[5].tolist() == [0] and empty[7].tolist() == [0.0]
+    with pytest.raises(ValueError):
+        batched.pack_instances([dict(calib=lone, Om=np.array([1j, 0]), delta=np.zeros(2), edges=None)])
