@@ -28,8 +28,11 @@ class PulseProblem:
 
     def __init__(self, calib, psi0, target=None, observable=None, plan=None, dtype='complex64',
                  omega_shape=None, delta_shape=None, device='cuda', tol=None):
-        torch = _torch()
         n = len(calib['atoms'])
+        # the reverse recurrence differentiates the Omega/delta/V model: a calib
+        # with J or A channels in use is refused before anything is built
+        model.model_columns(calib, np.zeros(n), np.zeros(n))
+        torch = _torch()
         ctx, basis, ham, _ = model.build(calib, np.zeros(n), np.zeros(n), plan=plan, device=device)
         self.ctx, self.basis, self.ham, self.n = ctx, basis, ham, n
         self.dtype = dtype

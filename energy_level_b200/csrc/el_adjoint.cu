@@ -387,6 +387,8 @@ extern "C" int el_adjoint_pulse(el_ctx *ctx, el_ham *h, int dtype, int K, const 
   if (dtype != EL_C64 && dtype != EL_C128) return fail(ctx, EL_EINVAL, "adjoint needs EL_C64 or EL_C128");
   if (K < 1) return fail(ctx, EL_EINVAL, "K must be >= 1");
   if (h->lossy) return fail(ctx, EL_EINVAL, "the adjoint gradient needs a Hermitian H (gamma = 0)");
+  if (!h->px.empty())
+    return fail(ctx, EL_EINVAL, "the adjoint gradient implements the Omega/delta/V model (no J/A channels)");
   if (!target && !obs_diag) return fail(ctx, EL_EINVAL, "give a target state or a diagonal observable");
   if (!(tol > 0) || tol >= 1) return fail(ctx, EL_EINVAL, "tol must be in (0, 1)");
   for (int k = 0; k < K; ++k)

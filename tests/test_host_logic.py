@@ -224,3 +224,12 @@ def test_pack_instances_matches_calib_pairs():
     assert empty[4].tolist() == [0, 0] and empty[5].tolist() == [0] and empty[7].tolist() == [0.0]
     with pytest.raises(ValueError):
         batched.pack_instances([dict(calib=lone, Om=np.array([1j, 0]), delta=np.zeros(2), edges=None)])
+
+
+def test_pulse_problem_refuses_exchange_channels():
+    """The adjoint differentiates the Omega/delta/V model: J or A in use is a
+    ConfigConflict, raised on the host before any device work."""
+    from energy_level_b200.adjoint import PulseProblem
+    xy = configs.xy_chain(6, seed=2)
+    with pytest.raises(model.ConfigConflict):
+        PulseProblem(dict(xy["calib"], terms=["I1", "I2"]), "g" * 6, target="rgrgrg")
