@@ -71,10 +71,9 @@ def model_columns(calib, Om=None, delta=None, gamma=None, terms=None, exchange=N
         return n, Om, delta, none
 
     def column(key):
-        try:       # real values (the common case) without building Python complex numbers
-            return np.fromiter((p.get(key) or 0.0 for p in raw), dtype=float, count=m).astype(complex)
-        except TypeError:
-            return np.array([p.get(key) or 0.0 for p in raw], dtype=complex)
+        # complex from the start: a float column would drop the imaginary
+        # part of numpy complex scalars with only a warning
+        return np.fromiter((p.get(key) or 0.0 for p in raw), dtype=complex, count=m)
     if terms is None:
         terms = (calib or {}).get('terms')
     if terms is None:

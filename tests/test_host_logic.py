@@ -95,6 +95,14 @@ def test_model_columns_match_active_terms():
         n, _, _, (pi, pj, V) = model.model_columns(c, np.ones(5), np.zeros(5), exchange=[])
         assert repr(list(zip(pi.tolist(), pj.tolist(), V.tolist()))) == repr(got[3])
         assert pi.dtype == np.int32 and V.dtype == np.float64
+    # numpy complex scalars keep their imaginary parts
+    cj = dict(calib, terms=["I1", "I2"], pairs=[dict(p, J=np.complex128(0.5 + 0.25j)) for p in calib["pairs"]])
+    ex = []
+    model.model_columns(cj, np.ones(5), np.zeros(5), exchange=ex)
+    assert ex and all(e[2] == 0.5 + 0.25j for e in ex)
+    with pytest.raises(ValueError):
+        model.model_columns(dict(calib, pairs=[dict(p, V=np.complex128(1 + 1j)) for p in calib["pairs"]]),
+                            np.ones(5), np.zeros(5))
     with pytest.raises(model.ConfigConflict):   # J in use without an exchange list
         model.model_columns(dict(calib, pairs=[dict(p, J=0.5) for p in calib["pairs"]]),
                             np.ones(5), np.zeros(5))
