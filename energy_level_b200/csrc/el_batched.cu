@@ -825,6 +825,11 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
   if (dtype != EL_F32 && dtype != EL_F64) return fail(ctx, EL_EINVAL, "batched Lanczos vectors must be EL_F32 or EL_F64");
   if (max_iter < 2 || max_iter > MAXIT) return fail(ctx, EL_EINVAL, "max_iter must be in [2, %d]", MAXIT);
   if (!(tol > 0) || !std::isfinite(tol)) return fail(ctx, EL_EINVAL, "tol must be positive");
+  for (int i = 0; i < count; ++i)
+    if (pair_off[i] < 0 || pair_off[i + 1] < pair_off[i])
+      return fail(ctx, EL_EINVAL, "pair offsets must be non-negative and non-decreasing (instance %d)", i);
+  if (pair_off[count] > pair_off[0] && (!pi || !pj || !V))
+    return fail(ctx, EL_EINVAL, "pair arrays missing for %d pairs", pair_off[count] - pair_off[0]);
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   std::vector<int64_t> dims(count);
   for (int i = 0; i < count; ++i) {

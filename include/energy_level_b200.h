@@ -219,7 +219,8 @@ typedef struct el_batch el_batch;
  * (<= 40), basis layout layouts[i] (EL_LAYOUT_CHAIN or EL_LAYOUT_RING
  * blockade sectors, or EL_LAYOUT_FULL up to 24 sites), per-site Omega and
  * delta (host, concatenated over instances) and the I1 pairs
- * pi/pj/V[pair_off[i] .. pair_off[i+1]).  Vectors in dtype (EL_F32/EL_F64),
+ * pi/pj/V[pair_off[i] .. pair_off[i+1]) (offsets non-decreasing, else
+ * EL_EINVAL).  Vectors in dtype (EL_F32/EL_F64),
  * alpha/beta and the tridiagonal solve in FP64; at most max_iter (<= 384)
  * Lanczos steps per instance; convergence when the residual estimates of the
  * two lowest Ritz pairs are <= tol * max(1, |theta|).
