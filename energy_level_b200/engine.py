@@ -25,6 +25,8 @@ when dim <= fullpop_max (65536), as the reference does.
 """
 from __future__ import annotations
 
+import bisect
+
 import numpy as np
 
 from . import model, solvers
@@ -77,6 +79,36 @@ def segment_drive(t, segments, n, interp='left'):
         om2, de2 = _segment_arrays(ordered[idx + 1], n)
         om, de = 0.5 * (om + om2), 0.5 * (de + de2)
     return om, de
+
+
+class SegmentTable:
+    """segment_drive over one fixed segment list: the segments are sorted
+    once and each one's arrays built once, so resolving the drive of many
+    intervals costs a bisection each (same values as segment_drive).  The
+    returned arrays are shared: callers copy before changing them."""
+
+    def __init__(self, segments, n):
+        self.ordered = sorted(segments, key=lambda s: float(s['t0']))
+        self.t0 = [float(s['t0']) for s in self.ordered]
+        self.n = n
+        self._arrays = {}
+
+    def _at(self, i):
+        a = self._arrays.get(i)
+        if a is None:
+            a = self._arrays[i] = _segment_arrays(self.ordered[i], self.n)
+        return a
+
+    def drive(self, t, interp='left'):
+        if interp not in ('left', 'midpoint'):
+            raise ValueError('drive_interp 须为 left/midpoint，得到 %r' % (interp,))
+        # the last segment with t0 <= t in t0 order (the first one if none)
+        idx = max(bisect.bisect_right(self.t0, t) - 1, 0)
+        om, de = self._at(idx)
+        if interp == 'midpoint' and idx < len(self.ordered) - 1:
+            om2, de2 = self._at(idx + 1)
+            om, de = 0.5 * (om + om2), 0.5 * (de + de2)
+        return om, de
 
 
 SCHMIDT_MAX_ENTRIES = 1 << 20
@@ -230,11 +262,12 @@ def evolve_manybody(calib, psi0=None, t_grid=None, Om=None, delta=None, gamma=No
     base_de = np.zeros(n) if delta is None else np.asarray(delta, float)
     reduce(0)
     current = None
+    table = SegmentTable(segments, n) if segments else None
     for k in range(1, n_t):
         for a, b in (segment_intervals(t[k - 1], t[k], segments) if segments else [(t[k - 1], t[k])]):
             check_cancel(progress_arr)
             if segments:
-                om, de = segment_drive(0.5 * (a + b), segments, n, interp=drive_interp)
+                om, de = table.drive(0.5 * (a + b), interp=drive_interp)
             else:
                 om, de = base_om, base_de
             key = (tuple(np.round(om, 15)), tuple(np.round(de, 15)))

@@ -241,3 +241,23 @@ def test_pulse_problem_refuses_exchange_channels():
     xy = configs.xy_chain(6, seed=2)
     with pytest.raises(model.ConfigConflict):
         PulseProblem(dict(xy["calib"], terms=["I1", "I2"]), "g" * 6, target="rgrgrg")
+
+
+def test_segment_table_equals_segment_drive():
+    """The evolution loop's pre-sorted segment table returns exactly the
+    drive of segment_drive (runtime.py:90-114) at every time, ties and
+    unsorted t0 included, for both interpolation rules."""
+    rng = np.random.default_rng(11)
+    n = 4
+    t0s = [5.0, 0.0, 2.5, 2.5, 9.0, 7.25]
+    segs = [{"t0": t0, "Om": rng.uniform(0, 3, n), "delta": rng.uniform(-2, 2, n),
+             "phase": rng.uniform(-1, 1, n)} for t0 in t0s]
+    table = engine.SegmentTable(segs, n)
+    times = [-1.0, 0.0, 1.0, 2.5, 3.0, 5.0, 7.25, 8.0, 9.0, 12.0] + list(rng.uniform(-1, 12, 40))
+    for interp in ("left", "midpoint"):
+        for t in times:
+            om, de = engine.segment_drive(t, segs, n, interp=interp)
+            om2, de2 = table.drive(t, interp=interp)
+            assert np.array_equal(om, om2) and np.array_equal(de, de2), (interp, t)
+    with pytest.raises(ValueError):
+        table.drive(1.0, interp="cubic")
