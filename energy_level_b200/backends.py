@@ -104,13 +104,19 @@ def engine_entries():
 def solve_equilibrium(system, want='gs', *, backend='b200-lanczos', betas=None, k=2, v0=None,
                       seed=0, num=400, nvec=200, dtype=None, memory_budget_mb=None,
                       return_state=False, sector=None, progress_arr=None, ramp=None, log=None,
-                      **unused):
-    """eq_route.solve_equilibrium for the b200 names (same result keys)."""
+                      exact=False, **unused):
+    """eq_route.solve_equilibrium for the b200 names (same result keys).
+
+    ``exact=True`` (the dense spectral trace of the CPU kpm / ed routes) is
+    refused for b200-kpm with ValueError, as eq_route.py:446-447 refuses it
+    for gpu-kpm: the moments here are always stochastic (Hutchinson)."""
     from . import kpm as bkpm
     from .matrix_free import b200_lanczos_ground_state
     if progress_arr is not None and float(progress_arr[1]) != 0:
         raise RuntimeError('用户取消')
     backend = normalize_equilibrium_backend(backend, want)
+    if exact and backend == 'b200-kpm':
+        raise ValueError('b200-kpm 不提供 exact 谱迹；请选择 CPU kpm 或 ed')
     system = dict(system)
     plan = system.get('plan') or {}
     for key in ('Om', 'delta', 'gamma', 'terms'):
@@ -343,13 +349,21 @@ def install_into(reference_backends, shim_module='b200_shim'):
     reference resolves time engines as '.manybody.<module>' (backends.py:177),
     so the entry names a shim module in that package that re-exports
     energy_level_b200.engine.evolve_manybody."""
+    import dataclasses
     eq = reference_backends.EQ_BACKENDS
     for name, wants in EQ_BACKENDS.items():
         eq[name] = tuple(wants)
     tb = reference_backends.TIME_BACKENDS
     cls = getattr(reference_backends, 'TimeBackend', TimeBackend)
+    # every capability field the target class declares (pauli, charge, order,
+    # native_state, algorithm, ... in backends.py:22-37), so that its own
+    # validate_time_capabilities sees what this backend implements
+    if dataclasses.is_dataclass(cls):
+        names = [f.name for f in dataclasses.fields(cls)]
+    else:
+        names = [f.name for f in dataclasses.fields(TimeBackend)]
+    ours = {f.name for f in dataclasses.fields(TimeBackend)}
     for name, b in TIME_BACKENDS.items():
-        tb[name] = cls(shim_module, b.function, aliases=b.aliases, options=b.options,
-                       segments=b.segments, projected=b.projected, gamma=b.gamma,
-                       return_state=b.return_state)
+        kw = {k: getattr(b, k) for k in names if k in ours and k not in ('module', 'function')}
+        tb[name] = cls(shim_module, b.function, **kw)
     return reference_backends

@@ -96,6 +96,11 @@ class BatchedGroundStates:
         self.ctx.call('el_batch_run_coop', self.handle, C.c_int(int(reorth_passes)), C.c_int(int(check_every)),
                       C.c_uint64(int(seed)))
 
+    def set_wait_limit(self, polls=1 << 22):
+        """Polls each grid-barrier wait of run_coop makes before the solve
+        gives up with RuntimeError (EL_ECUDA); see el_batch_set_wait_limit."""
+        self.ctx.call('el_batch_set_wait_limit', self.handle, C.c_int32(int(polls)))
+
     def results(self):
         e0 = np.zeros(self.count)
         gap = np.zeros(self.count)

@@ -20,6 +20,37 @@ def _torch():
     return torch
 
 
+def el_dtype(x):
+    """Library dtype code of a torch tensor (EL_F32/F64/C64/C128)."""
+    import torch
+    dt = {torch.float32: _lib.EL_F32, torch.float64: _lib.EL_F64,
+          torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}.get(getattr(x, 'dtype', None))
+    if dt is None:
+        raise ValueError('设备向量须为 float32/float64/complex64/complex128 张量')
+    return dt
+
+
+def check_device_vector(ctx, x, numel, name='psi', complex_only=False):
+    """Refuse, before its address reaches a kernel, any tensor that is not a
+    contiguous CUDA tensor on the context's device holding exactly ``numel``
+    elements of a library dtype; returns its dtype code.  The C ABI carries
+    device addresses without lengths, so this is where a short vector or a
+    host tensor is caught."""
+    import torch
+    if not isinstance(x, torch.Tensor):
+        raise ValueError('%s 须为 torch 张量' % name)
+    dt = el_dtype(x)
+    if complex_only and dt not in (_lib.EL_C64, _lib.EL_C128):
+        raise ValueError('%s must be complex64 or complex128' % name)
+    if x.numel() != int(numel):
+        raise ValueError('%s 元素数 %d ≠ %d（基维度 × 向量数）' % (name, x.numel(), int(numel)))
+    if not x.is_contiguous():
+        raise ValueError('%s must be contiguous' % name)
+    if not x.is_cuda or x.device.index != ctx.device.index:
+        raise ValueError('%s 须在 %s 上（实为 %s）' % (name, ctx.device, x.device))
+    return dt
+
+
 class Context:
     """One library context per (thread, device).  Mirrors the per-run device
     setup of matrix_free.py:177-185."""
@@ -241,13 +272,14 @@ class Hamiltonian:
 
     def hv(self, x):
         """y = H x for x of shape (dim,) or (dim, nvec) on the device."""
-        torch = _torch()
-        x = x.contiguous()
-        dt = {torch.float32: _lib.EL_F32, torch.float64: _lib.EL_F64,
-              torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}[x.dtype]
+        import torch
+        if not isinstance(x, torch.Tensor) or x.dim() not in (1, 2):
+            raise ValueError('x 须为 (dim,) 或 (dim, nvec) 的 torch 张量')
         nvec = 1 if x.dim() == 1 else int(x.shape[1])
         if x.shape[0] != self.dim:
             raise ValueError('通道内核：向量长度 %d ≠ 基维度 %d' % (x.shape[0], self.dim))
+        x = x.contiguous()
+        dt = check_device_vector(self.ctx, x, self.dim * nvec, name='x')
         y = torch.empty_like(x)
         self.ctx.call('el_hv', self.handle, C.c_int(dt), C.c_int(nvec),
                       C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()))

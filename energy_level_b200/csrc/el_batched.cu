@@ -500,6 +500,7 @@ struct CoopArgs {
   double *tot;                  // [2][MAXIT + 2] the sums, each formed by one CTA
   unsigned *bar;                // arrival counter, zero at launch
   int *err;
+  int poll_limit;               // polls per barrier before giving up
   uint64_t seed;
   double *e0, *e1, *res, *gap;
   int *iters, *conv;
@@ -514,7 +515,7 @@ __device__ __forceinline__ void grid_barrier(const CoopArgs &G, unsigned &gen) {
     if (!*(volatile int *)G.err) {
       int polls = 0;
       while (*(volatile unsigned *)G.bar < gen) {
-        if (++polls > (1 << 22)) { atomicExch(G.err, 1); break; }
+        if (++polls > G.poll_limit) { atomicExch(G.err, 1); break; }
         if (*(volatile int *)G.err) break;
         __nanosleep(64);
       }
@@ -793,6 +794,7 @@ struct el_batch_impl {
   int count = 0, dtype = 0, max_iter = 0;
   double tol = 0;
   int64_t total_rows = 0, dim_max = 0;
+  int wait_polls = 1 << 22;         // grid-barrier polls before a timeout (cooperative solver)
   std::vector<int> order;           // processing position -> caller index
   Inst *d_inst = nullptr;
   double *d_diag = nullptr;
@@ -995,10 +997,14 @@ int el_batch_run_coop(el_ctx *ctx, el_batch *b, int reorth_passes, int check_eve
     if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, EL_ENOMEM, "cooperative workspace"); }
     b->c_nctas = nctas_max;
   }
+  // counter and error flag start at zero; between instances only the
+  // counter is reset, so a timeout in any instance stays visible to the host
+  EL_CUDA_TRY(ctx, cudaMemsetAsync(b->c_sync, 0, 2 * sizeof(unsigned), ctx->stream));
   for (int p = 0; p < b->count; ++p) {
     const Plan &P = plans[p];
     CoopArgs G;
     memset(&G, 0, sizeof G);
+    G.poll_limit = b->wait_polls;
     G.p = p; G.m = m; G.nctas = P.nctas; G.check_every = check_every; G.passes = reorth_passes;
     G.tol = b->tol; G.eps = b->dtype == EL_F32 ? 1.19e-7 : 2.22e-16;
     G.inst = b->d_inst; G.diag = b->d_diag; G.vpub = b->c_vpub; G.part = b->c_part;
@@ -1006,7 +1012,7 @@ int el_batch_run_coop(el_ctx *ctx, el_batch *b, int reorth_passes, int check_eve
     G.bar = b->c_sync; G.err = (int *)(b->c_sync + 1); G.seed = seed;
     G.e0 = b->d_out; G.e1 = b->d_out + b->count; G.res = b->d_out + 2 * b->count; G.gap = b->d_out + 3 * b->count;
     G.iters = b->d_iout; G.conv = b->d_iout + b->count;
-    EL_CUDA_TRY(ctx, cudaMemsetAsync(b->c_sync, 0, 2 * sizeof(unsigned), ctx->stream));
+    if (p > 0) EL_CUDA_TRY(ctx, cudaMemsetAsync(b->c_sync, 0, sizeof(unsigned), ctx->stream));
     void *kargs[] = {(void *)&G};
     const void *fn = nullptr;
 #define EL_CPICK(TT)                                                                   \
@@ -1032,6 +1038,13 @@ int el_batch_run_coop(el_ctx *ctx, el_batch *b, int reorth_passes, int check_eve
   EL_CUDA_TRY(ctx, el::copy(ctx, hs, b->c_sync, sizeof hs, cudaMemcpyDeviceToHost));
   EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (hs[1]) return fail(ctx, EL_ECUDA, "cooperative Lanczos: a grid barrier timed out");
+  return EL_OK;
+}
+
+int el_batch_set_wait_limit(el_ctx *ctx, el_batch *b, int32_t polls) {
+  if (!ctx || !b) return EL_EINVAL;
+  if (polls < 0) return fail(ctx, EL_EINVAL, "wait limit must be >= 0 polls");
+  b->wait_polls = polls;
   return EL_OK;
 }
 

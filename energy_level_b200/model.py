@@ -129,7 +129,78 @@ def _is_chain_or_ring(n, edges):
     return es == chain or es == sorted(chain + [(0, n - 1)])
 
 
-def basis_for(ctx: Context, n, plan=None, basis_indices=None, constraint=None, max_states=None):
+_PROJECTING = ('blockade', 'pxp')
+
+
+def resolve_constraint(calib, constraint):
+    """A reference constraint spec -> (projected, edges, spec).
+
+    Same meaning as hamiltonian_plan.py:15-50: the spec is None, a kind
+    string or a dict with kind none/blockade/pxp (default none), mode
+    full/project (default project for blockade and pxp, else full),
+    threshold_mhz >= 0 and edges (an integer pair list, 'auto' or absent).
+    A blockade or pxp spec in project mode restricts the basis to the
+    independent sets of its graph: the explicit edges, else every pair of
+    the calib whose |V| reaches threshold_mhz; with neither, ValueError (no
+    spec ever yields a silently unconstrained basis).  Edges come back as
+    sorted (i < j) pairs without repeats."""
+    spec = {'kind': constraint} if isinstance(constraint, str) else constraint
+    if spec is None:
+        spec = {}
+    if not isinstance(spec, dict):
+        raise ValueError('manybody.constraint 须为 dict 或字符串')
+    kind = str(spec.get('kind', 'none')).lower()
+    if kind not in ('none',) + _PROJECTING:
+        raise ValueError('constraint.kind 只支持 none/blockade/pxp')
+    mode = str(spec.get('mode', 'project' if kind in _PROJECTING else 'full')).lower()
+    if mode not in ('full', 'project'):
+        raise ValueError('constraint.mode 只支持 full/project')
+    thr = float(spec.get('threshold_mhz', 0.0) or 0.0)
+    if not (np.isfinite(thr) and thr >= 0):
+        raise ValueError('constraint.threshold_mhz 必须是有限非负数')
+    given = spec.get('edges')
+    norm = dict(kind=kind, mode=mode, threshold_mhz=thr, edges=given)
+    if not (kind in _PROJECTING and mode == 'project'):
+        return False, [], norm
+    n = len(calib.get('atoms') or [])
+    if given is not None and not isinstance(given, str):
+        edges = set()
+        for e in given:
+            ok = len(e) == 2 and all(not isinstance(v, (bool, np.bool_)) and int(v) == v for v in e)
+            if not ok:
+                raise ValueError('blockade edge 必须是两个整数下标')
+            a, b = int(e[0]), int(e[1])
+            if a == b or min(a, b) < 0 or max(a, b) >= n:
+                raise ValueError('blockade edge 越界或自环：%r' % (e,))
+            edges.add((min(a, b), max(a, b)))
+        return True, [list(e) for e in sorted(edges)], norm
+    if given not in (None, 'auto'):
+        raise ValueError('constraint.edges 只支持 auto 或整数边列表')
+    if thr <= 0:
+        raise ValueError('blockade/PXP project 模式需要 threshold_mhz>0 或显式 edges')
+    pairs = calib.get('pairs') or []
+    strong = {(min(int(p['i']), int(p['j'])), max(int(p['i']), int(p['j'])))
+              for p in pairs if abs(complex(p.get('V', 0.0))) >= thr}
+    return True, [list(e) for e in sorted(strong)], norm
+
+
+def plan_edges(plan, calib=None):
+    """Blockade edges of a projected plan: its own 'blockade_edges' when the
+    plan carries them (build_plan output), else derived from its constraint
+    spec and calib by resolve_constraint."""
+    if plan.get('blockade_edges') is not None:
+        return [list(map(int, e)) for e in plan['blockade_edges']]
+    calib = plan.get('calib', calib)
+    if calib is None or plan.get('constraint') is None:
+        raise ValueError('projected plan 缺少 blockade_edges（也无 constraint + calib 可推导）')
+    projected, edges, _ = resolve_constraint(calib, plan['constraint'])
+    if not projected:
+        raise ValueError('plan 声明 projected，但其 constraint 不投影')
+    return edges
+
+
+def basis_for(ctx: Context, n, plan=None, basis_indices=None, constraint=None, max_states=None,
+              calib=None):
     """Native basis for the reference's basis descriptions.
 
     plan: HamiltonianPlan dict (hamiltonian_plan.py:129-148) -> its blockade
@@ -138,18 +209,19 @@ def basis_for(ctx: Context, n, plan=None, basis_indices=None, constraint=None, m
     basis (checked code by code); returns (Basis, permutation or None) where the
     permutation maps the caller's order to ascending order."""
     if plan is not None and plan.get('projected'):
-        edges = plan.get('blockade_edges') or []
+        edges = plan_edges(plan, calib)
         b = Basis(ctx, n, kind='blockade', edges=edges, max_states=max_states)
         if plan.get('states') is not None and len(plan['states']) != b.dim:
             raise ValueError('plan states do not match its blockade edges')
         return b, None
     if constraint is not None:
-        kind = constraint.get('kind')
-        if kind == 'blockade':
-            return Basis(ctx, n, kind='blockade', edges=constraint.get('edges') or [],
-                         max_states=max_states), None
-        if kind == 'charge':
+        if isinstance(constraint, dict) and constraint.get('kind') == 'charge':
             return Basis(ctx, n, kind='charge', k=int(constraint['k'])), None
+        if calib is None:
+            raise ValueError('a blockade/pxp constraint needs the calib (threshold edges)')
+        projected, edges, _ = resolve_constraint(calib, constraint)
+        if projected:
+            return Basis(ctx, n, kind='blockade', edges=edges, max_states=max_states), None
     if basis_indices is None:
         return Basis(ctx, n, kind='full'), None
     codes = np.asarray(basis_indices, np.int64).reshape(-1)
@@ -203,7 +275,7 @@ def build(calib, Om=None, delta=None, gamma=None, terms=None, plan=None, basis_i
         dev = int(dev.split(':')[1]) if ':' in dev else 0
     ctx = ctx or default_context(int(dev))
     b, perm = basis_for(ctx, n, plan=plan, basis_indices=basis_indices, constraint=constraint,
-                        max_states=max_states)
+                        max_states=max_states, calib=calib)
     h = Hamiltonian(ctx, b, Om, delta, pairs, exchange=exchange)
     if gamma is not None and np.any(np.asarray(gamma, float) != 0):
         h.set_loss(gamma)

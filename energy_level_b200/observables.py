@@ -67,64 +67,71 @@ def normalize_pauli_strings(spec, n_atoms=None, err=None):
     return out
 
 
+_NO_PHASE = 1e-14   # a bond amplitude at or below this has no defined phase
+
+
+def _closed_loop(loop, n_sites=None):
+    """Sites of a loop given without its closing repeat, and the site each
+    one links to (the next, the last back to the first)."""
+    q = np.asarray([int(x) for x in loop], dtype=np.int64)
+    if q.size < 2 or (n_sites is not None and (q.min() < 0 or q.max() >= n_sites)):
+        raise ValueError('loop 必须包含至少两个合法原子下标')
+    return q, np.roll(q, -1)
+
+
+def _phase_sum(z):
+    """z[..., e]: the complex amplitudes of a loop's directed bonds.  Returns
+    (sum_e arg z, that sum / 2 pi) over the last axis, NaN wherever a bond has
+    no defined phase (the gauge-invariant flux of observables.py:206-231)."""
+    z = np.asarray(z, complex)
+    defined = np.all(np.abs(z) > _NO_PHASE, axis=-1)
+    flux = np.where(defined, np.angle(z).sum(axis=-1), np.nan)
+    return flux, flux / (2.0 * np.pi)
+
+
 def loop_observables(xy_corr, loops):
-    """Phase sum arg<sigma+_a sigma-_b> around each loop (closing edge added)
-    and its winding (sum / 2 pi); NaN when an edge amplitude vanishes."""
+    """Flux arg<sigma+_a sigma-_b> summed around each loop of sites and its
+    winding (flux / 2 pi), from one <sigma+ sigma-> matrix; NaN for a loop
+    with a vanishing bond.  Returns two lists (one entry per loop)."""
     if loops is None:
         return [], []
     xy = np.asarray(xy_corr, complex)
-    phases, wind = [], []
+    flux, wind = [], []
     for loop in loops:
-        q = [int(x) for x in loop]
-        if len(q) < 2 or any(x < 0 or x >= xy.shape[0] for x in q):
-            raise ValueError('loop 必须包含至少两个合法原子下标')
-        vals = []
-        for a, b in zip(q, q[1:] + q[:1]):
-            z = xy[a, b]
-            vals.append(float(np.angle(z)) if abs(z) > 1e-14 else np.nan)
-        total = float(np.sum(vals)) if np.all(np.isfinite(vals)) else np.nan
-        phases.append(total)
-        wind.append(float(total / (2.0 * np.pi)) if np.isfinite(total) else np.nan)
-    return phases, wind
+        a, b = _closed_loop(loop, xy.shape[0])
+        f, w = _phase_sum(xy[a, b])
+        flux.append(float(f))
+        wind.append(float(w))
+    return flux, wind
 
 
 def link_loop_observables(link_corr, link_pairs, loops):
-    """Loop phase / winding time series from the selected links (either
-    orientation; the reverse one is the complex conjugate)."""
+    """The same flux and winding as time series, from the selected links only:
+    link_corr[t, q] = <sigma+_a sigma-_b> for link_pairs[q] = (a, b).  A bond
+    of a loop is the first link joining its two sites, read conjugated when
+    the link runs the other way; a loop with a bond no link covers stays NaN
+    (observables.py:234-278 semantics).  Returns (flux, winding), each of
+    shape (times, loops)."""
     if loops is None:
         return np.empty((0, 0), float), np.empty((0, 0), float)
-    lookup = {}
-    for q, (a, b) in enumerate([(int(a), int(b)) for a, b in (link_pairs or [])]):
-        lookup.setdefault((a, b), []).append((q, 1))
-        lookup.setdefault((b, a), []).append((q, -1))
-    arr = np.asarray(link_corr, complex)
-    if arr.ndim == 1:
-        arr = arr[None, :]
-    phase = np.full((arr.shape[0], len(loops)), np.nan, float)
-    winding = np.full_like(phase, np.nan)
-    for ell, raw in enumerate(loops):
-        loop = [int(x) for x in raw]
-        if len(loop) < 2:
-            raise ValueError('loop 必须包含至少两个合法原子下标')
-        cols = []
-        for a, b in zip(loop, loop[1:] + loop[:1]):
-            choice = lookup.get((a, b))
-            if not choice:
-                cols = None
-                break
-            cols.append(choice[0])
-        if cols is None:
+    links = np.asarray([(int(a), int(b)) for a, b in (link_pairs or [])], dtype=np.int64).reshape(-1, 2)
+    series = np.asarray(link_corr, complex)
+    series = series[None, :] if series.ndim == 1 else series
+    flux = np.full((series.shape[0], len(loops)), np.nan)
+    wind = np.full_like(flux, np.nan)
+    for ell, loop in enumerate(loops):
+        a, b = _closed_loop(loop)
+        fwd = (links[:, None, 0] == a) & (links[:, None, 1] == b)      # [link, bond]
+        rev = (links[:, None, 0] == b) & (links[:, None, 1] == a)
+        hit = fwd | rev
+        if not hit.any(axis=0).all():
             continue
-        vals = np.zeros((arr.shape[0], len(cols)))
-        valid = np.ones(arr.shape[0], bool)
-        for j, (q, sign) in enumerate(cols):
-            z = arr[:, q] if sign > 0 else np.conj(arr[:, q])
-            valid &= np.abs(z) > 1e-14
-            vals[:, j] = np.angle(z)
-        total = vals.sum(axis=1)
-        phase[valid, ell] = total[valid]
-        winding[valid, ell] = total[valid] / (2.0 * np.pi)
-    return phase, winding
+        col = np.argmax(hit, axis=0)                                   # first link per bond
+        z = series[:, col]
+        flip = ~fwd[col, np.arange(col.size)]
+        z[:, flip] = np.conj(z[:, flip])
+        flux[:, ell], wind[:, ell] = _phase_sum(z)
+    return flux, wind
 
 
 def product_label(n, s):

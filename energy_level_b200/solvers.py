@@ -9,7 +9,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from .core import Hamiltonian, _torch
+from .core import Hamiltonian, _torch, check_device_vector
 
 _TORCH_DT = {"float32": "float32", "float64": "float64", "complex64": "complex64",
              "complex128": "complex128"}
@@ -84,6 +84,7 @@ def lanczos_ground(ham: Hamiltonian, dtype="float64", v0=None, seed=0, max_iter=
         v0t = torch.as_tensor(v0, dtype=td, device=ham.ctx.device).contiguous()
         if v0t.numel() != ham.dim:
             raise ValueError('v0 length must equal the basis dimension')
+        check_device_vector(ham.ctx, v0t, ham.dim, name='v0')
         v0p = C.c_void_p(v0t.data_ptr())
     vec = torch.empty(ham.dim, dtype=td, device=ham.ctx.device) if return_vec else None
     ham.ctx.call('el_lanczos_ground', ham.handle, C.c_int(_lib.DTYPES[dtype]), v0p,
@@ -100,12 +101,7 @@ def lanczos_ground(ham: Hamiltonian, dtype="float64", v0=None, seed=0, max_iter=
 
 def cheb_step(ham: Hamiltonian, psi, tau_ns, tol=1e-12):
     """psi <- exp(-i CONV H tau) psi in place (complex64/complex128 tensor)."""
-    torch = _torch()
-    dt = {torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}.get(psi.dtype)
-    if dt is None:
-        raise ValueError('psi must be complex64 or complex128')
-    if not psi.is_contiguous():
-        raise ValueError('psi must be contiguous')
+    dt = check_device_vector(ham.ctx, psi, ham.dim, complex_only=True)
     nt = C.c_int()
     ham.ctx.call('el_cheb_step', ham.handle, C.c_int(dt), C.c_void_p(psi.data_ptr()),
                  C.c_double(float(tau_ns)), C.c_double(float(tol)), C.byref(nt))
@@ -114,12 +110,11 @@ def cheb_step(ham: Hamiltonian, psi, tau_ns, tol=1e-12):
 
 def observables(ham: Hamiltonian, psi):
     """(<n_i> per site, squared norm) of a device state."""
-    torch = _torch()
-    dt = {torch.float32: _lib.EL_F32, torch.float64: _lib.EL_F64,
-          torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}[psi.dtype]
+    psi_c = psi.contiguous() if hasattr(psi, 'contiguous') else psi   # kept alive across the call
+    dt = check_device_vector(ham.ctx, psi_c, ham.dim)
     ns = np.zeros(ham.n)
     nrm = C.c_double()
-    ham.ctx.call('el_observables', ham.handle, C.c_int(dt), C.c_void_p(psi.contiguous().data_ptr()),
+    ham.ctx.call('el_observables', ham.handle, C.c_int(dt), C.c_void_p(psi_c.data_ptr()),
                  _lib.dptr(ns), C.byref(nrm))
     return ns, float(nrm.value)
 
@@ -127,12 +122,7 @@ def observables(ham: Hamiltonian, psi):
 def taylor_step(ham: Hamiltonian, psi, tau_ns, tol=1e-13):
     """psi <- exp(-i CONV H tau) psi for any H (loss diagonal included):
     scaled Taylor polynomial (el_taylor_step); returns the H applications."""
-    torch = _torch()
-    dt = {torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}.get(psi.dtype)
-    if dt is None:
-        raise ValueError('psi must be complex64 or complex128')
-    if not psi.is_contiguous():
-        raise ValueError('psi must be contiguous')
+    dt = check_device_vector(ham.ctx, psi, ham.dim, complex_only=True)
     nt = C.c_int()
     ham.ctx.call('el_taylor_step', ham.handle, C.c_int(dt), C.c_void_p(psi.data_ptr()), C.c_double(float(tau_ns)),
                  C.c_double(float(tol)), C.byref(nt))
@@ -145,10 +135,8 @@ def spin_observables(ham: Hamiltonian, psi, pairs=()):
     Returns dict(n, norm, sm, nn, xy): <n_i>, squared norm, <sigma-_i>
     (complex) per site, and for each (i, j) of ``pairs`` <n_i n_j> and
     <sigma+_i sigma-_j> (complex)."""
-    torch = _torch()
-    dt = {torch.float32: _lib.EL_F32, torch.float64: _lib.EL_F64,
-          torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}[psi.dtype]
-    psi = psi.contiguous()
+    psi = psi.contiguous() if hasattr(psi, 'contiguous') else psi
+    dt = check_device_vector(ham.ctx, psi, ham.dim)
     n = ham.n
     pr = np.asarray(list(pairs), dtype=np.int32).reshape(-1, 2)
     pi = np.ascontiguousarray(pr[:, 0])
@@ -171,13 +159,11 @@ def pauli_expect(ham: Hamiltonian, psi, specs):
     """<psi|P|psi> (complex) of each Pauli string in ``specs``
     ([{'label', 'terms': [(site, axis), ...]}], axes 'x'/'y'/'z'), on the device
     (el_pauli_expect)."""
-    torch = _torch()
-    dt = {torch.float32: _lib.EL_F32, torch.float64: _lib.EL_F64,
-          torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}[psi.dtype]
+    psi = psi.contiguous() if hasattr(psi, 'contiguous') else psi
+    dt = check_device_vector(ham.ctx, psi, ham.dim)
     specs = list(specs or [])
     if not specs:
         return np.zeros(0, complex)
-    psi = psi.contiguous()
     offs, sites, axes = [0], [], []
     for sp in specs:
         for site, ax in sp['terms']:
@@ -197,11 +183,7 @@ def observables_noalloc(ham: Hamiltonian, psi):
     """observables() through el_observables_noalloc: no device allocation,
     static scratch shared per device (at most 40 sites; calls on one device
     must not overlap in time)."""
-    torch = _torch()
-    dt = {torch.float32: _lib.EL_F32, torch.float64: _lib.EL_F64,
-          torch.complex64: _lib.EL_C64, torch.complex128: _lib.EL_C128}[psi.dtype]
-    if not psi.is_contiguous():
-        raise ValueError('psi must be contiguous (no copy is made)')
+    dt = check_device_vector(ham.ctx, psi, ham.dim)   # contiguous: no copy is made
     ns = np.zeros(ham.n)
     nrm = C.c_double()
     ham.ctx.call('el_observables_noalloc', ham.handle, C.c_int(dt), C.c_void_p(psi.data_ptr()),

@@ -7,9 +7,10 @@ phi (typically O|0>), as in the reference's spectrum.py:
   three-term recurrence, FP64 alpha/beta, full reorthogonalisation twice per
   step) and returns the keys of spectrum.py:34-103 (alphas, betas, norm2, n,
   converged, ortho_loss, reortho, note, seconds);
-- ``quadrature`` and ``lorentz_spectrum`` are the host post-processing of
-  spectrum.py:106-135 (Ritz nodes / weights sum to |phi|^2, continued
-  fraction);
+- ``quadrature`` and ``lorentz_spectrum`` give the outputs of the host
+  post-processing of spectrum.py:106-135: Gauss nodes / weights of phi's
+  spectral measure (summing to |phi|^2) from a tridiagonal eigensolver, and
+  the broadened spectrum as a Lorentzian sum over those nodes;
 - ``source_spectrum`` is spectrum.py:138-180 with the same result dict;
 - ``resolve_source`` builds phi from a ``system['source']`` mapping as
   eq_route.py:160-257 does (vector, psi0/state, diagonal, site_weights with
@@ -88,68 +89,76 @@ def lanczos(ham, phi, n_krylov=200, *, reortho=True, memory_budget_mb=512.0, dty
 
 
 def quadrature(alphas, betas, norm2, shift=0.0):
-    """Ritz nodes (relative to shift) and weights norm2 |u_0|^2 (spectrum.py:106-121)."""
-    alphas = np.asarray(alphas, float)
-    betas = np.asarray(betas, float)
-    if alphas.size == 0:
+    """Gauss quadrature of phi's spectral measure (Golub-Welsch): nodes are
+    the eigenvalues of the Jacobi matrix J = tridiag(betas, alphas, betas)
+    less ``shift``; weights are norm2 times the squared first components of
+    J's unit eigenvectors, so they sum to |phi|^2 (the outputs of
+    spectrum.py:106-121).  J is handed to a symmetric tridiagonal solver
+    (LAPACK stemr through scipy) and never formed as a dense matrix."""
+    from scipy.linalg import eigh_tridiagonal
+    a = np.asarray(alphas, float).reshape(-1)
+    if a.size == 0:
         return np.zeros(0), np.zeros(0)
-    if betas.size:
-        evals, evecs = np.linalg.eigh(np.diag(alphas) + np.diag(betas, 1) + np.diag(betas, -1))
-    else:
-        evals, evecs = alphas.copy(), np.ones((1, 1))
-    weights = float(norm2) * np.abs(evecs[0, :]) ** 2
-    return evals - float(shift), weights
+    b = np.asarray(betas, float).reshape(-1)[:a.size - 1]
+    if a.size == 1:
+        return a - float(shift), np.array([float(norm2)])
+    lam, u = eigh_tridiagonal(a, b)
+    return lam - float(shift), float(norm2) * u[0] ** 2
 
 
 def lorentz_spectrum(alphas, betas, norm2, omega, eta, shift=0.0):
-    """Continued fraction for -1/pi Im <phi|(w + shift + i eta - H)^{-1}|phi>
-    (spectrum.py:124-135)."""
-    alphas = np.asarray(alphas, float)
-    betas = np.asarray(betas, float)
+    """S(w) = -1/pi Im <phi|(w + shift + i eta - H)^{-1}|phi> in the Krylov
+    model (spectrum.py:124-135).  The (0,0) element of J's resolvent is the
+    Stieltjes transform of the quadrature measure, sum_k w_k / (z - x_k), so
+    S is a sum of Lorentzians of half-width eta centred on the Ritz nodes --
+    the value of the continued fraction, evaluated here from the eigen-
+    decomposition in blocks of frequencies."""
     omega = np.asarray(omega, float)
-    if alphas.size == 0:
-        return np.zeros_like(omega)
-    z = omega + float(shift) + 1j * float(eta)
-    g = z - alphas[-1]
-    for j in range(alphas.size - 2, -1, -1):
-        g = z - alphas[j] - (betas[j] ** 2) / g
-    return -float(norm2) * np.imag(1.0 / g) / np.pi
+    x, w = quadrature(alphas, betas, norm2, shift)
+    eta = float(eta)
+    out = np.zeros(omega.size)
+    if x.size == 0 or eta == 0.0:
+        return out.reshape(omega.shape)
+    flat = omega.reshape(-1)
+    scale = w * (eta / np.pi)
+    for lo in range(0, flat.size, 4096):
+        d = flat[lo:lo + 4096, None] - x[None, :]
+        out[lo:lo + 4096] = (scale / (d * d + eta * eta)).sum(axis=1)
+    return out.reshape(omega.shape)
+
+
+def _display_window(nodes, eta, lo, hi):
+    """Frequency window: any bound the caller gave, else the Ritz nodes' span
+    widened on each side by the larger of 5 % of the span and four
+    half-widths (the default grid of spectrum.py:155-162, so that a default
+    call lands on the same frequencies)."""
+    first, last = (float(nodes.min()), float(nodes.max())) if nodes.size else (0.0, 1.0)
+    margin = max(0.05 * (last - first), 4.0 * float(eta))
+    return (first - margin if lo is None else float(lo)), (last + margin if hi is None else float(hi))
 
 
 def source_spectrum(ham, phi, *, shift=0.0, eta=0.05, n_krylov=None, omega_min=None, omega_max=None,
                     n_omega=800, reortho=True, memory_budget_mb=512.0, dtype=None):
-    """Lanczos -> quadrature + broadened spectrum + diagnostics
-    (spectrum.py:138-180, same result dict)."""
-    k = int(n_krylov) if n_krylov else min(ham.dim, 200)
-    lz = lanczos(ham, phi, k, reortho=reortho, memory_budget_mb=memory_budget_mb, dtype=dtype)
-    nodes, weights = quadrature(lz['alphas'], lz['betas'], lz['norm2'], shift)
-    if omega_min is None or omega_max is None:
-        if nodes.size:
-            lo, hi = float(nodes.min()), float(nodes.max())
-        else:
-            lo, hi = 0.0, 1.0
-        pad = max(0.05 * (hi - lo), 4.0 * float(eta))
-        omega_min = lo - pad if omega_min is None else float(omega_min)
-        omega_max = hi + pad if omega_max is None else float(omega_max)
-    omega = np.linspace(float(omega_min), float(omega_max), int(n_omega))
-    eta = float(eta)
-    spectral = lorentz_spectrum(lz['alphas'], lz['betas'], lz['norm2'], omega, eta, shift)
-    integral = float(np.trapezoid(spectral, omega)) if omega.size > 1 else 0.0
-    return {
-        'omega': omega, 'spectral': spectral,
-        'evals': nodes, 'spectrum_weights': weights,
-        'source_norm': float(lz['norm2']), 'eta': eta, 'shift': float(shift),
-        'krylov': {'n': lz['n'], 'n_requested': k, 'converged': lz['converged'],
-                   'ortho_loss': lz['ortho_loss'], 'reortho': lz['reortho'],
-                   'note': lz['note'], 'seconds': lz['seconds']},
-        'error_report': {'source_norm': float(lz['norm2']),
-                         'spectral_integral': integral,
-                         'integral_ratio': (integral / lz['norm2']) if lz['norm2'] else None,
-                         'eta_mhz': eta,
-                         'krylov_n': lz['n'],
-                         'ortho_loss': lz['ortho_loss'],
-                         'reortho': lz['reortho']},
-    }
+    """Device Lanczos from phi, then the quadrature, the broadened spectrum on
+    a frequency grid and diagnostics; result keys of spectrum.py:138-180
+    (omega, spectral, evals, spectrum_weights, source_norm, eta, shift,
+    krylov, error_report)."""
+    requested = int(n_krylov) if n_krylov else min(ham.dim, 200)
+    lz = lanczos(ham, phi, requested, reortho=reortho, memory_budget_mb=memory_budget_mb, dtype=dtype)
+    norm2, eta = float(lz['norm2']), float(eta)
+    nodes, weights = quadrature(lz['alphas'], lz['betas'], norm2, shift)
+    grid = np.linspace(*_display_window(nodes, eta, omega_min, omega_max), int(n_omega))
+    spectral = lorentz_spectrum(lz['alphas'], lz['betas'], norm2, grid, eta, shift)
+    # the broadened weight inside the window (trapezoid rule); close to
+    # |phi|^2 when the window holds the spectrum
+    inside = 0.5 * float(np.sum((spectral[1:] + spectral[:-1]) * np.diff(grid))) if grid.size > 1 else 0.0
+    health = {key: lz[key] for key in ('ortho_loss', 'reortho')}
+    krylov = dict(health, n=lz['n'], n_requested=requested, converged=lz['converged'], note=lz['note'],
+                  seconds=lz['seconds'])
+    report = dict(health, source_norm=norm2, spectral_integral=inside,
+                  integral_ratio=inside / norm2 if norm2 else None, eta_mhz=eta, krylov_n=lz['n'])
+    return dict(omega=grid, spectral=spectral, evals=nodes, spectrum_weights=weights, source_norm=norm2,
+                eta=eta, shift=float(shift), krylov=krylov, error_report=report)
 
 
 def resolve_source(source, psi0, n_sites, codes=None):

@@ -247,6 +247,15 @@ int el_batch_run(el_ctx *ctx, el_batch *batch, int threads, int ctas_per_sm, uin
  * last).  Same results layout as el_batch_run (read with el_batch_results). */
 int el_batch_run_coop(el_ctx *ctx, el_batch *batch, int reorth_passes, int check_every,
                       uint64_t seed);
+/* Bound of every grid-barrier wait of el_batch_run_coop, in polls of the
+ * arrival counter (about 64 ns apart; default 4,194,304).  When a wait runs
+ * out, that CTA stops waiting, sets the batch's error flag, every later
+ * barrier and step of the launch is skipped, and el_batch_run_coop returns
+ * EL_ECUDA ("a grid barrier timed out") with the flag of every instance
+ * kept; the context stays usable.  A small bound makes a slow or shared GPU
+ * report a stall early.  No counterpart in the reference (its CPU solvers
+ * have no device waits). */
+int el_batch_set_wait_limit(el_ctx *ctx, el_batch *batch, int32_t polls);
 /* Copy results (caller order): ground energy, gap E1 - E0, max residual
  * estimate, Lanczos steps, converged flag.  Synchronises the stream. */
 int el_batch_results(el_ctx *ctx, el_batch *batch, double *e0, double *gap, double *residual,

@@ -8,6 +8,24 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 
+# A checkout of the reference project (read only).  CPU tests that load its
+# modules skip when it is absent (e.g. on a GPU host).
+REFERENCE_ROOT = os.environ.get("EL_REFERENCE_ROOT", "/root/reference")
+
+
+def reference_module(relpath, name):
+    """Load one module file of the reference checkout under a private name (a
+    fresh module object, so a test may modify it), or skip."""
+    import importlib.util
+    path = os.path.join(REFERENCE_ROOT, relpath)
+    if not os.path.exists(path):
+        pytest.skip("reference checkout not present")
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
 

@@ -480,8 +480,55 @@ def loss_fixture(ref_root: str) -> None:
     print("loss fixture written to", HERE)
 
 
+def constraint_fixture(ref_root: str) -> None:
+    """Plans from constraint specs (hamiltonian_plan.py:15-50 _constraint_dict
+    / _edges, build_plan :53-72) on a 3x4 square lattice (a = 6 um, C6/r^6
+    pairs): blockade and pxp in project mode with edges from |V| >=
+    threshold_mhz (nearest and diagonal neighbours at 2 MHz: a general graph,
+    not a chain or ring; nearest neighbours only at 10 MHz), 'auto' edges and
+    mode='full'; each with the reference's ground state on its plan
+    (equilibrium.ground_state on compile_sparse, dense eigh), and the
+    refusal of a projecting spec with neither edges nor a threshold."""
+    import json
+    sys.path.insert(0, ref_root)
+    from src.core.manybody import equilibrium as req
+    from src.core.manybody import hamiltonian_plan as rplan
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from energy_level_b200 import configs
+    pos = [[6.0 * m, 6.0 * k, 0.0] for m in range(3) for k in range(4)]
+    n = len(pos)
+    calib = configs.calib_from_positions(pos)
+    rng = np.random.default_rng(11)
+    om = rng.uniform(1.0, 2.5, n)
+    de = rng.uniform(-2.0, 2.0, n)
+    specs = {"blockade_thr": {"kind": "blockade", "threshold_mhz": 2.0},
+             "pxp_auto": {"kind": "pxp", "edges": "auto", "threshold_mhz": 2.0},
+             "blockade_nn": {"kind": "blockade", "threshold_mhz": 10.0},
+             "blockade_full": {"kind": "blockade", "mode": "full", "threshold_mhz": 2.0}}
+    out = dict(pos=np.asarray(pos), om=om, de=de, names=np.asarray(list(specs)))
+    for name, spec in specs.items():
+        plan = rplan.build_plan(calib, Om=om, delta=de, terms=["I1"], constraint=spec)
+        gs = req.ground_state(rplan.compile_sparse(plan), dense_max=1 << 13, k=2)
+        out[name + "_spec"] = np.asarray(json.dumps(spec))
+        out[name + "_projected"] = np.asarray(bool(plan["projected"]))
+        out[name + "_edges"] = np.asarray(plan["blockade_edges"], np.int64).reshape(-1, 2)
+        out[name + "_dim"] = np.int64(plan["dim"])
+        out[name + "_states"] = np.asarray(plan["states"] if plan["states"] is not None else [], np.int64)
+        out[name + "_E0"] = np.float64(gs["E0"])
+        out[name + "_gap"] = np.float64(gs["gap"])
+    try:
+        rplan.build_plan(calib, Om=om, delta=de, terms=["I1"], constraint={"kind": "blockade"})
+        out["refusal"] = np.asarray("")
+    except ValueError as e:
+        out["refusal"] = np.asarray(str(e))
+    np.savez_compressed(os.path.join(HERE, "constraint.npz"), **out)
+    print("constraint fixture written to", HERE)
+
+
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <reference checkout> [all|spectrum|ramp|exchange|observables|loss|constraint]")
+    root = sys.argv[1]
     which = sys.argv[2] if len(sys.argv) > 2 else "all"
     if which == "spectrum":
         spectrum_fixture(root)
@@ -493,6 +540,8 @@ if __name__ == "__main__":
         observables_fixture(root)
     elif which == "loss":
         loss_fixture(root)
+    elif which == "constraint":
+        constraint_fixture(root)
     else:
         main(root)
         spectrum_fixture(root)
@@ -500,3 +549,4 @@ if __name__ == "__main__":
         exchange_fixture(root)
         observables_fixture(root)
         loss_fixture(root)
+        constraint_fixture(root)

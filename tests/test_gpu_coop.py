@@ -84,3 +84,30 @@ def test_coop_check_interval_and_passes_agree(ctx):
         r = b.results()
         assert r["converged"][0] and abs(r["E0"][0] - C1_E0) < 1e-9, (ce, ps)
     b.close()
+
+
+def test_coop_barrier_timeout_is_reported_and_the_context_recovers(ctx):
+    """A grid-barrier wait bounded at zero polls runs out in the first of two
+    instances: el_batch_run_coop returns EL_ECUDA (RuntimeError, 'grid
+    barrier timed out') instead of hanging or returning stale energies, and
+    with the default bound restored the same batch solves normally on the
+    same context.  No asynchronous copy is in flight in this kernel, so a
+    CTA that stops waiting leaves nothing behind."""
+    from energy_level_b200.batched import BatchedGroundStates
+    cfg = configs.chain12()
+    n = 10
+    calib = configs.calib_from_positions(configs.chain_positions(n))
+    inst = [dict(calib=cfg["calib"], Om=cfg["Om"], delta=cfg["delta"], edges=None),
+            dict(calib=calib, Om=np.full(n, 2.0), delta=np.full(n, -1.0), edges=None)]
+    b = BatchedGroundStates(inst, dtype="float64", max_iter=300, tol=1e-10)
+    b.set_wait_limit(0)
+    with pytest.raises(RuntimeError, match="grid barrier timed out"):
+        b.run_coop()
+    b.set_wait_limit()
+    b.run_coop()
+    r = b.results()
+    assert r["converged"].all()
+    assert abs(r["E0"][0] - C1_E0) < 1e-9
+    with pytest.raises(ValueError):
+        b.set_wait_limit(-1)
+    b.close()

@@ -162,3 +162,45 @@ def test_tma_kpm_matches_generic_kernel(ctx, n, dtype, tol):
         want = ob.kpm_full(n, om, ob.diag_full(n, de, pairs), c, r, num, z[:2])
         got2 = solvers.kpm_moments(h, num, 2, c, r, dtype="float64", chunk=2, probes=z[:2])
         assert np.abs(got2 - want).max() < 1e-10
+
+
+def headline_probe_block(n, distinct=4, block=32, seed=2):
+    """The benchmark's probe block with the C oracle's probes in it: `distinct`
+    counter-based probes, repeated to fill a block of `block` with the sign
+    flipped on every second repetition.  A moment is quadratic in its probe,
+    so the block mean equals the mean over the distinct probes, while each
+    probe group of the pass holds data of its own (a mix-up of groups changes
+    the result)."""
+    from energy_level_b200.probes import rademacher_host
+    z = rademacher_host(seed=seed, probe0=0, nvec=distinct, dim=1 << n)
+    reps = block // distinct
+    zz = np.empty((block, 1 << n), dtype=np.int8)
+    for k in range(reps):
+        zz[k * distinct:(k + 1) * distinct] = z if k % 2 == 0 else -z
+    return z, zz
+
+
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-10), ("float32", 2e-4)])
+def test_tma_kpm_benchmark_shape_matches_oracle(ctx, dtype, tol):
+    """The benchmark's exact shape -- 5x5 lattice (N = 25, full 2^25 basis),
+    one block of 32 probes (chunk 32), doubling recurrence, TMA pass kernel --
+    against the C oracle's direct recurrence (kpm.py:26-75 / 115-151) on the
+    same probes, 24 moments."""
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import solvers
+    from oracle import build as ob
+    cfg = configs.square25()
+    n = cfg["n"]
+    pairs = [(p["i"], p["j"], p["V"]) for p in cfg["calib"]["pairs"]]
+    d = ob.diag_full(n, cfg["delta"], pairs)
+    half = 0.5 * float(np.sum(np.abs(cfg["Om"])))
+    lo, hi = float(d.min()) - half, float(d.max()) + half   # a rigorous spectral interval
+    c, r = solvers.kpm_scale(lo, hi)
+    num = 24
+    z, zz = headline_probe_block(n)
+    want = ob.kpm_full(n, cfg["Om"], d, c, r, num, z)
+    b = Basis(ctx, n, kind="full")
+    h = Hamiltonian(ctx, b, cfg["Om"], cfg["delta"], pairs)
+    got = solvers.kpm_moments(h, num, 32, c, r, dtype=dtype, chunk=32, probes=zz, mode="doubling")
+    assert abs(got[0] - 1.0) < 1e-12
+    assert np.abs(got - want).max() < tol

@@ -83,3 +83,29 @@ def test_one_state_sectors(ctx):
         r = solvers.lanczos_ground(h, dtype="float64", tol=1e-12, nev=2, max_iter=10)
         d = ref.diagonal(n, ref.number_sector_basis(n, k), xy["delta"], pairs)[0]
         assert r["converged"] and abs(r["evals"][0] - d) < 1e-12
+
+
+def test_constraint_plans_match_reference_ground_states(ctx):
+    """Bases and ground states of plans given only as constraint specs
+    (threshold edges on a 3x4 lattice: a general blockade graph in the table
+    layout; 'auto' pxp; mode='full') against the reference's build_plan
+    states and ground_state energies."""
+    import json
+    import os
+    from energy_level_b200 import model, solvers
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "constraint.npz"))
+    calib = configs.calib_from_positions(g["pos"])
+    for nm in g["names"]:
+        nm = str(nm)
+        spec = json.loads(str(g[nm + "_spec"]))
+        projected = bool(g[nm + "_projected"])
+        plan = {"projected": projected, "constraint": spec, "calib": calib}
+        _, basis, ham, _ = model.build(calib, g["om"], g["de"], plan=plan if projected else None,
+                                       constraint=spec)
+        assert basis.dim == int(g[nm + "_dim"]), nm
+        if projected:
+            assert np.array_equal(basis.codes().cpu().numpy(), g[nm + "_states"]), nm
+        r = solvers.lanczos_ground(ham, dtype="float64", tol=1e-12, nev=2, max_iter=min(400, basis.dim))
+        assert r["converged"], nm
+        assert abs(r["evals"][0] - float(g[nm + "_E0"])) < 1e-9, nm
+        assert abs((r["evals"][1] - r["evals"][0]) - float(g[nm + "_gap"])) < 1e-7, nm

@@ -59,6 +59,44 @@ def test_install_into_reference_shaped_module():
     assert fake.TIME_BACKENDS["b200-cheb"].projected
 
 
+def test_install_into_the_reference_backends_module():
+    """install_into on the reference's own backends.py (a fresh copy of the
+    module), then the reference's validate_time_capabilities for b200-cheb:
+    Pauli strings, drive segments, a projected plan, loss rates and
+    return_state pass; a real-time charge sector is refused as for ed."""
+    from conftest import reference_module
+    rb = reference_module("src/core/manybody/backends.py", "_el_ref_backends")
+    backends.install_into(rb)
+    tb = rb.TIME_BACKENDS["b200-cheb"]
+    assert isinstance(tb, rb.TimeBackend)
+    ours = backends.TIME_BACKENDS["b200-cheb"]
+    for f in ("segments", "projected", "gamma", "return_state", "charge", "order", "pauli",
+              "native_state", "algorithm", "aliases", "options"):
+        assert getattr(tb, f) == getattr(ours, f), f
+    assert rb.normalize_time_backend("chebyshev-gpu") == "b200-cheb"
+    assert "b200-cheb" in rb.pauli_backends()
+    assert rb.normalize_equilibrium_backend("b200-kpm", "dos") == "b200-kpm"
+    assert rb.normalize_equilibrium_backend("b200-lanczos", "spectrum") == "b200-lanczos"
+    rb.validate_time_capabilities("b200-cheb", pauli_strings=[{"label": "zz", "terms": [(0, "z")]}],
+                                  segments=[{"t0": 0.0}], plan={"projected": True},
+                                  gamma=[0.1, 0.0], return_state=True, psi0="gggg")
+    with pytest.raises(rb.ConfigConflict) as e:
+        rb.validate_time_capabilities("b200-cheb", charge_sector=2)
+    assert e.value.keys == ("manybody.charge_sector",)
+    entries = rb.engine_entries()
+    assert entries[("b200-cheb", "many")] == (".manybody.b200_shim", "evolve_manybody")
+
+
+def test_b200_kpm_refuses_exact_trace():
+    """exact=True asks for the dense spectral trace; b200-kpm refuses it
+    before any work, like gpu-kpm (eq_route.py:446-447)."""
+    system = {"calib": configs.calib_from_positions(configs.chain_positions(4)),
+              "Om": np.ones(4), "delta": np.zeros(4)}
+    for want in ("dos", "thermal"):
+        with pytest.raises(ValueError, match="exact"):
+            backends.solve_equilibrium(system, want, backend="b200-kpm", exact=True)
+
+
 def test_model_refuses_unimplemented_channels():
     calib = configs.calib_from_positions(configs.chain_positions(4))
     n, om, de, pairs = model.model_arrays(calib, np.ones(4), np.zeros(4))
@@ -261,3 +299,85 @@ def test_segment_table_equals_segment_drive():
             assert np.array_equal(om, om2) and np.array_equal(de, de2), (interp, t)
     with pytest.raises(ValueError):
         table.drive(1.0, interp="cubic")
+
+
+class _NoLaunchContext:
+    """Stands in for a library context: any call through it fails the test,
+    so a refusal is shown to happen before a device address is passed on."""
+
+    def __init__(self):
+        import torch
+        self.device = torch.device("cuda", 0)
+
+    def call(self, name, *args):
+        raise AssertionError("%s reached the library" % name)
+
+
+@pytest.mark.parametrize("wrapper", ["cheb_step", "taylor_step", "observables", "observables_noalloc",
+                                     "spin_observables", "pauli_expect"])
+def test_state_wrappers_refuse_bad_vectors_before_any_call(wrapper):
+    """Every wrapper that hands a state's address to the library refuses a
+    vector of the wrong length, a non-contiguous view and a host tensor with
+    ValueError, without calling the library."""
+    import torch
+    from energy_level_b200 import solvers
+    ham = types.SimpleNamespace(ctx=_NoLaunchContext(), dim=16, n=4, handle=None)
+    args = {"cheb_step": (1.0,), "taylor_step": (1.0,), "spin_observables": ((),),
+            "pauli_expect": ([{"label": "z", "terms": [(0, "z")]}],)}.get(wrapper, ())
+    fn = getattr(solvers, wrapper)
+    short = torch.zeros(15, dtype=torch.complex64)
+    host = torch.zeros(16, dtype=torch.complex64)
+    strided = torch.zeros(32, dtype=torch.complex64)[::2]
+    for bad in (short, host) + ((strided,) if wrapper in ("cheb_step", "taylor_step", "observables_noalloc") else ()):
+        with pytest.raises(ValueError):
+            fn(ham, bad, *args)
+    if wrapper in ("cheb_step", "taylor_step"):
+        with pytest.raises(ValueError):
+            fn(ham, torch.zeros(16, dtype=torch.float32), *args)
+
+
+def test_hv_refuses_host_and_short_vectors():
+    import torch
+    from energy_level_b200.core import Hamiltonian
+    ham = Hamiltonian.__new__(Hamiltonian)
+    ham.ctx, ham.dim, ham.handle = _NoLaunchContext(), 16, None
+    for bad in (torch.zeros(15), torch.zeros(16), torch.zeros(16, 3, dtype=torch.int32)):
+        with pytest.raises(ValueError):
+            ham.hv(bad)
+
+
+def _constraint_gold():
+    import json
+    g = np.load(os.path.join(GOLD, "constraint.npz"))
+    calib = configs.calib_from_positions(g["pos"])
+    return g, calib, [(str(nm), json.loads(str(g[str(nm) + "_spec"]))) for nm in g["names"]]
+
+
+def test_constraint_specs_resolve_like_build_plan():
+    """Edges and projection of blockade / pxp specs with threshold_mhz,
+    'auto' edges and mode='full' equal the reference's build_plan
+    (hamiltonian_plan.py:15-72) on a 3x4 lattice; a projecting spec with
+    neither edges nor a threshold is refused."""
+    g, calib, specs = _constraint_gold()
+    for name, spec in specs:
+        projected, edges, norm = model.resolve_constraint(calib, spec)
+        assert projected == bool(g[name + "_projected"]), name
+        assert np.array_equal(np.asarray(edges, np.int64).reshape(-1, 2), g[name + "_edges"]), name
+    with pytest.raises(ValueError, match="threshold_mhz"):
+        model.resolve_constraint(calib, {"kind": "blockade"})
+    assert str(g["refusal"]).startswith("blockade/PXP project")
+    with pytest.raises(ValueError):
+        model.resolve_constraint(calib, "pxp")
+    with pytest.raises(ValueError):
+        model.resolve_constraint(calib, {"kind": "rydberg"})
+    with pytest.raises(ValueError):
+        model.resolve_constraint(calib, {"kind": "blockade", "edges": [[0, 0]]})
+    with pytest.raises(ValueError):
+        model.resolve_constraint(calib, {"kind": "blockade", "edges": "nearest"})
+    assert model.resolve_constraint(calib, None)[0] is False
+    assert model.resolve_constraint(calib, {"kind": "blockade", "edges": [[3, 1], [1, 3]]})[1] == [[1, 3]]
+    # a projected plan without edges takes them from its spec, or is refused
+    assert model.plan_edges({"projected": True, "constraint": specs[0][1], "calib": calib}) == \
+        g[specs[0][0] + "_edges"].tolist()
+    with pytest.raises(ValueError):
+        model.plan_edges({"projected": True})
