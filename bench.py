@@ -141,9 +141,16 @@ def profiled_traffic():
 
 # ---------------------------------------------------------------- CPU side
 
-def cpu_sample(cfg, moments=8, probes=2):
-    """Time the C oracle's direct KPM recurrence on a bounded sample of the
-    workload; return (seconds per probe-moment, threads, description)."""
+CPU_PROBES, CPU_MOMENTS = 4, 64          # the CPU sample of the native line
+REF_PROBES, REF_MOMENTS = 4, 16          # one step of the reference arm
+
+
+def cpu_sample(cfg, moments=CPU_MOMENTS, probes=CPU_PROBES):
+    """Time the C oracle's direct KPM recurrence (the reference's algorithm,
+    kpm.py:115-151, one H.v per moment) on a bounded sample of the workload.
+    Returns a dict: seconds per probe-moment, threads, description, and the
+    sample itself (probes, the spectral interval, the oracle's moments) for
+    the parity check of the GPU path on the same probes."""
     from oracle import build as ob
     n = cfg["n"]
     pairs = [(p["i"], p["j"], p["V"]) for p in cfg["calib"]["pairs"]]
@@ -156,10 +163,31 @@ def cpu_sample(cfg, moments=8, probes=2):
     c, r = 0.5 * (lo + hi), 0.5 * (hi - lo) * (1.0 + 1e-3)
     lib = ob.load()
     t0 = time.perf_counter()
-    ob.kpm_full(n, cfg["Om"], d, c, r, moments, z)
+    mu = ob.kpm_full(n, cfg["Om"], d, c, r, moments, z)
     dt = time.perf_counter() - t0
-    return dt / (moments * probes), int(lib.oracle_threads()), \
-        "N=%d full basis, %d probes x %d moments (direct recurrence, FP64)" % (n, probes, moments)
+    return {"s_per_probe_moment": dt / (moments * probes), "threads": int(lib.oracle_threads()),
+            "desc": "N=%d full basis, %d probes x %d moments (direct recurrence, FP64)" % (n, probes, moments),
+            "z": z, "c": c, "r": r, "mu": mu, "moments": moments}
+
+
+def oracle_check(ham, sample, block=NVEC):
+    """The GPU moments of the benchmark's kernel shape (one block of `block`
+    probes, chunk = block, doubling recurrence) against the C oracle's on the
+    sample's probes.  The block holds the sample's probes repeated with
+    alternating signs (a moment is quadratic in its probe, so the block mean
+    equals the sample mean while every probe group holds data of its own)."""
+    from energy_level_b200 import solvers
+    z = sample["z"]
+    reps = block // z.shape[0]
+    zz = np.concatenate([z if k % 2 == 0 else -z for k in range(reps)])
+    out = {"probes": int(z.shape[0]), "block": block, "moments": int(sample["moments"])}
+    for dt in ("float32", "float64"):
+        mu = solvers.kpm_moments(ham, sample["moments"], block, sample["c"], sample["r"], dtype=dt,
+                                 chunk=block, probes=zz, mode="doubling")
+        out["max_abs_moment_" + ("fp32" if dt == "float32" else "fp64")] = float(np.max(np.abs(mu - sample["mu"])))
+    out["tolerance"] = {"fp64": 1e-10, "fp32": 2e-4}
+    out["pass"] = bool(out["max_abs_moment_fp64"] <= 1e-10 and out["max_abs_moment_fp32"] <= 2e-4)
+    return out
 
 
 def run_reference(args):
@@ -169,10 +197,12 @@ def run_reference(args):
     cfg = workload(args.sites)
     times = []
     for i in range(args.warmup + args.steps):
-        tpm, threads, desc = cpu_sample(cfg)
+        # warm-up steps run a minimal sample; each timed step a bounded one
+        smp = cpu_sample(cfg, moments=REF_MOMENTS if i >= args.warmup else 2,
+                         probes=REF_PROBES if i >= args.warmup else 1)
         if i >= args.warmup:
-            times.append(tpm)
-    tpm = float(np.mean(times))
+            times.append(smp["s_per_probe_moment"])
+    tpm, threads, desc = float(np.mean(times)), smp["threads"], smp["desc"]
     solve_s = tpm * NUM * NVEC
     value = 1.0 / solve_s
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
@@ -310,12 +340,15 @@ def run_native(args):
         h2d = (b1[0] - b0[0]) // reps          # parameters copied in (Omega, delta, V table)
         d2h = (b1[1] - b0[1]) // reps          # scalars and moments copied out
 
-    # CPU baseline on the host cores (rank 0, single GPU only)
-    cpu = None
+    # CPU baseline on the host cores (rank 0, single GPU only), and the GPU
+    # kernel shape against the oracle on the sample's probes
+    cpu, check = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
-        tpm, threads, desc = cpu_sample(cfg)
-        cpu = {"value": 1.0 / (tpm * NUM * NVEC), "unit": "solves/s", "cores": threads, "kind": "port",
-               "sample": desc + "; extrapolated linearly to 1024 moments x 32 probes"}
+        smp = cpu_sample(cfg)
+        cpu = {"value": 1.0 / (smp["s_per_probe_moment"] * NUM * NVEC), "unit": "solves/s",
+               "cores": smp["threads"], "kind": "port",
+               "sample": smp["desc"] + "; extrapolated linearly to %d moments x %d probes" % (NUM, NVEC)}
+        check = oracle_check(ham, smp)
 
     if rank == 0:
         line = {
@@ -342,6 +375,7 @@ def run_native(args):
                                           "%d moments timed, scaled to %d" % (DIRECT_SAMPLE, NUM),
                                   "max_abs_moment_vs_doubling": err_direct},
             "error_vs_fp64": {"max_abs_moment": err_mu, "max_rel_dos": err_dos},
+            "oracle_check": check,
             "hv_gbs": achieved,
         }
         print(json.dumps(line))

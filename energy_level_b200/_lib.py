@@ -67,6 +67,8 @@ PROTOTYPES = {
     "el_batch_run": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _u64]),
     "el_batch_run_coop": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _u64]),
     "el_batch_set_wait_limit": (C.c_int, [_vp, _vp, C.c_int32]),
+    "el_batch_want_occupations": (C.c_int, [_vp, _vp, C.c_int]),
+    "el_batch_occupations": (C.c_int, [_vp, _vp, _dp]),
     "el_batch_results": (C.c_int, [_vp, _vp, _dp, _dp, _dp, _vp, _vp]),
     "el_batch_destroy": (C.c_int, [_vp]),
     "el_cheb_step": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_double, C.c_double, _ip]),

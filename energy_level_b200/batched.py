@@ -60,7 +60,13 @@ def pack_instances(instances):
 
 
 class BatchedGroundStates:
-    def __init__(self, instances, dtype='float32', max_iter=200, tol=None, device=0, ctx=None):
+    """A batch of instances on the device.  occupations=True also forms each
+    ground state's site occupations <n_i> (the n_atom of the reference's
+    batched_ground_state, equilibrium.py:251-311) from the Krylov basis in
+    every run; results() then carries an 'n_atom' array [count, max n]."""
+
+    def __init__(self, instances, dtype='float32', max_iter=200, tol=None, device=0, ctx=None,
+                 occupations=False):
         if dtype not in ('float32', 'float64'):
             raise ValueError('dtype 必须为 float32/float64')
         self.ctx = ctx or default_context(device)
@@ -77,6 +83,9 @@ class BatchedGroundStates:
                       C.c_void_p(k[6].ctypes.data), _lib.dptr(k[7]), C.c_int(_lib.DTYPES[dtype]),
                       C.c_int(int(max_iter)), C.c_double(self.tol), C.byref(h))
         self.handle = h
+        self.occupations = bool(occupations)
+        if self.occupations:
+            self.ctx.call('el_batch_want_occupations', self.handle, C.c_int(1))
         self.config = (512, 1)
         self.signature = (self.count, tuple(np.bincount(self.n_sites).tolist()), dtype, int(max_iter))
 
@@ -109,8 +118,13 @@ class BatchedGroundStates:
         cv = np.zeros(self.count, np.int32)
         self.ctx.call('el_batch_results', self.handle, _lib.dptr(e0), _lib.dptr(gap), _lib.dptr(res),
                       C.c_void_p(it.ctypes.data), C.c_void_p(cv.ctypes.data))
-        return dict(E0=e0, gap=gap, residuals=res, iters=it, converged=cv.astype(bool),
-                    backend='b200-batch-lanczos', dtype=self.dtype, tolerance=self.tol)
+        out = dict(E0=e0, gap=gap, residuals=res, iters=it, converged=cv.astype(bool),
+                   backend='b200-batch-lanczos', dtype=self.dtype, tolerance=self.tol)
+        if self.occupations:
+            nat = np.zeros((self.count, 40))
+            self.ctx.call('el_batch_occupations', self.handle, _lib.dptr(nat))
+            out['n_atom'] = nat[:, :int(self.n_sites.max())]
+        return out
 
     def autotune(self, candidates=((256, 1), (256, 2), (512, 1), (512, 2), (1024, 1)), reps=1):
         """Time each (threads, ctas_per_sm) on this batch; keep the fastest."""
@@ -161,14 +175,18 @@ COOP_MAX_INSTANCES = 8
 
 
 def batched_ground_states(instances, dtype='float32', max_iter=200, tol=None, device=0, tune=False,
-                          mode='auto'):
-    """Ground energies and gaps of many instances.  mode 'batch': one
-    persistent launch, one CTA per instance; 'coop': one cooperative launch
-    per instance over many CTAs; 'auto': 'coop' for a few instances
-    (<= COOP_MAX_INSTANCES) that fit it, else 'batch'."""
+                          mode='auto', occupations=True):
+    """Ground energies, gaps and (occupations=True) site occupations n_atom
+    of many instances: the keys of the reference's batched_ground_state
+    (E0, gap, n_atom, backend; equilibrium.py:251-311) plus residuals,
+    iterations and convergence flags.  mode 'batch': one persistent launch,
+    one CTA per instance; 'coop': one cooperative launch per instance over
+    many CTAs; 'auto': 'coop' for a few instances (<= COOP_MAX_INSTANCES)
+    that fit it, else 'batch'."""
     if mode not in ('auto', 'batch', 'coop'):
         raise ValueError("mode must be 'auto', 'batch' or 'coop'")
-    b = BatchedGroundStates(instances, dtype=dtype, max_iter=max_iter, tol=tol, device=device)
+    b = BatchedGroundStates(instances, dtype=dtype, max_iter=max_iter, tol=tol, device=device,
+                            occupations=occupations)
     used = 'batch'
     try:
         if mode == 'coop' or (mode == 'auto' and b.count <= COOP_MAX_INSTANCES):

@@ -45,6 +45,7 @@ struct BatchArgs {
   uint64_t seed;
   double *e0, *e1, *res, *gap;  // outputs in processing order
   int *iters, *conv;
+  double *nat;                  // [count][MAXN] ground-state <n_k> by bit position, or null
 };
 
 
@@ -470,6 +471,46 @@ __global__ void __launch_bounds__(NT) k_lanczos_batch(const BatchArgs A) {
       A.conv[idx] = (s_res[0] <= A.tol * fmax(1.0, fabs(s_th[0])) &&
                      s_res[1] <= A.tol * fmax(1.0, fabs(s_th[1]))) ? 1 : 0;
     }
+    if (A.nat) {
+      // site occupations of the ground-state Ritz vector x = sum_j y_j v_j
+      // (y: unit eigenvector of T for theta_0, by inverse iteration):
+      // <n_k> = sum_r x_r^2 bit_k(r) / sum_r x_r^2, fixed-order block sums
+      __syncthreads();
+      if (tid == 0) {
+        if (steps == 1) work[2 * MAXIT + 4] = 1.0;   // a one-vector Krylov space
+        else last_component(al, be, steps, s_th[0], work + 2 * MAXIT);
+      }
+      __syncthreads();
+      const double *y = work + 2 * MAXIT + 4 * steps;
+      // lane l of each warp owns bit positions l and l + 32: the warp's rows
+      // pass by shuffles, so no thread keeps a per-site array
+      const int lane = tid & 31;
+      double occ_lo = 0.0, occ_hi = 0.0, tot = 0.0;
+      for (int64_t r0 = tid - lane; r0 < dim; r0 += NT) {
+        const int64_t r = r0 + lane;
+        double p2 = 0.0;
+        uint64_t code = 0;
+        if (r < dim) {
+          double x = 0.0;
+          for (int jj = 0; jj < steps; ++jj) x += y[jj] * (double)Vb[(size_t)jj * A.dim_max + r];
+          p2 = x * x;
+          code = unrank_b(I, fib, r);
+        }
+        tot += p2;
+        for (int src = 0; src < 32; ++src) {
+          const double ps = __shfl_sync(0xffffffffu, p2, src);
+          const uint64_t cs = __shfl_sync(0xffffffffu, code, src);
+          if ((cs >> lane) & 1ULL) occ_lo += ps;
+          if (lane + 32 < MAXN && ((cs >> (lane + 32)) & 1ULL)) occ_hi += ps;
+        }
+      }
+      tot = block_sum<NT>(tot, red);
+      for (int k = 0; k < I.n; ++k) {
+        const double mine = (lane == (k & 31)) ? (k < 32 ? occ_lo : occ_hi) : 0.0;
+        const double sk = block_sum<NT>(mine, red);
+        if (tid == 0) A.nat[(size_t)idx * MAXN + k] = tot > 0 ? sk / tot : 0.0;
+      }
+    }
   }
 }
 
@@ -504,6 +545,7 @@ struct CoopArgs {
   uint64_t seed;
   double *e0, *e1, *res, *gap;
   int *iters, *conv;
+  double *nat;                  // [count][MAXN] ground-state <n_k>, or null
 };
 
 __device__ __forceinline__ void grid_barrier(const CoopArgs &G, unsigned &gen) {
@@ -531,6 +573,26 @@ __host__ __device__ inline size_t coop_slice_bytes(int m, int nt, int es) {
   return (((size_t)(m + 1) * (nt + 1) * es) + 15) / 16 * 16;
 }
 constexpr size_t COOP_WORK_BYTES = 2 * (6 * MAXIT + 8) * sizeof(double);
+
+// Per-CTA partial sums of the ground-state occupations: x = sum_j y_j v_j on
+// this thread's row (v_j in the CTA's Krylov slice), out[k] = sum over the
+// CTA's rows of x^2 bit_k, out[n] = sum of x^2 (kept out of line: it runs
+// once per solve and must not add to the main loop's registers).
+template <typename T, int NT>
+__device__ __noinline__ void coop_occupation_partials(const double *y, const T *Vs, int pitch, int steps,
+                                                      bool valid, uint64_t code, int n, double *red,
+                                                      double *out) {
+  double x = 0.0;
+  if (valid)
+    for (int jj = 0; jj < steps; ++jj) x += y[jj] * (double)Vs[(size_t)jj * pitch + threadIdx.x];
+  const double p2 = x * x;
+  for (int k = 0; k < n; ++k) {
+    const double sk = block_sum<NT>(((code >> k) & 1ULL) ? p2 : 0.0, red);
+    if (threadIdx.x == 0) out[k] = sk;
+  }
+  const double tot = block_sum<NT>(p2, red);
+  if (threadIdx.x == 0) out[n] = tot;
+}
 
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT) k_lanczos_coop(const CoopArgs G) {
@@ -742,6 +804,23 @@ __global__ void __launch_bounds__(NT) k_lanczos_coop(const CoopArgs G) {
     if (valid) vpub[row] = vn;
     grid_barrier(G, gen);
   }
+  if (G.nat) {
+    // site occupations of the ground-state Ritz vector (as in the batched
+    // kernel): every CTA forms y from the same alpha/beta, its rows of x from
+    // its Krylov slice, and per-site partial sums that reduce_all adds up
+    __syncthreads();
+    if (tid == 0) {
+      if (steps <= 1) work[4] = 1.0;
+      else last_component(al, be, steps, s_th[0], work);
+    }
+    __syncthreads();
+    coop_occupation_partials<T, NT>(work + 4 * (steps <= 1 ? 1 : steps), Vs, PITCH, steps, valid,
+                                    valid ? unrank_b(I, fib, row) : 0, I.n, red,
+                                    part(slot, blockIdx.x, 0));
+    reduce_all(I.n + 1);
+    if (blockIdx.x == 0 && tid < I.n)
+      G.nat[(size_t)G.p * MAXN + tid] = cs[I.n] > 0 ? cs[tid] / cs[I.n] : 0.0;
+  }
   if (blockIdx.x == 0 && tid == 0) {
     const int p = G.p;
     G.e0[p] = s_th[0];
@@ -795,6 +874,8 @@ struct el_batch_impl {
   double tol = 0;
   int64_t total_rows = 0, dim_max = 0;
   int wait_polls = 1 << 22;         // grid-barrier polls before a timeout (cooperative solver)
+  int want_nat = 0;                 // form the ground-state site occupations
+  double *d_nat = nullptr;          // [count][MAXN]
   std::vector<int> order;           // processing position -> caller index
   Inst *d_inst = nullptr;
   double *d_diag = nullptr;
@@ -805,6 +886,7 @@ struct el_batch_impl {
   size_t ws_bytes = 0;
   int device = 0;
   std::vector<int64_t> dims;        // per processing position
+  std::vector<int> nsites;          // per processing position
   // cooperative solver workspace
   void *c_vpub = nullptr;
   double *c_part = nullptr;
@@ -883,6 +965,7 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
     }
     off += dims[i];
     b->dims.push_back(dims[i]);
+    b->nsites.push_back(n);
     b->dim_max = std::max(b->dim_max, dims[i]);
   }
   b->total_rows = off;
@@ -943,6 +1026,7 @@ int el_batch_run(el_ctx *ctx, el_batch *b, int threads, int ctas_per_sm, uint64_
   A.seed = seed;
   A.e0 = b->d_out; A.e1 = b->d_out + b->count; A.res = b->d_out + 2 * b->count; A.gap = b->d_out + 3 * b->count;
   A.iters = b->d_iout; A.conv = b->d_iout + b->count;
+  A.nat = b->want_nat ? b->d_nat : nullptr;
 #define EL_BCASE(TT, NTV) k_lanczos_batch<TT, NTV><<<grid, NTV, 0, ctx->stream>>>(A)
   if (b->dtype == EL_F32) {
     if (threads == 256) EL_BCASE(float, 256); else if (threads == 512) EL_BCASE(float, 512); else EL_BCASE(float, 1024);
@@ -1012,6 +1096,7 @@ int el_batch_run_coop(el_ctx *ctx, el_batch *b, int reorth_passes, int check_eve
     G.bar = b->c_sync; G.err = (int *)(b->c_sync + 1); G.seed = seed;
     G.e0 = b->d_out; G.e1 = b->d_out + b->count; G.res = b->d_out + 2 * b->count; G.gap = b->d_out + 3 * b->count;
     G.iters = b->d_iout; G.conv = b->d_iout + b->count;
+    G.nat = b->want_nat ? b->d_nat : nullptr;
     if (p > 0) EL_CUDA_TRY(ctx, cudaMemsetAsync(b->c_sync, 0, sizeof(unsigned), ctx->stream));
     void *kargs[] = {(void *)&G};
     const void *fn = nullptr;
@@ -1038,6 +1123,36 @@ int el_batch_run_coop(el_ctx *ctx, el_batch *b, int reorth_passes, int check_eve
   EL_CUDA_TRY(ctx, el::copy(ctx, hs, b->c_sync, sizeof hs, cudaMemcpyDeviceToHost));
   EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (hs[1]) return fail(ctx, EL_ECUDA, "cooperative Lanczos: a grid barrier timed out");
+  return EL_OK;
+}
+
+int el_batch_want_occupations(el_ctx *ctx, el_batch *b, int want) {
+  if (!ctx || !b) return EL_EINVAL;
+  if (want && !b->d_nat) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx->stream, &cs);
+    if (cs != cudaStreamCaptureStatusNone) return fail(ctx, EL_EINVAL, "request occupations before capturing");
+    cudaError_t e = cudaMalloc(&b->d_nat, (size_t)b->count * MAXN * sizeof(double));
+    if (e != cudaSuccess) { cudaGetLastError(); b->d_nat = nullptr; return fail(ctx, EL_ENOMEM, "occupation buffer"); }
+    EL_CUDA_TRY(ctx, cudaMemsetAsync(b->d_nat, 0, (size_t)b->count * MAXN * sizeof(double), ctx->stream));
+  }
+  b->want_nat = want ? 1 : 0;
+  return EL_OK;
+}
+
+int el_batch_occupations(el_ctx *ctx, el_batch *b, double *n_atom) {
+  if (!ctx || !b || !n_atom) return EL_EINVAL;
+  if (!b->d_nat) return fail(ctx, EL_EINVAL, "occupations were not requested (el_batch_want_occupations)");
+  std::vector<double> h((size_t)b->count * MAXN);
+  EL_CUDA_TRY(ctx, el::copy(ctx, h.data(), b->d_nat, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  // processing order -> caller order; bit position k is site n-1-k
+  for (int p = 0; p < b->count; ++p) {
+    const int i = b->order[p];
+    const int n = b->nsites[p];
+    for (int s2 = 0; s2 < MAXN; ++s2)
+      n_atom[(size_t)i * MAXN + s2] = s2 < n ? h[(size_t)p * MAXN + (n - 1 - s2)] : 0.0;
+  }
   return EL_OK;
 }
 
@@ -1080,6 +1195,7 @@ int el_batch_destroy(el_batch *b) {
   if (b->c_vpub) cudaFree(b->c_vpub);
   if (b->c_part) cudaFree(b->c_part);
   if (b->c_sync) cudaFree(b->c_sync);
+  if (b->d_nat) cudaFree(b->d_nat);
   delete b;
   return EL_OK;
 }

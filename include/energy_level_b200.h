@@ -247,6 +247,17 @@ int el_batch_run(el_ctx *ctx, el_batch *batch, int threads, int ctas_per_sm, uin
  * last).  Same results layout as el_batch_run (read with el_batch_results). */
 int el_batch_run_coop(el_ctx *ctx, el_batch *batch, int reorth_passes, int check_every,
                       uint64_t seed);
+/* Also form each instance's ground-state site occupations <n_i> in later
+ * runs (want != 0; el_batch_run and el_batch_run_coop): the Ritz vector of
+ * the lowest Ritz value from the stored Krylov basis, normalised, its
+ * weights summed per excited site.  The n_atom output of the reference's
+ * batched_ground_state (equilibrium.py:251-311).  Call outside graph
+ * capture the first time (it allocates the result buffer). */
+int el_batch_want_occupations(el_ctx *ctx, el_batch *batch, int want);
+/* Copy the occupations of the last run: n_atom[i * 40 + s] = <n_s> of
+ * instance i (caller order, site s as in the calib; zeros beyond n_sites).
+ * Synchronises the stream. */
+int el_batch_occupations(el_ctx *ctx, el_batch *batch, double *n_atom);
 /* Bound of every grid-barrier wait of el_batch_run_coop, in polls of the
  * arrival counter (about 64 ns apart; default 4,194,304).  When a wait runs
  * out, that CTA stops waiting, sets the batch's error flag, every later

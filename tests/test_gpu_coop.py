@@ -111,3 +111,28 @@ def test_coop_barrier_timeout_is_reported_and_the_context_recovers(ctx):
     with pytest.raises(ValueError):
         b.set_wait_limit(-1)
     b.close()
+
+
+@pytest.mark.parametrize("mode", ["batch", "coop"])
+def test_batched_occupations_match_dense_ground_states(ctx, mode):
+    """n_atom of the batched solvers (persistent and cooperative) against the
+    occupations of the dense ground-state eigenvectors, as the reference's
+    batched_ground_state returns them (equilibrium.py:251-311)."""
+    from energy_level_b200.batched import batched_ground_states
+    rng = np.random.default_rng(12)
+    insts, want = [], []
+    for n, kind in [(12, "full"), (14, "chain"), (11, "ring"), (16, "chain")]:
+        edges = None if kind == "full" else (configs.ring_edges(n) if kind == "ring" else configs.chain_edges(n))
+        calib = configs.calib_from_positions(configs.chain_positions(n, jitter=rng.uniform(-0.3, 0.3, n)))
+        om, de = np.full(n, 2.0), rng.uniform(-3.0, 1.0, n)
+        insts.append(dict(calib=calib, Om=om, delta=de, edges=edges))
+        codes = None if edges is None else ref.independent_states(n, edges, None)
+        pairs = [(p["i"], p["j"], p["V"]) for p in calib["pairs"]]
+        w, v = np.linalg.eigh(ref.dense_h(n, codes, om, de, pairs))
+        want.append(ref.site_occupations(n, codes, v[:, 0]))
+    out = batched_ground_states(insts, dtype="float64", max_iter=300, tol=1e-11, mode=mode)
+    assert out["mode"] == mode and out["converged"].all()
+    for i, inst in enumerate(insts):
+        n = len(inst["Om"])
+        assert np.max(np.abs(out["n_atom"][i, :n] - want[i])) < 1e-7, i
+        assert np.all(out["n_atom"][i, n:] == 0)
