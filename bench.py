@@ -646,8 +646,16 @@ def native_lanczos12(h, args):
                       "form": "cooperative Lanczos, one launch per solve over 64 CTAs with the Krylov basis "
                               "in shared memory, full reorthogonalisation, FP32 vectors, FP64 alpha/beta",
                       "l2": "latency-bound (dim 4096 fits in L2)"})
+    # algorithmic bytes of a solve (FP32 vectors, FP64 diagonal): per step an
+    # H.v (read v, write w, read d) and two Gram-Schmidt passes over the j+1
+    # stored vectors (read twice each); the basis sits in shared memory, so
+    # this is a latency-bound solve and the fraction is of HBM for reference
+    it = int(r32["iters"][0])
+    alg = sum(4096 * (2 * 4 + 8) + 2 * 2 * (j + 1) * 4096 * 4 for j in range(it))
+    rl = roofline(alg, el / steps, kernel="k_lanczos_coop (whole solve: one launch)")
+    rl["note"] = "dim 4096: vectors and Krylov basis on chip; latency-bound (grid barriers), not HBM-bound"
     line.update({
-        "roofline": None,
+        "roofline": rl,
         "e2e": {"value": h.world / e2e_s, "unit": "solves/s",
                 "h2d_bytes_per_step": (b1[0] - b0[0]) // reps, "d2h_bytes_per_step": (b1[1] - b0[1]) // reps},
         "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
@@ -701,13 +709,18 @@ def ramp_runner(h, dtype, tol):
     psi = torch.zeros(basis.dim, dtype=getattr(torch, dtype), device="cuda")
     dt = 3000.0 / len(segs)
 
+    terms = [0]
+
     def solve():
         psi.zero_()
         psi[0] = 1.0                                          # all-g is code 0, rank 0
+        nt = 0
         for s in segs:
             ham.set_drive(s["Om"], s["delta"])
-            solvers.cheb_step(ham, psi, dt, tol=tol)
+            nt += solvers.cheb_step(ham, psi, dt, tol=tol)
+        terms[0] = nt
         return psi
+    solve.terms = terms
     return cfg, basis, ham, solve
 
 
@@ -785,8 +798,15 @@ def native_ramp31(h, args):
                       "segments": 300, "T_ns": 3000.0, "Om": 2.0, "Delta": "-6 -> +6 linear (left rule)",
                       "propagator": "Chebyshev (Jacobi-Anger), tol 1e-7", "psi0": "all g",
                       "l2": "state 28 MB x 4 live vectors: partly L2-resident (reported, no HBM claim)"})
+    # one Chebyshev term (complex64 state, FP32 diagonal): recurrence t_{m-2},
+    # t_{m-1} read and t_m written, accumulator read and written, diagonal read
+    nterms = int(solve32.terms[0])
+    rl = roofline(basis.dim * (3 * 8 + 2 * 8 + 4) * nterms, el / steps,
+                  kernel="k_apply_chain_tile (Chebyshev terms; whole solve: %d terms)" % nterms)
+    rl["note"] = "state 28 MB: the recurrence vectors are largely L2-resident"
     line.update({
-        "roofline": None,
+        "roofline": rl,
+        "chebyshev_terms_per_solve": nterms,
         "e2e": {"value": h.world / e2e_s, "unit": "solves/s",
                 "h2d_bytes_per_step": b1[0] - b0[0], "d2h_bytes_per_step": b1[1] - b0[1]},
         "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
@@ -869,13 +889,20 @@ def native_batch512(h, args):
     if h.rank == 0 and h.world == 1 and not args.no_cpu:
         cpu = cpu_batch_sample(insts)
     dims = [configs_fib(inst["n"] + 2) for inst in insts]
+    dims_p = dims
     line = base_line(args, h.world, "batch512", value, "solves/s", steps, el, "f32",
                      {"instances": len(insts), "n_sites": "16..22", "dims": [min(dims), max(dims)],
                       "mean_dim": float(np.mean(dims)), "form": "one persistent launch (CUDA graph), FP32 vectors, "
                       "FP64 alpha/beta and tridiagonal", "launch": {"threads": best[0], "ctas_per_sm": best[1]},
                       "l2": "8.6M rows x 4 B per vector; working set partly L2-resident"})
+    # lower bound of the compulsory bytes: per Lanczos step of each instance
+    # read v and w, write w (FP32) and read the FP64 diagonal (the partial
+    # reorthogonalisation passes are not counted)
+    alg = int(sum(int(r32["iters"][i]) * dims_p[i] * (3 * 4 + 8) for i in range(len(insts))))
+    rl = roofline(alg, el / steps, kernel="k_lanczos_batch (one persistent launch per batch)")
+    rl["note"] = "lower-bound bytes (no reorthogonalisation traffic); per-CTA vectors of <= 46k rows live in L2"
     line.update({
-        "roofline": None,
+        "roofline": rl,
         "e2e": {"value": h.world * len(insts) / e2e_s, "unit": "solves/s",
                 "h2d_bytes_per_step": b1[0] - b0[0], "d2h_bytes_per_step": b1[1] - b0[1]},
         "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
@@ -987,8 +1014,14 @@ def native_adjoint20(h, args):
                       "pulse_steps": len(tau), "T_ns": float(np.sum(tau)), "objective": "|<Z2|psi(T)>|^2",
                       "parameters": 2 * len(tau), "form": "adjoint through the Chebyshev steps, complex64, "
                       "terms recomputed per step", "l2": "dim 15,127: L2-resident (latency-bound)"})
+    # every launch of the gradient is counted as one sweep of a Chebyshev or
+    # reverse term over the basis (state, two recurrence vectors, adjoint,
+    # accumulator: 5 complex64 vectors and the FP32 diagonal) -- an estimate
+    rl = roofline(launches / steps * p32.basis.dim * (5 * 8 + 4), el / steps,
+                  kernel="k_apply_row / k_adjoint_step (estimate: every launch one term sweep)")
+    rl["note"] = "dim 15,127: L2-resident and launch-latency-bound"
     line.update({
-        "roofline": None,
+        "roofline": rl,
         "e2e": {"value": h.world / e2e_s, "unit": "grads/s",
                 "h2d_bytes_per_step": (b1[0] - b0[0]) // reps, "d2h_bytes_per_step": (b1[1] - b0[1]) // reps},
         "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks, "F": F32,
