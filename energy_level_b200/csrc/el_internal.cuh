@@ -90,6 +90,8 @@ struct ExPair {
   double are, aim;   // A: amplitude A into a row with (r, r), conj(A) into (g, g)
 };
 
+struct el_hv_plan;   // el_kpm_tma.cu
+
 struct el_ham {
   el_basis *basis = nullptr;
   int n = 0;
@@ -350,6 +352,15 @@ struct ChebPlan {
   std::vector<double> c_re, c_im;
 };
 int cheb_plan(el_ctx *ctx, el_ham *h, double tau_ns, double tol, ChebPlan *plan);
+// Tiled single-vector FP64 H x on the full basis, 20 <= N <= 25 (el_kpm_tma.cu):
+// a plan over three vector buffers, then y = H x + cz z per call with
+// <x,x>, <x,y>, 0, <y,y> in dots[0..3].
+bool hv_tiled_eligible(const el_ham *h, int dtype);
+int hv_tiled_plan(el_ctx *ctx, el_ham *h, void *const bufs[3], int slot, el_hv_plan **out);
+int hv_tiled(el_ctx *ctx, el_ham *h, el_hv_plan *P, int ix, int iy, int iz, double cz, double *dots);
+int hv_tiled_error(el_ctx *ctx, el_hv_plan *P);
+void hv_tiled_free(el_hv_plan *P);
+
 // TMA-fed tiled full-basis KPM recurrence (el_kpm_tma.cu), 20 <= N <= 25
 bool kpm_tma_eligible(const el_ham *h, int dtype, int chunk);
 int kpm_tma(el_ctx *ctx, el_ham *h, int dtype, int num, int nvec, int chunk, uint64_t seed,

@@ -67,6 +67,10 @@ struct TmaArgs {
   T amp[16];
   T amp2[16];          // (2/r) amp: the X t_m term of p_{m+1}
   T *gP, *gQ;          // the two recurrence buffers (cells [probe][row])
+  // apply passes (single vector): y = D x + X_A x + cz z, then y += X_B x
+  const T *dfull, *z;
+  T *y;
+  T cz;
   const T *d2;
   double *partials;
   unsigned int *counter;
@@ -668,6 +672,135 @@ k_kpm_v2(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
   if (tid == 0) *A.counter = 0u;
 }
 
+// ------------------------------------------------------ single-vector H x
+//
+// y = H x + cz z on the full basis as two tiled passes over one vector (the
+// Lanczos steps of the spectral bounds): the A pass (tiles of 2^a
+// consecutive rows) writes y = D x + X_A x + cz z, the B pass (tiles of
+// 2^C-row pieces 2^a rows apart) adds X_B x and forms <x,x>, <x,y>, <y,y>.
+// x arrives by TMA, double-buffered; z, D and y move by 16-byte loads and
+// stores.  Seven vector moves per product, instead of the row kernel's
+// repeated DRAM reads of every high-bit partner.
+template <typename T, int NWARP>
+__device__ __forceinline__ void hv_finish_dots(const TmaArgs<T> &A, double sxx, double sxy, double syy,
+                                               double (*wred)[3]);
+
+template <typename T, int TB, int KIND, int LNT>
+__global__ void __launch_bounds__(1 << LNT, 1)
+k_hv_pass(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapX) {
+  constexpr int VN = V16<T>::N, VB = V16<T>::LOG;
+  constexpr int NT = 1 << LNT;
+  constexpr int QB = TB - VB - LNT;
+  static_assert(QB >= 0, "tile smaller than one vector per thread");
+  constexpr int QR = 1 << QB;
+  constexpr int R = VN * QR;
+  constexpr int NWARP = NT / 32;
+  constexpr unsigned TILE_BYTES = (1u << TB) * (unsigned)sizeof(T);
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  T *const buf0 = reinterpret_cast<T *>(smem_raw);
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ double wred[NWARP][3];
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_async_smem();
+  }
+  __syncthreads();
+  unsigned par[2] = {0u, 0u};
+  int cur = 0;
+  int64_t item = blockIdx.x;
+  if (tid == 0 && item < A.items) {
+    mbar_expect(&bar[0], TILE_BYTES);
+    tile_load<KIND>(A, buf0, &mapX, (uint32_t)item, 0, &bar[0]);
+  }
+  double sxx = 0.0, sxy = 0.0, syy = 0.0;
+  for (; item < A.items; item += gridDim.x) {
+    const uint32_t tile = (uint32_t)item;
+    const int64_t nxt = item + gridDim.x;
+    if (tid == 0 && nxt < A.items) {   // the other buffer was released at the end of the last item
+      mbar_expect(&bar[cur ^ 1], TILE_BYTES);
+      tile_load<KIND>(A, buf0 + (size_t)(cur ^ 1) * (1u << TB), &mapX, (uint32_t)nxt, 0, &bar[cur ^ 1]);
+    }
+    mbar_wait(&bar[cur], par[cur], A.err);
+    par[cur] ^= 1u;
+    const T *S = buf0 + (size_t)cur * (1u << TB);
+    T own[R], h[R];
+#pragma unroll
+    for (int q = 0; q < QR; ++q) ld16(S + (size_t)VN * (tid + NT * q), own + VN * q);
+#pragma unroll
+    for (int j = 0; j < R; ++j) h[j] = z8(T{});
+    xapply_v2<T, TB, KIND, LNT, true, R>(S, own, h, A.amp, tid);
+#pragma unroll
+    for (int q = 0; q < QR; ++q) {
+      const int l0 = VN * (tid + NT * q);
+      const size_t row = gcell<T, KIND>(A.a, tile, l0);
+      T yv[VN];
+      if (KIND == KIND_A) {
+        T dv[VN], zv[VN];
+        ldg16(A.dfull + row, dv);
+        if (A.z) ldg16(A.z + row, zv);
+#pragma unroll
+        for (int v = 0; v < VN; ++v) {
+          T t = fma8(dv[v], own[VN * q + v], h[VN * q + v]);
+          if (A.z) t = fma8(A.cz, zv[v], t);
+          yv[v] = t;
+        }
+      } else {
+        T yo[VN];
+        ld16(A.y + row, yo);
+#pragma unroll
+        for (int v = 0; v < VN; ++v) {
+          yv[v] = yo[v] + h[VN * q + v];
+          const double xo = (double)own[VN * q + v], yn = (double)yv[v];
+          sxx += xo * xo;
+          sxy += xo * yn;
+          syy += yn * yn;
+        }
+      }
+      stcs16(A.y + row, yv);
+    }
+    __syncthreads();   // every thread is done with this buffer: the next prefetch may fill it
+    cur ^= 1;
+  }
+  if constexpr (KIND == KIND_B) hv_finish_dots<T, NWARP>(A, sxx, sxy, syy, wred);
+}
+
+// B pass: CTA sums of <x,x>, <x,y>, <y,y>, then the last CTA adds them up
+template <typename T, int NWARP>
+__device__ __forceinline__ void hv_finish_dots(const TmaArgs<T> &A, double sxx, double sxy, double syy,
+                                               double (*wred)[3]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    sxx += __shfl_xor_sync(0xffffffffu, sxx, o);
+    sxy += __shfl_xor_sync(0xffffffffu, sxy, o);
+    syy += __shfl_xor_sync(0xffffffffu, syy, o);
+  }
+  if (lane == 0) { wred[warp][0] = sxx; wred[warp][1] = sxy; wred[warp][2] = syy; }
+  __syncthreads();
+  double *mine = A.partials + (size_t)blockIdx.x * 3;
+  if (tid < 3) {
+    double sum = 0.0;
+#pragma unroll
+    for (int w = 0; w < NWARP; ++w) sum += wred[w][tid];
+    mine[tid] = sum;
+  }
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(A.counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (tid < 3) {
+    double sum = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) sum += __ldcg(&A.partials[(size_t)b * 3 + tid]);
+    A.dots[tid == 0 ? 0 : (tid == 1 ? 1 : 3)] = sum;
+  }
+  if (tid == 3) A.dots[2] = 0.0;
+  if (tid == 0) *A.counter = 0u;
+}
+
 // probes -> cells [probe group][row]; probe p = g*PU + lane
 template <typename T>
 __global__ void k_cells8(int64_t dim, int ng, uint64_t seed, int64_t probe0, int nvalid,
@@ -925,7 +1058,122 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
 
 }  // namespace
 
+// Tiled single-vector H x for the spectral bounds (FP64, full basis).
+struct el_hv_plan {
+  int n = 0, a = 0, hb = 0;
+  double *dfull = nullptr;          // [dim] D = diag V + sum delta n
+  void *bufs[3] = {nullptr, nullptr, nullptr};
+  CUtensorMap mA[3], mB[3];
+  int *err = nullptr;
+};
+
 namespace el {
+
+int hv_tiled_fill(el_ctx *ctx, el_ham *h, void *const bufs[3], int slot, el_hv_plan *P);
+
+bool hv_tiled_eligible(const el_ham *h, int dtype) {
+  return h->basis->layout == EL_LAYOUT_FULL && !h->complex_drive && h->px.empty() && !h->lossy &&
+         dtype == EL_F64 && h->n >= 20 && h->n <= 25 && encode_fn() != nullptr;
+}
+
+// Plan the tiled product over the three Lanczos buffers (each dim doubles);
+// the diagonal array and error flag come from workspace slot `slot`.
+int hv_tiled_plan(el_ctx *ctx, el_ham *h, void *const bufs[3], int slot, el_hv_plan **out) {
+  *out = nullptr;
+  el_hv_plan *P = new el_hv_plan();
+  const int rc = hv_tiled_fill(ctx, h, bufs, slot, P);
+  if (rc) { delete P; return rc; }
+  *out = P;
+  return EL_OK;
+}
+
+void hv_tiled_free(el_hv_plan *P) { delete P; }
+
+int hv_tiled_fill(el_ctx *ctx, el_ham *h, void *const bufs[3], int slot, el_hv_plan *P) {
+  typedef double T;
+  constexpr int C = Cell<T>::CARRY;
+  const int n = h->n;
+  const int64_t dim = h->basis->dim;
+  char *ws = (char *)workspace(ctx, slot, (size_t)dim * sizeof(T) + 64);
+  if (!ws) return EL_ENOMEM;
+  P->n = n;
+  P->dfull = reinterpret_cast<T *>(ws);
+  P->err = reinterpret_cast<int *>(ws + (size_t)dim * sizeof(T));
+  EL_CUDA_TRY(ctx, cudaMemsetAsync(P->err, 0, sizeof(int), ctx->stream));
+  double *d_delta = (double *)workspace(ctx, 8, 64 * sizeof(double));
+  if (!d_delta) return EL_ENOMEM;
+  EL_CUDA_TRY(ctx, copy(ctx, d_delta, h->delta, 64 * sizeof(double), cudaMemcpyHostToDevice));
+  // 2 (d - 0) / 2 = d exactly
+  k_d2_8<T><<<grid_for(dim, 256), 256, 0, ctx->stream>>>(n, dim, h->d_diagV64, d_delta, 0.0, 2.0, P->dfull);
+  EL_LAUNCH_CHECK(ctx);
+  const int amax = 13;
+  P->a = std::min(amax, std::max((n + C + 1) / 2, n + C - amax));
+  P->hb = (int)std::min<int64_t>(256, (int64_t)1 << (n - P->a));
+  for (int b = 0; b < 3; ++b) {
+    P->bufs[b] = bufs[b];
+    const int rc = make_maps<T>(ctx, bufs[b], n, P->a, 1, P->hb, &P->mA[b], &P->mB[b]);
+    if (rc) return rc;
+  }
+  return EL_OK;
+}
+
+// y = H x + cz z (z may be null), dots[0..3] = <x,x>, <x,y>, 0, <y,y>;
+// x, y, z are three of the planned buffers (ix, iy, iz indices; iz < 0: none).
+int hv_tiled(el_ctx *ctx, el_ham *h, el_hv_plan *P, int ix, int iy, int iz, double cz, double *dots) {
+  typedef double T;
+  constexpr int C = Cell<T>::CARRY;
+  const int n = P->n, a = P->a;
+  const int64_t dim = h->basis->dim;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  for (int kind = KIND_A; kind <= KIND_B; ++kind) {
+    TmaArgs<T> A;
+    memset(&A, 0, sizeof A);
+    const int TB = kind == KIND_B ? n - a + C : a;
+    A.n = n; A.a = a; A.ng = 1; A.dim = dim; A.hb = P->hb;
+    A.nbox = (int)(((int64_t)1 << (n - a)) / P->hb);
+    A.tiles = kind == KIND_A ? (dim >> a) : ((int64_t)1 << (a - C));
+    A.items = A.tiles;
+    for (int k = 0; k < TB && k < 16; ++k) {
+      const int rowbit = (kind == KIND_A) ? k : (k >= C ? a + k - C : -1);
+      A.amp[k] = (T)((rowbit >= 0) ? 0.5 * h->om_re[rowbit] : 0.0);
+    }
+    A.dfull = P->dfull;
+    A.z = iz >= 0 ? reinterpret_cast<const T *>(P->bufs[iz]) : nullptr;
+    A.cz = cz;
+    A.y = reinterpret_cast<T *>(P->bufs[iy]);
+    A.err = P->err;
+    A.counter = ctx->d_counter;
+    A.dots = dots;
+    const int grid = (int)std::min<int64_t>(A.items, sms);
+    int e = ensure_partials(ctx, (size_t)grid * 3);
+    if (e) return e;
+    A.partials = ctx->d_partials;
+    const CUtensorMap &mx = kind == KIND_A ? P->mA[ix] : P->mB[ix];
+    const size_t smem = (size_t)2 * ((size_t)1 << TB) * sizeof(T);
+    bool ok = false;
+#define EL_HCASE(TBV, KV)                                                                          \
+  if (TB == TBV && kind == KV) {                                                                   \
+    auto kern = k_hv_pass<T, TBV, KV, (TBV - V16<T>::LOG < 9 ? TBV - V16<T>::LOG : 9)>;            \
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);            \
+    kern<<<grid, 1 << (TBV - V16<T>::LOG < 9 ? TBV - V16<T>::LOG : 9), smem, ctx->stream>>>(A, mx); \
+    ok = true;                                                                                     \
+  }
+    EL_HCASE(11, KIND_A) EL_HCASE(12, KIND_A) EL_HCASE(13, KIND_A)
+    EL_HCASE(10, KIND_B) EL_HCASE(11, KIND_B) EL_HCASE(12, KIND_B) EL_HCASE(13, KIND_B)
+#undef EL_HCASE
+    if (!ok) return fail(ctx, EL_EINVAL, "tiled H x with %d tile bits not instantiated", TB);
+    EL_LAUNCH_CHECK(ctx);
+  }
+  return EL_OK;
+}
+
+int hv_tiled_error(el_ctx *ctx, el_hv_plan *P) {
+  int herr = 0;
+  EL_CUDA_TRY(ctx, copy(ctx, &herr, P->err, sizeof(int), cudaMemcpyDeviceToHost));
+  EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return herr ? fail(ctx, EL_ECUDA, "TMA transaction wait timed out in the tiled H x") : EL_OK;
+}
 
 bool kpm_tma_eligible(const el_ham *h, int dtype, int chunk) {
   if (h->basis->layout != EL_LAYOUT_FULL || h->complex_drive) return false;

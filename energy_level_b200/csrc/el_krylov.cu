@@ -73,17 +73,31 @@ extern "C" int el_bounds(el_ctx *ctx, el_ham *h, int max_iter, double tol,
   rc = el::launch_scale(ctx, dtype, dim, d_sc + 8, 1, v);
   if (rc) return rc;
   EL_CUDA_TRY(ctx, cudaMemsetAsync(vp, 0, vb, ctx->stream));
+  // large full bases: the tiled two-pass product (el_kpm_tma.cu) instead of
+  // the row kernel, whose high-bit partners come from DRAM again and again
+  el_hv_plan *plan = nullptr;
+  if (el::hv_tiled_eligible(h, dtype)) {
+    void *const bb[3] = {vp, v, w};
+    rc = el::hv_tiled_plan(ctx, h, bb, 15, &plan);
+    if (rc) return rc;
+  }
+  struct PlanGuard { el_hv_plan *p; ~PlanGuard() { if (p) el::hv_tiled_free(p); } } guard{plan};
+  int ivp = 0, iv = 1, iw = 2;   // buffer indices of vp, v, w in the plan
   std::vector<double> al, be;
   double beta = 0.0, lo_prev = 0, hi_prev = 0;
   int stable = 0;
   const int maxit = (int)std::min<int64_t>(max_iter, dim);
   for (int j = 0; j < maxit; ++j) {
     if (el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
-    ApplyArgs A;
-    memset(&A, 0, sizeof A);
-    A.dtype = dtype; A.nvec = 1; A.x = v; A.z = vp; A.y = w;
-    A.a = 1.0; A.b = 0.0; A.c = -beta; A.dots = d_sc; A.want_dots = 2;
-    rc = el::launch_apply(ctx, h, A);
+    if (plan) {
+      rc = el::hv_tiled(ctx, h, plan, iv, iw, ivp, -beta, d_sc);
+    } else {
+      ApplyArgs A;
+      memset(&A, 0, sizeof A);
+      A.dtype = dtype; A.nvec = 1; A.x = v; A.z = vp; A.y = w;
+      A.a = 1.0; A.b = 0.0; A.c = -beta; A.dots = d_sc; A.want_dots = 2;
+      rc = el::launch_apply(ctx, h, A);
+    }
     if (rc) return rc;
     double dots[4];
     rc = sync_read(ctx, d_sc, 4, dots);
@@ -112,8 +126,14 @@ extern "C" int el_bounds(el_ctx *ctx, el_ham *h, int max_iter, double tol,
     // v_prev <- v ; v <- w / beta
     std::swap(vp, v);
     std::swap(v, w);
+    std::swap(ivp, iv);
+    std::swap(iv, iw);
     double inv = 1.0 / beta;
     rc = el::launch_axpby(ctx, dtype, dim, 0, 0, nullptr, inv, 0, v, nullptr);
+    if (rc) return rc;
+  }
+  if (plan) {
+    rc = el::hv_tiled_error(ctx, plan);
     if (rc) return rc;
   }
   *emin = lo_prev;

@@ -204,3 +204,54 @@ def test_tma_kpm_benchmark_shape_matches_oracle(ctx, dtype, tol):
     got = solvers.kpm_moments(h, num, 32, c, r, dtype=dtype, chunk=32, probes=zz, mode="doubling")
     assert abs(got[0] - 1.0) < 1e-12
     assert np.abs(got - want).max() < tol
+
+
+def _oracle_extremes(n, om, d, steps=300, seed=0):
+    """Extremal eigenvalues by a plain Lanczos run on the C oracle's H x."""
+    import ctypes as C
+    from scipy.linalg import eigvalsh_tridiagonal
+    from oracle import build as ob
+    lib = ob.load()
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    om = np.ascontiguousarray(om, dtype=np.float64)
+    d = np.ascontiguousarray(d, dtype=np.float64)
+
+    def hv(x):
+        y = np.empty_like(x)
+        lib.oracle_apply_full(n, dp(om), dp(d), 1, 1.0, 0.0, 0.0, dp(x), None, dp(y))
+        return y
+    v = np.random.default_rng(seed).standard_normal(1 << n)
+    v /= np.linalg.norm(v)
+    vp = np.zeros_like(v)
+    al, be, beta = [], [], 0.0
+    for _ in range(steps):
+        w = hv(v) - beta * vp
+        a = float(v @ w)
+        w -= a * v
+        al.append(a)
+        beta = float(np.linalg.norm(w))
+        be.append(beta)
+        vp, v = v, w / beta
+    ev = eigvalsh_tridiagonal(np.array(al), np.array(be[:-1]))
+    return ev[0], ev[-1]
+
+
+@pytest.mark.parametrize("n", [20, 21])
+def test_tiled_bounds_match_oracle_lanczos(ctx, n):
+    """Spectral bounds of the full basis at N >= 20, where the FP64 Lanczos
+    runs the tiled two-pass product (A tiles, then B pieces), against a
+    Lanczos run on the C oracle's H x (the reference's kpm._bounds role,
+    kpm.py:82-97)."""
+    from energy_level_b200.core import Basis, Hamiltonian
+    from energy_level_b200 import solvers
+    from oracle import build as ob
+    rng = np.random.default_rng(40 + n)
+    om = rng.uniform(0.5, 2.0, n)
+    de = rng.uniform(-3, 3, n)
+    pos = [[6.0 * (i % 5), 6.0 * (i // 5), 0.0] for i in range(n)]
+    pairs = configs.pairs_from_positions(pos)
+    lo_want, hi_want = _oracle_extremes(n, om, ob.diag_full(n, de, pairs))
+    h = Hamiltonian(ctx, Basis(ctx, n, kind="full"), om, de, pairs)
+    lo, hi = solvers.bounds(h, max_iter=400, tol=1e-12)
+    scale = max(abs(lo_want), abs(hi_want))
+    assert abs(lo - lo_want) < 1e-9 * scale and abs(hi - hi_want) < 1e-9 * scale
