@@ -62,6 +62,7 @@ enum { MODE_STEP = 0, MODE_PROLOGUE = 1, MODE_LAST = 2 };
 template <typename T>
 struct TmaArgs {
   int n, a, mode, ng, log_tiles, hb, nbox;
+  int tile_major, log_ng;   // work-item order: tile-major (all probe groups of a tile together) or group-major
   int64_t dim, tiles, items;
   T s_m, two_r, pro_alpha, pro_beta;
   T amp[16];
@@ -77,6 +78,19 @@ struct TmaArgs {
   double *dots;
   int *err;
 };
+
+// Work item -> (probe group, tile).  Tile-major order puts the ng probe
+// groups of one tile next to each other, so the CTAs working at the same
+// time share that tile's diagonal values in L2 (it is read from DRAM once
+// per pass instead of once per probe group).
+template <typename T>
+__device__ __forceinline__ int item_group(const TmaArgs<T> &A, int64_t item) {
+  return A.tile_major ? (int)(item & (A.ng - 1)) : (int)(item >> A.log_tiles);
+}
+template <typename T>
+__device__ __forceinline__ uint32_t item_tile(const TmaArgs<T> &A, int64_t item) {
+  return A.tile_major ? (uint32_t)(item >> A.log_ng) : (uint32_t)(item & (A.tiles - 1));
+}
 
 // ---------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -216,15 +230,15 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
   double acc_tt[PU], acc_tq[PU];
 #pragma unroll
   for (int q = 0; q < PU; ++q) { acc_tt[q] = 0.0; acc_tq[q] = 0.0; }
-  int gacc = (int)(item >> A.log_tiles);
+  int gacc = item_group(A, item);
   if (tid == 0 && item < A.items) {
-    const uint32_t tile = (uint32_t)(item & (A.tiles - 1));
+    const uint32_t tile = item_tile(A, item);
     mbar_expect(&bar[0], TILE_BYTES);
     tile_load<KIND>(A, Sb0, &mapQ, tile, gacc, &bar[0]);
   }
   for (; item < A.items; item += gridDim.x) {
-    const int g = (int)(item >> A.log_tiles);
-    const uint32_t tile = (uint32_t)(item & (A.tiles - 1));
+    const int g = item_group(A, item);
+    const uint32_t tile = item_tile(A, item);
     const int64_t nxt = item + gridDim.x;
     if (g != gacc) {   // uniform across the CTA: flush the previous group's sums
 #pragma unroll
@@ -278,8 +292,8 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
     if (tid == 0 && nxt < A.items) {
       // prefetch the next t_{m-1} tile once the previous S store has read Sn
       bulk_wait_read<0>();
-      const int gn = (int)(nxt >> A.log_tiles);
-      const uint32_t tn = (uint32_t)(nxt & (A.tiles - 1));
+      const int gn = item_group(A, nxt);
+      const uint32_t tn = item_tile(A, nxt);
       uint64_t *bn = cur ? &bar[0] : &bar[1];
       mbar_expect(bn, TILE_BYTES);
       tile_load<KIND>(A, Sn, &mapQ, tn, gn, bn);
@@ -941,6 +955,8 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   // 2 = v2 with shuffled lane gathers
   int variant = 0;
   if (const char *ev = getenv("EL_KPM_KERNEL")) variant = atoi(ev);
+  int order = 0;
+  if (const char *ev = getenv("EL_KPM_ORDER")) order = atoi(ev);
   auto launch = [&](int kind, int mode, double s_m, int pbuf, double *dots) -> int {
     TmaArgs<T> A;
     memset(&A, 0, sizeof A);
@@ -951,6 +967,9 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     A.items = A.tiles * ng;
     A.log_tiles = 0;
     while (((int64_t)1 << A.log_tiles) < A.tiles) ++A.log_tiles;
+    A.log_ng = 0;
+    while ((1 << A.log_ng) < ng) ++A.log_ng;
+    A.tile_major = order;
     A.s_m = (T)s_m; A.two_r = (T)(2.0 / r); A.pro_alpha = (T)0.5; A.pro_beta = (T)(1.0 / r);
     for (int k = 0; k < TB && k < 16; ++k) {
       int rowbit = (kind == KIND_A) ? k : (k >= C ? a + k - C : -1);
