@@ -66,8 +66,6 @@ struct TmaArgs {
   int64_t dim, tiles, items;
   T s_m, two_r, pro_alpha, pro_beta;
   T amp[16];
-  T amp2[16];          // (2/r) amp: the X t_m term of p_{m+1}
-  T *gP, *gQ;          // the two recurrence buffers (cells [probe][row])
   // apply passes (single vector): y = D x + X_A x + cz z, then y += X_B x
   const T *dfull, *z;
   T *y;
@@ -400,49 +398,20 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
   if (tid == 0) *A.counter = 0u;
 }
 
-// ------------------------------------------------------------ pass kernel v2
+// --------------------------------------------- 16-byte vector helpers
 //
-// The same recurrence and tiles, with the shared-memory traffic per cell cut
-// to what the sigma^x gathers need:
-//   - every access is a 16-byte vector (float4 / double2) of consecutive
-//     cells, so the two (FP32) or one (FP64) lowest tile bits are register
-//     bits: cell l = v + VN (tid + NT q) for vector lane v and block q;
-//   - t_m and p_{m+1} go from registers straight to global memory (st.cs),
-//     not through shared memory and a TMA store: only the gathered t_m is
-//     written to shared memory;
-//   - the five lane bits of the thread index are gathered by warp shuffles
-//     (SHF) or by 16-byte shared loads (!SHF); the warp bits by shared loads;
-//   - the three tile buffers rotate: at item i the t_{m-1} tile of item i+1
-//     is loaded into the free buffer at the start, the p_{m+1}... p tile of
-//     item i+1 into the buffer of t_{m-1}(i) once the first X application
-//     has read it, and the p / t_m buffer of item i is free at its end.
+// Used by the single-vector FP64 tiled H x below: every access is a
+// 16-byte vector (double2) of consecutive cells, so the lowest tile bit is a
+// register bit: cell l = v + VN (tid + NT q) for vector lane v and block q.
 template <typename T> struct V16;
-template <> struct V16<float> { static constexpr int N = 4, LOG = 2; };
 template <> struct V16<double> { static constexpr int N = 2, LOG = 1; };
 
-__device__ __forceinline__ void ld16(const float *p, float *d) {
-  const float4 v = *reinterpret_cast<const float4 *>(p);
-  d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-}
 __device__ __forceinline__ void ld16(const double *p, double *d) {
   const double2 v = *reinterpret_cast<const double2 *>(p);
   d[0] = v.x; d[1] = v.y;
 }
-__device__ __forceinline__ void st16(float *p, const float *d) {
-  *reinterpret_cast<float4 *>(p) = make_float4(d[0], d[1], d[2], d[3]);
-}
-__device__ __forceinline__ void st16(double *p, const double *d) {
-  *reinterpret_cast<double2 *>(p) = make_double2(d[0], d[1]);
-}
-__device__ __forceinline__ void stcs16(float *p, const float *d) {
-  __stcs(reinterpret_cast<float4 *>(p), make_float4(d[0], d[1], d[2], d[3]));
-}
 __device__ __forceinline__ void stcs16(double *p, const double *d) {
   __stcs(reinterpret_cast<double2 *>(p), make_double2(d[0], d[1]));
-}
-__device__ __forceinline__ void ldg16(const float *p, float *d) {
-  const float4 v = __ldg(reinterpret_cast<const float4 *>(p));
-  d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
 }
 __device__ __forceinline__ void ldg16(const double *p, double *d) {
   const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
@@ -453,7 +422,7 @@ __device__ __forceinline__ void ldg16(const double *p, double *d) {
 // this thread's R cells: x in registers (src) and, for the thread-index
 // bits, in shared memory (S, natural cell order).
 template <typename T, int TB, int KIND, int LNT, bool SHF, int R>
-__device__ __forceinline__ void xapply_v2(const T *S, const T (&src)[R], T (&h)[R], const T *amp, int tid) {
+__device__ __forceinline__ void xapply_tile(const T *S, const T (&src)[R], T (&h)[R], const T *amp, int tid) {
   constexpr int VN = V16<T>::N, VB = V16<T>::LOG, C = Cell<T>::CARRY;
   constexpr int NT = 1 << LNT;
   constexpr int QB = TB - VB - LNT;
@@ -500,190 +469,6 @@ __device__ __forceinline__ void xapply_v2(const T *S, const T (&src)[R], T (&h)[
 template <typename T, int KIND>
 __device__ __forceinline__ size_t gcell(int a, uint32_t tile, int l0) {
   return row_of<KIND, Cell<T>::CARRY>(a, tile, l0);
-}
-
-template <typename T, int TB, int KIND, int LNT, bool SHF>
-__global__ void __launch_bounds__(1 << LNT, 1)
-k_kpm_v2(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
-         const __grid_constant__ CUtensorMap mapQ) {
-  constexpr int VN = V16<T>::N, VB = V16<T>::LOG;
-  constexpr int NT = 1 << LNT;
-  constexpr int QB = TB - VB - LNT;
-  static_assert(QB >= 0, "tile smaller than one vector per thread");
-  constexpr int QR = 1 << QB;
-  constexpr int R = VN * QR;
-  constexpr int NWARP = NT / 32;
-  constexpr unsigned TILE_BYTES = (1u << TB) * (unsigned)sizeof(T);
-  static_assert(TILE_BYTES <= 65536, "three tile buffers must fit in shared memory");
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  T *const buf0 = reinterpret_cast<T *>(smem_raw);
-  __shared__ __align__(8) uint64_t bar[3];
-  __shared__ double wred[NWARP][2];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int ndots = A.ng * 2;
-  double *dacc = A.partials + (size_t)blockIdx.x * ndots;
-  for (int i = tid; i < ndots; i += NT) dacc[i] = 0.0;
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    mbar_init(&bar[2], 1);
-    fence_async_smem();
-  }
-  __syncthreads();
-  unsigned par[3] = {0u, 0u, 0u};
-  int bx = 0, bp = 1, bf = 2;   // buffers: t_{m-1}, p_m (then t_m), free
-  const T *__restrict__ d2 = A.d2;
-  int64_t item = blockIdx.x;
-  int gacc = (int)(item >> A.log_tiles);
-  if (tid == 0 && item < A.items) {
-    const uint32_t tile = (uint32_t)(item & (A.tiles - 1));
-    mbar_expect(&bar[bx], TILE_BYTES);
-    tile_load<KIND>(A, buf0 + (size_t)bx * (1u << TB), &mapQ, tile, gacc, &bar[bx]);
-    if (A.mode != MODE_PROLOGUE) {
-      mbar_expect(&bar[bp], TILE_BYTES);
-      tile_load<KIND>(A, buf0 + (size_t)bp * (1u << TB), &mapP, tile, gacc, &bar[bp]);
-    }
-  }
-  double acc_tt = 0.0, acc_tq = 0.0;
-  for (; item < A.items; item += gridDim.x) {
-    const int g = (int)(item >> A.log_tiles);
-    const uint32_t tile = (uint32_t)(item & (A.tiles - 1));
-    const int64_t nxt = item + gridDim.x;
-    const int gn = (int)(nxt >> A.log_tiles);
-    const uint32_t tn = (uint32_t)(nxt & (A.tiles - 1));
-    if (g != gacc) {   // uniform across the CTA: flush the previous group's sums
-      double x = acc_tt, y = acc_tq;
-      for (int o = 16; o > 0; o >>= 1) {
-        x += __shfl_xor_sync(0xffffffffu, x, o);
-        y += __shfl_xor_sync(0xffffffffu, y, o);
-      }
-      if (lane == 0) { wred[warp][0] = x; wred[warp][1] = y; }
-      acc_tt = 0.0; acc_tq = 0.0;
-      __syncthreads();
-      if (tid < 2) {
-        double sum = 0.0;
-#pragma unroll
-        for (int w = 0; w < NWARP; ++w) sum += wred[w][tid];
-        dacc[gacc * 2 + tid] += sum;
-      }
-      gacc = g;
-    }
-    // the next item's t_{m-1} tile into the free buffer
-    if (tid == 0 && nxt < A.items) {
-      mbar_expect(&bar[bf], TILE_BYTES);
-      tile_load<KIND>(A, buf0 + (size_t)bf * (1u << TB), &mapQ, tn, gn, &bar[bf]);
-    }
-    mbar_wait(&bar[bx], par[bx], A.err);
-    par[bx] ^= 1u;
-    const T *S = buf0 + (size_t)bx * (1u << TB);
-    T own[R], hx[R];
-#pragma unroll
-    for (int q = 0; q < QR; ++q) ld16(S + (size_t)VN * (tid + NT * q), own + VN * q);
-#pragma unroll
-    for (int j = 0; j < R; ++j) hx[j] = z8(T{});
-    xapply_v2<T, TB, KIND, LNT, SHF, R>(S, own, hx, A.amp, tid);
-    __syncthreads();   // every thread is done with S: it takes the next item's p tile
-    if (tid == 0 && nxt < A.items && A.mode != MODE_PROLOGUE) {
-      mbar_expect(&bar[bx], TILE_BYTES);
-      tile_load<KIND>(A, buf0 + (size_t)bx * (1u << TB), &mapP, tn, gn, &bar[bx]);
-    }
-    T *const gP = A.gP + (size_t)g * A.dim;
-    T *const gQ = A.gQ + (size_t)g * A.dim;
-    T pt[2] = {(T)0, (T)0}, pq[2] = {(T)0, (T)0};
-    if (A.mode == MODE_PROLOGUE) {
-      // p_1 = (D-c)/r t_0 + pro_beta X t_0
-#pragma unroll
-      for (int q = 0; q < QR; ++q) {
-        const int l0 = VN * (tid + NT * q);
-        T dv[VN], o[VN];
-        ldg16(d2 + d2_index<T, KIND, TB>(A.a, tile, l0), dv);
-#pragma unroll
-        for (int v = 0; v < VN; ++v) {
-          o[v] = fma8(A.pro_beta, hx[VN * q + v], scl8(A.pro_alpha * dv[v], own[VN * q + v]));
-          pt[v & 1] = fma(own[VN * q + v], own[VN * q + v], pt[v & 1]);
-        }
-        stcs16(gP + gcell<T, KIND>(A.a, tile, l0), o);
-      }
-    } else {
-      mbar_wait(&bar[bp], par[bp], A.err);
-      par[bp] ^= 1u;
-      T *const P = buf0 + (size_t)bp * (1u << TB);
-      // t_m = p_m + s_m X t_{m-1}: into registers, global memory and (for the
-      // second X application) shared memory
-#pragma unroll
-      for (int q = 0; q < QR; ++q) {
-        const int l0 = VN * (tid + NT * q);
-        T pm[VN];
-        ld16(P + l0, pm);
-#pragma unroll
-        for (int v = 0; v < VN; ++v) {
-          const T t = fma8(A.s_m, hx[VN * q + v], pm[v]);
-          hx[VN * q + v] = t;
-          pt[v & 1] = fma(t, t, pt[v & 1]);
-          pq[v & 1] = fma(t, own[VN * q + v], pq[v & 1]);
-        }
-        if (A.mode != MODE_LAST) {
-          st16(P + l0, hx + VN * q);
-          stcs16(gP + gcell<T, KIND>(A.a, tile, l0), hx + VN * q);
-        }
-      }
-      if (A.mode != MODE_LAST) {
-        fence_async_smem();   // generic writes to P precede a later TMA load into it
-        __syncthreads();      // t_m complete in shared memory
-        // p_{m+1} = d2 t_m - t_{m-1} + (2/r) X t_m
-        T h2[R];
-#pragma unroll
-        for (int q = 0; q < QR; ++q) {
-          T dv[VN];
-          ldg16(d2 + d2_index<T, KIND, TB>(A.a, tile, VN * (tid + NT * q)), dv);
-#pragma unroll
-          for (int v = 0; v < VN; ++v) h2[VN * q + v] = sub8(scl8(dv[v], hx[VN * q + v]), own[VN * q + v]);
-        }
-        xapply_v2<T, TB, KIND, LNT, SHF, R>(P, hx, h2, A.amp2, tid);
-#pragma unroll
-        for (int q = 0; q < QR; ++q) {
-          const int l0 = VN * (tid + NT * q);
-          stcs16(gQ + gcell<T, KIND>(A.a, tile, l0), h2 + VN * q);
-        }
-      }
-    }
-    acc_tt += (double)pt[0] + (double)pt[1];
-    acc_tq += (double)pq[0] + (double)pq[1];
-    __syncthreads();   // every thread is done with the p buffer: it is the next free one
-    const int t3 = bf;
-    bf = bp;
-    bp = bx;
-    bx = t3;
-  }
-  // flush the last group
-  {
-    double x = acc_tt, y = acc_tq;
-    for (int o = 16; o > 0; o >>= 1) {
-      x += __shfl_xor_sync(0xffffffffu, x, o);
-      y += __shfl_xor_sync(0xffffffffu, y, o);
-    }
-    if (lane == 0) { wred[warp][0] = x; wred[warp][1] = y; }
-  }
-  __syncthreads();
-  if (tid < 2 && blockIdx.x < A.items) {
-    double sum = 0.0;
-#pragma unroll
-    for (int w = 0; w < NWARP; ++w) sum += wred[w][tid];
-    dacc[gacc * 2 + tid] += sum;
-  }
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) last = (atomicAdd(A.counter, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  for (int i = tid; i < ndots; i += NT) {
-    double sum = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) sum += __ldcg(&A.partials[(size_t)b * ndots + i]);
-    A.dots[i] = sum;
-  }
-  if (tid == 0) *A.counter = 0u;
 }
 
 // ------------------------------------------------------ single-vector H x
@@ -744,7 +529,7 @@ k_hv_pass(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapX) {
     for (int q = 0; q < QR; ++q) ld16(S + (size_t)VN * (tid + NT * q), own + VN * q);
 #pragma unroll
     for (int j = 0; j < R; ++j) h[j] = z8(T{});
-    xapply_v2<T, TB, KIND, LNT, true, R>(S, own, h, A.amp, tid);
+    xapply_tile<T, TB, KIND, LNT, true, R>(S, own, h, A.amp, tid);
 #pragma unroll
     for (int q = 0; q < QR; ++q) {
       const int l0 = VN * (tid + NT * q);
@@ -951,10 +736,6 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   if (rc) return rc;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  // pass kernel: 0 = v1 (TMA stores), 1 = v2 with shared-memory lane gathers,
-  // 2 = v2 with shuffled lane gathers
-  int variant = 0;
-  if (const char *ev = getenv("EL_KPM_KERNEL")) variant = atoi(ev);
   int order = 0;
   if (const char *ev = getenv("EL_KPM_ORDER")) order = atoi(ev);
   auto launch = [&](int kind, int mode, double s_m, int pbuf, double *dots) -> int {
@@ -974,10 +755,7 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     for (int k = 0; k < TB && k < 16; ++k) {
       int rowbit = (kind == KIND_A) ? k : (k >= C ? a + k - C : -1);
       A.amp[k] = (T)((rowbit >= 0) ? 0.5 * h->om_re[rowbit] : 0.0);
-      A.amp2[k] = (T)((rowbit >= 0) ? (2.0 / r) * 0.5 * h->om_re[rowbit] : 0.0);
     }
-    A.gP = reinterpret_cast<T *>(pbuf == 0 ? P : Q);
-    A.gQ = reinterpret_cast<T *>(pbuf == 0 ? Q : P);
     A.d2 = (kind == KIND_B && sizeof(T) == 4) ? d2b : d2; A.dots = dots; A.err = d_err; A.counter = ctx->d_counter;
     const int grid = (int)std::min<int64_t>(A.items, sms);
     int e = el::ensure_partials(ctx, (size_t)grid * ng * PU * 2);
@@ -992,28 +770,6 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     // 1024 threads: twice the registers per cell made 512 threads slower.
     const int lnt = (sizeof(T) == 4 && TB >= 12) ? 9 : 10;
     bool ok = false;
-    if (variant > 0) {
-      const bool shf = variant == 2;
-#define EL_VCASE(TBV, KV)                                                                           \
-  if (TB == TBV && kind == KV) {                                                                    \
-    auto kern = shf ? k_kpm_v2<T, TBV, KV, (TBV - V16<T>::LOG < 9 ? TBV - V16<T>::LOG : 9), true>   \
-                    : k_kpm_v2<T, TBV, KV, (TBV - V16<T>::LOG < 9 ? TBV - V16<T>::LOG : 9), false>; \
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
-    kern<<<grid, 1 << (TBV - V16<T>::LOG < 9 ? TBV - V16<T>::LOG : 9), smem, ctx->stream>>>(A, mp, mq); \
-    ok = true;                                                                                      \
-  }
-      if constexpr (sizeof(T) == 4) {
-        EL_VCASE(11, KIND_A) EL_VCASE(12, KIND_A) EL_VCASE(13, KIND_A) EL_VCASE(14, KIND_A)
-        EL_VCASE(11, KIND_B) EL_VCASE(12, KIND_B) EL_VCASE(13, KIND_B) EL_VCASE(14, KIND_B)
-      } else {
-        EL_VCASE(10, KIND_A) EL_VCASE(11, KIND_A) EL_VCASE(12, KIND_A) EL_VCASE(13, KIND_A)
-        EL_VCASE(10, KIND_B) EL_VCASE(11, KIND_B) EL_VCASE(12, KIND_B) EL_VCASE(13, KIND_B)
-      }
-#undef EL_VCASE
-      if (!ok) return fail(ctx, EL_EINVAL, "TMA pass with %d tile bits not instantiated", TB);
-      EL_LAUNCH_CHECK(ctx);
-      return EL_OK;
-    }
 #define EL_TCASE(TBV, KV, LV)                                                                     \
   if (TB == TBV && kind == KV && lnt == LV) {                                                     \
     cudaFuncSetAttribute(k_kpm_tma<T, TBV, KV, LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
