@@ -25,6 +25,8 @@
 // records an error flag (read by the host) and finishes without hanging.
 #include "el_internal.cuh"
 
+#define EL_KPM_MAXN 25   // sites of the tiled full-basis passes
+
 #include <algorithm>
 #include <cstdlib>
 #include <cuda.h>
@@ -63,6 +65,12 @@ template <typename T>
 struct TmaArgs {
   int n, a, mode, ng, log_tiles, hb, nbox;
   int tile_major, log_ng;   // work-item order: tile-major (all probe groups of a tile together) or group-major
+  // diagonal from tile sums instead of the d2 array (diag_otf): V between
+  // row bits [n][n], delta per row bit, d2 = s2 d + s2c
+  int diag_otf;
+  const T *vbits;
+  T delta_b[32];
+  T s2, s2c;
   int64_t dim, tiles, items;
   T s_m, two_r, pro_alpha, pro_beta;
   T amp[16];
@@ -175,6 +183,16 @@ __device__ __forceinline__ size_t d2_index(int a, uint32_t tile, int l) {
   return ((size_t)tile << TB) + (size_t)l;
 }
 
+// Row bit of tile bit k, and of tile-index bit i.
+template <int KIND, int C>
+__device__ __forceinline__ int tile_rowbit(int a, int k) {
+  return KIND == KIND_A ? k : (k < C ? k : a + k - C);
+}
+template <int KIND, int C>
+__device__ __forceinline__ int index_rowbit(int a, int i) {
+  return KIND == KIND_A ? a + i : C + i;
+}
+
 // h[j] += sum_{k in [K0, KMAX)} amp_k * S[(tid ^ 2^k) + NT*j] for the R cells
 // of this thread (NT = 2^KMAX threads).  Bit-outer order: one address per
 // bit, R independent FMA chains per bit.
@@ -187,6 +205,35 @@ __device__ __forceinline__ void gather_all(const T *S, int tid, const TmaArgs<T>
 #pragma unroll
     for (int j = 0; j < R; ++j) h[j] = fma8(a, base[(1 << KMAX) * j], h[j]);
   }
+}
+
+// d2 = 2 (D - c) / r of this thread's R cells of a tile: from the d2 array
+// or (diag_otf) from the per-thread, per-CTA and per-tile sums
+template <typename T, int KIND, int TB, int LNT>
+__device__ __forceinline__ void tile_diag(const TmaArgs<T> &A, uint32_t tile, int tid, T cT,
+                                          const T (&cTJ)[(TB - LNT) > 0 ? (TB - LNT) : 1], const T *tJ,
+                                          const T *wH, T cH, const T *__restrict__ d2,
+                                          T (&dv)[1 << (TB - LNT)]) {
+  constexpr int RB = TB - LNT;
+  constexpr int R = 1 << RB;
+  constexpr int NT = 1 << LNT;
+  if (!A.diag_otf) {
+#pragma unroll
+    for (int j = 0; j < R; ++j) dv[j] = d2[d2_index<T, KIND, TB>(A.a, tile, tid + NT * j)];
+    return;
+  }
+  T base = cT + cH;
+  for (int x = 0; x < LNT; ++x)
+    if ((tid >> x) & 1) base += wH[x];
+  dv[0] = (T)0;
+#pragma unroll
+  for (int k = 0; k < RB; ++k) {
+    const T u = cTJ[k] + wH[LNT + k];
+#pragma unroll
+    for (int j = 0; j < (1 << k); ++j) dv[j + (1 << k)] = dv[j] + u;
+  }
+#pragma unroll
+  for (int j = 0; j < R; ++j) dv[j] = fma8(A.s2, base + tJ[j] + dv[j], A.s2c);
 }
 
 template <typename T, int TB, int KIND, int LNT>
@@ -209,10 +256,25 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
   U *const S2 = reinterpret_cast<U *>(smem_raw + 2 * TILE_BYTES);
   __shared__ __align__(8) uint64_t bar[3];   // S buffers 0/1, S2
   __shared__ double wred[NWARP][2 * PU];
+  // The diagonal of a cell's row, d = sum_b delta_b + sum_{b<b'} V_bb' over
+  // its set row bits, split over the three sets of bits a cell's row has:
+  // the thread's index bits (T, fixed per thread), its register bits (J,
+  // the cell's slot j) and the tile index bits (H, fixed per tile):
+  //   d = cT + tJ[j] + cH + sum_{x in T} wH_x + sum_{k in J(j)} (cTJ_k + wH_k)
+  // with cT, cTJ per thread once, tJ per CTA once, and cH, wH_k (the
+  // couplings of every tile bit to the tile's set index bits) per tile.
+  constexpr int RB = TB - LNT;               // register bits
+  __shared__ T sV[EL_KPM_MAXN * EL_KPM_MAXN];
+  __shared__ T tJ[R];
+  __shared__ T wH[16];
+  __shared__ T s_cH;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ndots = A.ng * PU * 2;
+  const int nb = A.n;
   double *dacc = A.partials + (size_t)blockIdx.x * ndots;
   for (int i = tid; i < ndots; i += NT) dacc[i] = 0.0;
+  if (A.diag_otf)
+    for (int i = tid; i < nb * nb; i += NT) sV[i] = A.vbits[i];
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -220,6 +282,35 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
     fence_async_smem();
   }
   __syncthreads();
+  T cT = (T)0, cTJ[RB > 0 ? RB : 1];
+  if (A.diag_otf) {
+    for (int x = 0; x < LNT; ++x) {
+      if (!((tid >> x) & 1)) continue;
+      const int X = tile_rowbit<KIND, C>(A.a, x);
+      cT += A.delta_b[X];
+      for (int x2 = 0; x2 < x; ++x2)
+        if ((tid >> x2) & 1) cT += sV[X * nb + tile_rowbit<KIND, C>(A.a, x2)];
+    }
+#pragma unroll
+    for (int k = 0; k < RB; ++k) {
+      const int K = tile_rowbit<KIND, C>(A.a, LNT + k);
+      T sacc = (T)0;
+      for (int x = 0; x < LNT; ++x)
+        if ((tid >> x) & 1) sacc += sV[tile_rowbit<KIND, C>(A.a, x) * nb + K];
+      cTJ[k] = sacc;
+    }
+    for (int j = tid; j < R; j += NT) {
+      T v = (T)0;
+      for (int k = 0; k < RB; ++k) {
+        if (!((j >> k) & 1)) continue;
+        const int K = tile_rowbit<KIND, C>(A.a, LNT + k);
+        v += A.delta_b[K];
+        for (int k2 = 0; k2 < k; ++k2)
+          if ((j >> k2) & 1) v += sV[K * nb + tile_rowbit<KIND, C>(A.a, LNT + k2)];
+      }
+      tJ[j] = v;
+    }
+  }
   unsigned par[3] = {0u, 0u, 0u};
   const T *__restrict__ d2 = A.d2;
   int cur = 0;
@@ -265,6 +356,28 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
     // the S store may still be reading Sn; in the prologue it is the only
     // group) and (2) every thread has finished the previous item, whose last
     // pass reads S2 after its final barrier.
+    if (A.diag_otf && warp == NWARP - 1) {
+      // this tile's couplings: wH_k = sum over set index bits i of V(k, i),
+      // cH = the diagonal of the index bits alone
+      if (lane < TB) {
+        const int K = tile_rowbit<KIND, C>(A.a, lane);
+        T sacc = (T)0;
+        for (int i = 0; i < A.log_tiles; ++i)
+          if ((tile >> i) & 1u) sacc += sV[K * nb + index_rowbit<KIND, C>(A.a, i)];
+        wH[lane] = sacc;
+      }
+      if (lane == 31) {
+        T sacc = (T)0;
+        for (int i = 0; i < A.log_tiles; ++i) {
+          if (!((tile >> i) & 1u)) continue;
+          const int I = index_rowbit<KIND, C>(A.a, i);
+          sacc += A.delta_b[I];
+          for (int i2 = 0; i2 < i; ++i2)
+            if ((tile >> i2) & 1u) sacc += sV[I * nb + index_rowbit<KIND, C>(A.a, i2)];
+        }
+        s_cH = sacc;
+      }
+    }
     if (tid == 0) {
       if (A.mode == MODE_PROLOGUE) bulk_wait_read<0>();
       else bulk_wait_read<1>();
@@ -303,10 +416,12 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
     for (int q = 0; q < PU; ++q) { pt[q][0] = pt[q][1] = pq[q][0] = pq[q][1] = (T)0; }
     if (A.mode == MODE_PROLOGUE) {
       // p_1 = (D-c)/r t_0 + pro_beta X_G t_0 -> S2 -> P
+      T dv[R];
+      tile_diag<T, KIND, TB, LNT>(A, tile, tid, cT, cTJ, tJ, wH, s_cH, d2, dv);
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         const int l = tid + NT * j;
-        S2[l] = fma8(A.pro_beta, hx[j], scl8(A.pro_alpha * d2[d2_index<T, KIND, TB>(A.a, tile, l)], own[j]));
+        S2[l] = fma8(A.pro_beta, hx[j], scl8(A.pro_alpha * dv[j], own[j]));
 #pragma unroll
         for (int q = 0; q < PU; ++q) pt[q][j & 1] = fma(get8(own[j], q), get8(own[j], q), pt[q][j & 1]);
       }
@@ -337,8 +452,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
         // the diagonal of this thread's rows, loaded before the gathers so
         // that its latency hides behind them
         T dv[R];
-#pragma unroll
-        for (int j = 0; j < R; ++j) dv[j] = d2[d2_index<T, KIND, TB>(A.a, tile, tid + NT * j)];
+        tile_diag<T, KIND, TB, LNT>(A, tile, tid, cT, cTJ, tJ, wH, s_cH, d2, dv);
         U h2[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) h2[j] = z8(U{});
@@ -698,12 +812,20 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   const int64_t dim = h->basis->dim;
   const int ng = chunk / PU;
   const size_t vb = (size_t)dim * chunk * sizeof(T);
-  char *buf = (char *)el::workspace(ctx, 6, 2 * vb + 2 * (size_t)dim * sizeof(T) + 64);
+  const size_t vbits_bytes = (size_t)EL_KPM_MAXN * EL_KPM_MAXN * sizeof(T);
+  char *buf = (char *)el::workspace(ctx, 6, 2 * vb + 2 * (size_t)dim * sizeof(T) + 256 + vbits_bytes);
   if (!buf) return EL_ENOMEM;
   void *P = buf, *Q = buf + vb;
   T *d2 = reinterpret_cast<T *>(buf + 2 * vb);
   T *d2b = d2 + dim;   // the same diagonal in B-tile order
   int *d_err = reinterpret_cast<int *>(buf + 2 * vb + 2 * (size_t)dim * sizeof(T));
+  T *d_vbits = reinterpret_cast<T *>(buf + 2 * vb + 2 * (size_t)dim * sizeof(T) + 256);
+  {
+    std::vector<T> vb_host((size_t)n * n);
+    for (size_t i = 0; i < vb_host.size(); ++i) vb_host[i] = (T)h->Vbits[i];
+    EL_CUDA_TRY(ctx, el::copy(ctx, d_vbits, vb_host.data(), vb_host.size() * sizeof(T), cudaMemcpyHostToDevice));
+    EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));   // vb_host leaves scope
+  }
   const int M = (num + 1) / 2;
   double *d_dots = (double *)el::workspace(ctx, 7, (size_t)(M + 1) * chunk * 2 * sizeof(double));
   if (!d_dots) return EL_ENOMEM;
@@ -738,6 +860,8 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   int order = 0;
   if (const char *ev = getenv("EL_KPM_ORDER")) order = atoi(ev);
+  int diag_otf = 0;
+  if (const char *ev = getenv("EL_KPM_DIAG")) diag_otf = atoi(ev);
   auto launch = [&](int kind, int mode, double s_m, int pbuf, double *dots) -> int {
     TmaArgs<T> A;
     memset(&A, 0, sizeof A);
@@ -751,6 +875,11 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     A.log_ng = 0;
     while ((1 << A.log_ng) < ng) ++A.log_ng;
     A.tile_major = order;
+    A.diag_otf = diag_otf;
+    A.vbits = d_vbits;
+    for (int k = 0; k < n && k < 32; ++k) A.delta_b[k] = (T)h->delta[k];
+    A.s2 = (T)(2.0 / r);
+    A.s2c = (T)(-2.0 * c / r);
     A.s_m = (T)s_m; A.two_r = (T)(2.0 / r); A.pro_alpha = (T)0.5; A.pro_beta = (T)(1.0 / r);
     for (int k = 0; k < TB && k < 16; ++k) {
       int rowbit = (kind == KIND_A) ? k : (k >= C ? a + k - C : -1);
