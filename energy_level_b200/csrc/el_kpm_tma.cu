@@ -64,12 +64,11 @@ enum { MODE_STEP = 0, MODE_PROLOGUE = 1, MODE_LAST = 2 };
 template <typename T>
 struct TmaArgs {
   int n, a, mode, ng, log_tiles, hb, nbox;
-  // diagonal from tile sums instead of the d2 array (diag_otf): V between
-  // row bits [n][n], delta per row bit, d2 = s2 d + s2c
-  int diag_otf;
-  const T *vbits;
-  T delta_b[32];
-  T s2, s2c;
+  // FP32 passes: the diagonal from tile sums instead of a d2 array (V
+  // between row bits [n][n] and delta per row bit, FP64), d2 = s2 d + s2c
+  const double *vbits;
+  double delta_b[32];
+  double s2, s2c;
   int64_t dim, tiles, items;
   T s_m, two_r, pro_alpha, pro_beta;
   T amp[16];
@@ -147,14 +146,15 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 
 // Tile <-> tensor-map coordinates.  A: 3-D map {256-byte chunk, chunk index,
 // probe}; B: 4-D map {low-bit piece, tile, h, probe}.
-template <int KIND, typename T>
+template <int KIND, typename T, int CR = Cell<T>::CARRY>
 __device__ __forceinline__ void tile_load(const TmaArgs<T> &A, void *dst, const CUtensorMap *m,
                                           uint32_t tile, int g, uint64_t *bar) {
   if (KIND == KIND_A) {
     tma_load3(dst, m, 0, (int)(tile << (A.a - Cell<T>::LOGCH)), g, bar);
   } else {
+    constexpr int PIECE = (1 << CR) * (int)sizeof(T);
     for (int k = 0; k < A.nbox; ++k)
-      tma_load4((char *)dst + (size_t)k * A.hb * Cell<T>::PIECE, m, 0, (int)tile, k * A.hb, g, bar);
+      tma_load4((char *)dst + (size_t)k * A.hb * PIECE, m, 0, (int)tile, k * A.hb, g, bar);
   }
 }
 template <int KIND, typename T>
@@ -174,13 +174,10 @@ __device__ __forceinline__ uint32_t row_of(int a, uint32_t tile, int l) {
   return (uint32_t)(l & ((1 << C) - 1)) + ((uint32_t)(l >> C) << a) + (tile << C);
 }
 
-// Index of cell l of a tile in the diagonal array the kernel is given: FP32
-// B tiles read a B-tile-ordered copy (one coalesced request per warp); A
-// tiles, and FP64 B tiles (measured slower with the copy), read row order.
+// Index of cell l of a tile in the (row-ordered) diagonal array.
 template <typename T, int KIND, int TB>
 __device__ __forceinline__ size_t d2_index(int a, uint32_t tile, int l) {
-  if (KIND == KIND_B && sizeof(T) == 8) return row_of<KIND_B, Cell<T>::CARRY>(a, tile, l);
-  return ((size_t)tile << TB) + (size_t)l;
+  return row_of<KIND, Cell<T>::CARRY>(a, tile, l);
 }
 
 // Row bit of tile bit k, and of tile-index bit i.
@@ -207,33 +204,38 @@ __device__ __forceinline__ void gather_all(const T *S, int tid, const TmaArgs<T>
   }
 }
 
-// d2 = 2 (D - c) / r of this thread's R cells of a tile: from the d2 array
-// or (diag_otf) from the per-thread, per-CTA and per-tile sums
+// d2 = 2 (D - c) / r of this thread's R cells of a tile.  FP32 passes form
+// it from the per-thread, per-CTA and per-tile sums in FP64 and round once
+// (as a precomputed FP32 array would be rounded); FP64 passes read the d2
+// array (their registers have no room for the sums).
+template <typename T> struct OnTheFly { static constexpr bool value = sizeof(T) == 4; };
+
 template <typename T, int KIND, int TB, int LNT>
-__device__ __forceinline__ void tile_diag(const TmaArgs<T> &A, uint32_t tile, int tid, T cT,
-                                          const T (&cTJ)[(TB - LNT) > 0 ? (TB - LNT) : 1], const T *tJ,
-                                          const T *wH, T cH, const T *__restrict__ d2,
-                                          T (&dv)[1 << (TB - LNT)]) {
+__device__ __forceinline__ void tile_diag(const TmaArgs<T> &A, uint32_t tile, int tid, double cT,
+                                          const double *cTJ, const double *tJ, const double *wH, double cH,
+                                          const T *__restrict__ d2, T (&dv)[1 << (TB - LNT)]) {
   constexpr int RB = TB - LNT;
   constexpr int R = 1 << RB;
   constexpr int NT = 1 << LNT;
-  if (!A.diag_otf) {
+  if constexpr (!OnTheFly<T>::value) {
 #pragma unroll
     for (int j = 0; j < R; ++j) dv[j] = d2[d2_index<T, KIND, TB>(A.a, tile, tid + NT * j)];
-    return;
+  } else {
+    double base = cT + cH;
+    for (int x = 0; x < LNT; ++x)
+      if ((tid >> x) & 1) base += wH[x];
+    double u[RB > 0 ? RB : 1];
+#pragma unroll
+    for (int k = 0; k < RB; ++k) u[k] = cTJ[k * NT + tid] + wH[LNT + k];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      double dj = base + tJ[j];
+#pragma unroll
+      for (int k = 0; k < RB; ++k)
+        if ((j >> k) & 1) dj += u[k];
+      dv[j] = (T)fma(A.s2, dj, A.s2c);
+    }
   }
-  T base = cT + cH;
-  for (int x = 0; x < LNT; ++x)
-    if ((tid >> x) & 1) base += wH[x];
-  dv[0] = (T)0;
-#pragma unroll
-  for (int k = 0; k < RB; ++k) {
-    const T u = cTJ[k] + wH[LNT + k];
-#pragma unroll
-    for (int j = 0; j < (1 << k); ++j) dv[j + (1 << k)] = dv[j] + u;
-  }
-#pragma unroll
-  for (int j = 0; j < R; ++j) dv[j] = fma8(A.s2, base + tJ[j] + dv[j], A.s2c);
 }
 
 template <typename T, int TB, int KIND, int LNT>
@@ -264,16 +266,18 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
   // with cT, cTJ per thread once, tJ per CTA once, and cH, wH_k (the
   // couplings of every tile bit to the tile's set index bits) per tile.
   constexpr int RB = TB - LNT;               // register bits
-  __shared__ T sV[EL_KPM_MAXN * EL_KPM_MAXN];
-  __shared__ T tJ[R];
-  __shared__ T wH[16];
-  __shared__ T s_cH;
+  constexpr bool OTF = OnTheFly<T>::value;
+  __shared__ double sV[OTF ? EL_KPM_MAXN * EL_KPM_MAXN : 1];
+  __shared__ double tJ[OTF ? R : 1];
+  __shared__ double cTJ[OTF ? (RB > 0 ? RB : 1) * NT : 1];   // [k][tid]: couplings of the thread bits to register bit k
+  __shared__ double wH[16];
+  __shared__ double s_cH;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ndots = A.ng * PU * 2;
   const int nb = A.n;
   double *dacc = A.partials + (size_t)blockIdx.x * ndots;
   for (int i = tid; i < ndots; i += NT) dacc[i] = 0.0;
-  if (A.diag_otf)
+  if constexpr (OTF)
     for (int i = tid; i < nb * nb; i += NT) sV[i] = A.vbits[i];
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -282,8 +286,8 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
     fence_async_smem();
   }
   __syncthreads();
-  T cT = (T)0, cTJ[RB > 0 ? RB : 1];
-  if (A.diag_otf) {
+  double cT = 0.0;
+  if constexpr (OTF) {
     for (int x = 0; x < LNT; ++x) {
       if (!((tid >> x) & 1)) continue;
       const int X = tile_rowbit<KIND, C>(A.a, x);
@@ -294,13 +298,13 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
 #pragma unroll
     for (int k = 0; k < RB; ++k) {
       const int K = tile_rowbit<KIND, C>(A.a, LNT + k);
-      T sacc = (T)0;
+      double sacc = 0.0;
       for (int x = 0; x < LNT; ++x)
         if ((tid >> x) & 1) sacc += sV[tile_rowbit<KIND, C>(A.a, x) * nb + K];
-      cTJ[k] = sacc;
+      cTJ[k * NT + tid] = sacc;
     }
     for (int j = tid; j < R; j += NT) {
-      T v = (T)0;
+      double v = 0.0;
       for (int k = 0; k < RB; ++k) {
         if (!((j >> k) & 1)) continue;
         const int K = tile_rowbit<KIND, C>(A.a, LNT + k);
@@ -356,18 +360,18 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
     // the S store may still be reading Sn; in the prologue it is the only
     // group) and (2) every thread has finished the previous item, whose last
     // pass reads S2 after its final barrier.
-    if (A.diag_otf && warp == NWARP - 1) {
+    if (OTF && warp == NWARP - 1) {
       // this tile's couplings: wH_k = sum over set index bits i of V(k, i),
       // cH = the diagonal of the index bits alone
       if (lane < TB) {
         const int K = tile_rowbit<KIND, C>(A.a, lane);
-        T sacc = (T)0;
+        double sacc = 0.0;
         for (int i = 0; i < A.log_tiles; ++i)
           if ((tile >> i) & 1u) sacc += sV[K * nb + index_rowbit<KIND, C>(A.a, i)];
         wH[lane] = sacc;
       }
       if (lane == 31) {
-        T sacc = (T)0;
+        double sacc = 0.0;
         for (int i = 0; i < A.log_tiles; ++i) {
           if (!((tile >> i) & 1u)) continue;
           const int I = index_rowbit<KIND, C>(A.a, i);
@@ -524,6 +528,9 @@ __device__ __forceinline__ void ld16(const double *p, double *d) {
   const double2 v = *reinterpret_cast<const double2 *>(p);
   d[0] = v.x; d[1] = v.y;
 }
+__device__ __forceinline__ void st16(double *p, const double *d) {
+  *reinterpret_cast<double2 *>(p) = make_double2(d[0], d[1]);
+}
 __device__ __forceinline__ void stcs16(double *p, const double *d) {
   __stcs(reinterpret_cast<double2 *>(p), make_double2(d[0], d[1]));
 }
@@ -535,9 +542,9 @@ __device__ __forceinline__ void ldg16(const double *p, double *d) {
 // h[j] += amp[k] x[partner_k(j)] over every flipped bit k of the tile for
 // this thread's R cells: x in registers (src) and, for the thread-index
 // bits, in shared memory (S, natural cell order).
-template <typename T, int TB, int KIND, int LNT, bool SHF, int R>
+template <typename T, int TB, int KIND, int LNT, bool SHF, int R, int C = Cell<T>::CARRY>
 __device__ __forceinline__ void xapply_tile(const T *S, const T (&src)[R], T (&h)[R], const T *amp, int tid) {
-  constexpr int VN = V16<T>::N, VB = V16<T>::LOG, C = Cell<T>::CARRY;
+  constexpr int VN = V16<T>::N, VB = V16<T>::LOG;
   constexpr int NT = 1 << LNT;
   constexpr int QB = TB - VB - LNT;
   constexpr int QR = 1 << QB;
@@ -580,20 +587,21 @@ __device__ __forceinline__ void xapply_tile(const T *S, const T (&src)[R], T (&h
 
 // global cell index (within one probe group) of the first cell of 16-byte
 // block l0 of a tile
-template <typename T, int KIND>
+template <typename T, int KIND, int CR = Cell<T>::CARRY>
 __device__ __forceinline__ size_t gcell(int a, uint32_t tile, int l0) {
-  return row_of<KIND, Cell<T>::CARRY>(a, tile, l0);
+  return row_of<KIND, CR>(a, tile, l0);
 }
 
 // ------------------------------------------------------ single-vector H x
 //
 // y = H x + cz z on the full basis as two tiled passes over one vector (the
-// Lanczos steps of the spectral bounds): the A pass (tiles of 2^a
-// consecutive rows) writes y = D x + X_A x + cz z, the B pass (tiles of
-// 2^C-row pieces 2^a rows apart) adds X_B x and forms <x,x>, <x,y>, <y,y>.
-// x arrives by TMA, double-buffered; z, D and y move by 16-byte loads and
-// stores.  Seven vector moves per product, instead of the row kernel's
-// repeated DRAM reads of every high-bit partner.
+// Lanczos steps of the spectral bounds): the B pass (tiles of 2^C-row
+// pieces 2^a rows apart) writes y = X_B x, the A pass (tiles of 2^a
+// consecutive rows) completes y = D x + X_A x + cz z + y and forms <x,x>,
+// <x,y>, <y,y>.  x arrives by TMA, double-buffered; z, D and y move by
+// 16-byte loads and stores, so the strided B pieces of y are only written
+// (the reads of y are contiguous A rows).  Seven vector moves per product,
+// instead of the row kernel's repeated DRAM reads of every high-bit partner.
 template <typename T, int NWARP>
 __device__ __forceinline__ void hv_finish_dots(const TmaArgs<T> &A, double sxx, double sxy, double syy,
                                                double (*wred)[3]);
@@ -650,36 +658,36 @@ k_hv_pass(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapX) {
       const size_t row = gcell<T, KIND>(A.a, tile, l0);
       T yv[VN];
       if (KIND == KIND_A) {
-        T dv[VN], zv[VN];
+        T dv[VN], zv[VN], yb[VN];
         ldg16(A.dfull + row, dv);
+        ldg16(A.y + row, yb);
         if (A.z) ldg16(A.z + row, zv);
 #pragma unroll
         for (int v = 0; v < VN; ++v) {
-          T t = fma8(dv[v], own[VN * q + v], h[VN * q + v]);
+          T t = fma8(dv[v], own[VN * q + v], h[VN * q + v] + yb[v]);
           if (A.z) t = fma8(A.cz, zv[v], t);
           yv[v] = t;
-        }
-      } else {
-        T yo[VN];
-        ld16(A.y + row, yo);
-#pragma unroll
-        for (int v = 0; v < VN; ++v) {
-          yv[v] = yo[v] + h[VN * q + v];
-          const double xo = (double)own[VN * q + v], yn = (double)yv[v];
+          const double xo = (double)own[VN * q + v], yn = (double)t;
           sxx += xo * xo;
           sxy += xo * yn;
           syy += yn * yn;
         }
+      } else {
+#pragma unroll
+        for (int v = 0; v < VN; ++v) yv[v] = h[VN * q + v];
       }
-      stcs16(A.y + row, yv);
+      // B pieces: default L2 policy, so the neighbouring tile's half of the
+      // 32-byte sector joins it before the sector is written back
+      if (KIND == KIND_B) st16(A.y + row, yv);
+      else stcs16(A.y + row, yv);
     }
     __syncthreads();   // every thread is done with this buffer: the next prefetch may fill it
     cur ^= 1;
   }
-  if constexpr (KIND == KIND_B) hv_finish_dots<T, NWARP>(A, sxx, sxy, syy, wred);
+  if constexpr (KIND == KIND_A) hv_finish_dots<T, NWARP>(A, sxx, sxy, syy, wred);
 }
 
-// B pass: CTA sums of <x,x>, <x,y>, <y,y>, then the last CTA adds them up
+// A pass: CTA sums of <x,x>, <x,y>, <y,y>, then the last CTA adds them up
 template <typename T, int NWARP>
 __device__ __forceinline__ void hv_finish_dots(const TmaArgs<T> &A, double sxx, double sxy, double syy,
                                                double (*wred)[3]) {
@@ -746,17 +754,6 @@ __global__ void k_d2_8(int n, int64_t dim, const double *diagV, const double *de
   }
 }
 
-// out[(tile << tb) + l] = d[row of cell l of B tile `tile`]
-template <typename T>
-__global__ void k_d2_border(int64_t dim, int a, int tb, const T *d, T *out) {
-  constexpr int C = Cell<T>::CARRY;
-  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < dim;
-       q += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t tile = (uint32_t)(q >> tb);
-    const int l = (int)(q & (((int64_t)1 << tb) - 1));
-    out[q] = d[row_of<KIND_B, C>(a, tile, l)];
-  }
-}
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -773,11 +770,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // A map: {chunk cells (256 B), chunks, probes};
 // B map: {piece cells (2^C), 2^(a-C) tiles, 2^(n-a), probes}
 template <typename T>
-int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap *mA, CUtensorMap *mB) {
+int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap *mA, CUtensorMap *mB,
+              int C = Cell<T>::CARRY) {
   auto enc = encode_fn();
   if (!enc) return fail(ctx, EL_ECUDA, "cuTensorMapEncodeTiled unavailable");
   const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-  constexpr int C = Cell<T>::CARRY, LOGCH = Cell<T>::LOGCH;
+  constexpr int LOGCH = Cell<T>::LOGCH;
   const uint64_t dim = 1ull << n, cb = sizeof(T);
   const uint64_t e256 = 256 / cb, epc = 1ull << C;
   {
@@ -812,20 +810,20 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   const int64_t dim = h->basis->dim;
   const int ng = chunk / PU;
   const size_t vb = (size_t)dim * chunk * sizeof(T);
-  const size_t vbits_bytes = (size_t)EL_KPM_MAXN * EL_KPM_MAXN * sizeof(T);
-  char *buf = (char *)el::workspace(ctx, 6, 2 * vb + 2 * (size_t)dim * sizeof(T) + 256 + vbits_bytes);
+  // FP32: no diagonal array (formed in the kernel from V and delta, FP64);
+  // FP64: the d2 array, in row order
+  constexpr bool OTF = OnTheFly<T>::value;
+  const size_t dbytes = OTF ? 0 : (size_t)dim * sizeof(T);
+  const size_t vbits_bytes = (size_t)EL_KPM_MAXN * EL_KPM_MAXN * sizeof(double);
+  char *buf = (char *)el::workspace(ctx, 6, 2 * vb + dbytes + 256 + vbits_bytes);
   if (!buf) return EL_ENOMEM;
   void *P = buf, *Q = buf + vb;
-  T *d2 = reinterpret_cast<T *>(buf + 2 * vb);
-  T *d2b = d2 + dim;   // the same diagonal in B-tile order
-  int *d_err = reinterpret_cast<int *>(buf + 2 * vb + 2 * (size_t)dim * sizeof(T));
-  T *d_vbits = reinterpret_cast<T *>(buf + 2 * vb + 2 * (size_t)dim * sizeof(T) + 256);
-  {
-    std::vector<T> vb_host((size_t)n * n);
-    for (size_t i = 0; i < vb_host.size(); ++i) vb_host[i] = (T)h->Vbits[i];
-    EL_CUDA_TRY(ctx, el::copy(ctx, d_vbits, vb_host.data(), vb_host.size() * sizeof(T), cudaMemcpyHostToDevice));
-    EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));   // vb_host leaves scope
-  }
+  T *d2 = OTF ? nullptr : reinterpret_cast<T *>(buf + 2 * vb);
+  int *d_err = reinterpret_cast<int *>(buf + 2 * vb + dbytes);
+  double *d_vbits = reinterpret_cast<double *>(buf + 2 * vb + dbytes + 256);
+  if (OTF)
+    EL_CUDA_TRY(ctx, el::copy(ctx, d_vbits, h->Vbits.data(), (size_t)n * n * sizeof(double),
+                              cudaMemcpyHostToDevice));
   const int M = (num + 1) / 2;
   double *d_dots = (double *)el::workspace(ctx, 7, (size_t)(M + 1) * chunk * 2 * sizeof(double));
   if (!d_dots) return EL_ENOMEM;
@@ -835,7 +833,7 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     if (!d_probe8) return EL_ENOMEM;
   }
   EL_CUDA_TRY(ctx, cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
-  {
+  if (!OTF) {
     double *d_delta = (double *)el::workspace(ctx, 8, 64 * sizeof(double));
     if (!d_delta) return EL_ENOMEM;
     EL_CUDA_TRY(ctx, el::copy(ctx, d_delta, h->delta, 64 * sizeof(double), cudaMemcpyHostToDevice));
@@ -846,10 +844,6 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   const int amax = sizeof(T) == 4 ? 14 : 13;
   const int a = std::min(amax, std::max((n + C + 1) / 2, n + C - amax));
   const int TBA = a, TBB = n - a + C;
-  if (sizeof(T) == 4) {   // B-tile-ordered copy of the diagonal (see d2_index)
-    k_d2_border<T><<<el::grid_for(dim, 256), 256, 0, ctx->stream>>>(dim, a, TBB, d2, d2b);
-    EL_LAUNCH_CHECK(ctx);
-  }
   const int hb = (int)std::min<int64_t>(256, (int64_t)1 << (n - a));
   CUtensorMap mA[2], mB[2];   // [P buffer, Q buffer]
   int rc = make_maps<T>(ctx, P, n, a, ng, hb, &mA[0], &mB[0]);
@@ -858,8 +852,6 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   if (rc) return rc;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  int diag_otf = 0;
-  if (const char *ev = getenv("EL_KPM_DIAG")) diag_otf = atoi(ev);
   auto launch = [&](int kind, int mode, double s_m, int pbuf, double *dots) -> int {
     TmaArgs<T> A;
     memset(&A, 0, sizeof A);
@@ -870,17 +862,16 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     A.items = A.tiles * ng;
     A.log_tiles = 0;
     while (((int64_t)1 << A.log_tiles) < A.tiles) ++A.log_tiles;
-    A.diag_otf = diag_otf;
     A.vbits = d_vbits;
-    for (int k = 0; k < n && k < 32; ++k) A.delta_b[k] = (T)h->delta[k];
-    A.s2 = (T)(2.0 / r);
-    A.s2c = (T)(-2.0 * c / r);
+    for (int k = 0; k < n && k < 32; ++k) A.delta_b[k] = h->delta[k];
+    A.s2 = 2.0 / r;
+    A.s2c = -2.0 * c / r;
     A.s_m = (T)s_m; A.two_r = (T)(2.0 / r); A.pro_alpha = (T)0.5; A.pro_beta = (T)(1.0 / r);
     for (int k = 0; k < TB && k < 16; ++k) {
       int rowbit = (kind == KIND_A) ? k : (k >= C ? a + k - C : -1);
       A.amp[k] = (T)((rowbit >= 0) ? 0.5 * h->om_re[rowbit] : 0.0);
     }
-    A.d2 = (kind == KIND_B && sizeof(T) == 4) ? d2b : d2; A.dots = dots; A.err = d_err; A.counter = ctx->d_counter;
+    A.d2 = d2; A.dots = dots; A.err = d_err; A.counter = ctx->d_counter;
     const int grid = (int)std::min<int64_t>(A.items, sms);
     int e = el::ensure_partials(ctx, (size_t)grid * ng * PU * 2);
     if (e) return e;
@@ -1025,7 +1016,8 @@ int hv_tiled(el_ctx *ctx, el_ham *h, el_hv_plan *P, int ix, int iy, int iz, doub
   const int64_t dim = h->basis->dim;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  for (int kind = KIND_A; kind <= KIND_B; ++kind) {
+  for (int pass = 0; pass < 2; ++pass) {
+    const int kind = pass == 0 ? KIND_B : KIND_A;   // X_B x first, then the rest and the dots
     TmaArgs<T> A;
     memset(&A, 0, sizeof A);
     const int TB = kind == KIND_B ? n - a + C : a;
