@@ -1091,9 +1091,15 @@ int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap
     cuuint64_t gstr[3] = {epc * cb, (1ull << a) * cb, dim * cb};
     cuuint32_t box[4] = {(cuuint32_t)epc, 1, (cuuint32_t)hb, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
+    CUtensorMapL2promotion promo = CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+    if (const char *ev = getenv("EL_TMA_PROMO")) {
+      const int pv = atoi(ev);
+      promo = pv == 0 ? CU_TENSOR_MAP_L2_PROMOTION_NONE
+            : pv == 1 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
+            : pv == 2 ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B : CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+    }
     CUresult r = enc(mB, dt, 4, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                     CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(ctx, EL_ECUDA, "tensor map B encode failed (%d)", (int)r);
   }
   return EL_OK;
