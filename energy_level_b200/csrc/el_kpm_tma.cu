@@ -64,8 +64,10 @@ template <typename T>
 struct TmaArgs {
   int n, a, mode, ng, log_tiles, hb, nbox;
   // FP32 passes: the diagonal from tile sums instead of a d2 array (V
-  // between row bits [n][n] and delta per row bit, FP64), d2 = s2 d + s2c
+  // between row bits [n][n] and delta per row bit, FP64), d2 = s2 d + s2c;
+  // wtab: per tile, OTF_ROW doubles {wH_0 .. wH_{TB-1}, ..., cH}
   const double *vbits;
+  const double *wtab;
   double delta_b[32];
   double s2, s2c;
   int64_t dim, tiles, items;
@@ -135,6 +137,12 @@ __device__ __forceinline__ void tma_store3(const CUtensorMap *m, int c0, int c1,
 __device__ __forceinline__ void tma_store4(const CUtensorMap *m, int c0, int c1, int c2, int c3, const void *src) {
   asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
                ::"l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src)) : "memory");
+}
+// Untiled bulk copy global -> shared (16-byte aligned addresses, size a
+// multiple of 16), completing on the mbarrier of the tile it travels with.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void bulk_wait_read() {
@@ -209,6 +217,39 @@ __device__ __forceinline__ void gather_all(const T *S, int tid, const TmaArgs<T>
 // array (their registers have no room for the sums).
 template <typename T> struct OnTheFly { static constexpr bool value = sizeof(T) == 4; };
 
+// Per-tile couplings of the FP32 passes, one 128-byte row per tile:
+// slot k < TB holds wH_k = sum over the tile's set index bits i of
+// V(row bit of tile bit k, row bit of index bit i); the last slot holds cH,
+// the diagonal of the set index bits alone (their delta plus the V among
+// them); the slots between are zero.  The row travels with the tile's TMA
+// load, so no thread sums couplings while the others wait.
+constexpr int OTF_ROW = 16;
+struct DeltaBits { double v[32]; };
+
+template <int KIND, int C>
+__global__ void k_otf_table(int n, int a, int TB, int log_tiles, int64_t tiles, const double *__restrict__ vbits,
+                            DeltaBits delta, double *__restrict__ out) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= tiles * OTF_ROW) return;
+  const uint32_t tile = (uint32_t)(gid / OTF_ROW);
+  const int slot = (int)(gid % OTF_ROW);
+  double sacc = 0.0;
+  if (slot < TB) {
+    const int K = tile_rowbit<KIND, C>(a, slot);
+    for (int i = 0; i < log_tiles; ++i)
+      if ((tile >> i) & 1u) sacc += vbits[K * n + index_rowbit<KIND, C>(a, i)];
+  } else if (slot == OTF_ROW - 1) {
+    for (int i = 0; i < log_tiles; ++i) {
+      if (!((tile >> i) & 1u)) continue;
+      const int I = index_rowbit<KIND, C>(a, i);
+      sacc += delta.v[I];
+      for (int i2 = 0; i2 < i; ++i2)
+        if ((tile >> i2) & 1u) sacc += vbits[I * n + index_rowbit<KIND, C>(a, i2)];
+    }
+  }
+  out[gid] = sacc;
+}
+
 template <typename T, int KIND, int TB, int LNT>
 __device__ __forceinline__ void tile_diag(const TmaArgs<T> &A, uint32_t tile, int tid, double cT,
                                           const double *cTJ, const double *tJ, const double *wH, double cH,
@@ -269,8 +310,8 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
   __shared__ double sV[OTF ? EL_KPM_MAXN * EL_KPM_MAXN : 1];
   __shared__ double tJ[OTF ? R : 1];
   __shared__ double cTJ[OTF ? (RB > 0 ? RB : 1) * NT : 1];   // [k][tid]: couplings of the thread bits to register bit k
-  __shared__ double wH[16];
-  __shared__ double s_cH;
+  __shared__ __align__(16) double wHt[2][OTF_ROW];   // the table rows of the tiles in S buffers 0/1
+  constexpr unsigned WROW_BYTES = OTF ? OTF_ROW * sizeof(double) : 0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ndots = A.ng * PU * 2;
   const int nb = A.n;
@@ -325,8 +366,9 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
   int gacc = item_group(A, item);
   if (tid == 0 && item < A.items) {
     const uint32_t tile = item_tile(A, item);
-    mbar_expect(&bar[0], TILE_BYTES);
+    mbar_expect(&bar[0], TILE_BYTES + WROW_BYTES);
     tile_load<KIND>(A, Sb0, &mapQ, tile, gacc, &bar[0]);
+    if constexpr (OTF) bulk_load(wHt[0], A.wtab + (size_t)tile * OTF_ROW, WROW_BYTES, &bar[0]);
   }
   for (; item < A.items; item += gridDim.x) {
     const int g = item_group(A, item);
@@ -359,28 +401,6 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
     // the S store may still be reading Sn; in the prologue it is the only
     // group) and (2) every thread has finished the previous item, whose last
     // pass reads S2 after its final barrier.
-    if (OTF && warp == NWARP - 1) {
-      // this tile's couplings: wH_k = sum over set index bits i of V(k, i),
-      // cH = the diagonal of the index bits alone
-      if (lane < TB) {
-        const int K = tile_rowbit<KIND, C>(A.a, lane);
-        double sacc = 0.0;
-        for (int i = 0; i < A.log_tiles; ++i)
-          if ((tile >> i) & 1u) sacc += sV[K * nb + index_rowbit<KIND, C>(A.a, i)];
-        wH[lane] = sacc;
-      }
-      if (lane == 31) {
-        double sacc = 0.0;
-        for (int i = 0; i < A.log_tiles; ++i) {
-          if (!((tile >> i) & 1u)) continue;
-          const int I = index_rowbit<KIND, C>(A.a, i);
-          sacc += A.delta_b[I];
-          for (int i2 = 0; i2 < i; ++i2)
-            if ((tile >> i2) & 1u) sacc += sV[I * nb + index_rowbit<KIND, C>(A.a, i2)];
-        }
-        s_cH = sacc;
-      }
-    }
     if (tid == 0) {
       if (A.mode == MODE_PROLOGUE) bulk_wait_read<0>();
       else bulk_wait_read<1>();
@@ -409,8 +429,9 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
       const int gn = item_group(A, nxt);
       const uint32_t tn = item_tile(A, nxt);
       uint64_t *bn = cur ? &bar[0] : &bar[1];
-      mbar_expect(bn, TILE_BYTES);
+      mbar_expect(bn, TILE_BYTES + WROW_BYTES);
       tile_load<KIND>(A, Sn, &mapQ, tn, gn, bn);
+      if constexpr (OTF) bulk_load(wHt[cur ^ 1], A.wtab + (size_t)tn * OTF_ROW, WROW_BYTES, bn);
     }
     // per-tile products: two interleaved FP32 partial sums per quantity,
     // widened to FP64 once per tile
@@ -420,7 +441,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
     if (A.mode == MODE_PROLOGUE) {
       // p_1 = (D-c)/r t_0 + pro_beta X_G t_0 -> S2 -> P
       T dv[R];
-      tile_diag<T, KIND, TB, LNT>(A, tile, tid, cT, cTJ, tJ, wH, s_cH, d2, dv);
+      tile_diag<T, KIND, TB, LNT>(A, tile, tid, cT, cTJ, tJ, wHt[cur], wHt[cur][OTF_ROW - 1], d2, dv);
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         const int l = tid + NT * j;
@@ -455,7 +476,7 @@ k_kpm_tma(const TmaArgs<T> A, const __grid_constant__ CUtensorMap mapP,
         // the diagonal of this thread's rows, loaded before the gathers so
         // that its latency hides behind them
         T dv[R];
-        tile_diag<T, KIND, TB, LNT>(A, tile, tid, cT, cTJ, tJ, wH, s_cH, d2, dv);
+        tile_diag<T, KIND, TB, LNT>(A, tile, tid, cT, cTJ, tJ, wHt[cur], wHt[cur][OTF_ROW - 1], d2, dv);
         U h2[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) h2[j] = z8(U{});
@@ -816,16 +837,37 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   // FP64: the d2 array, in row order
   constexpr bool OTF = OnTheFly<T>::value;
   const size_t dbytes = OTF ? 0 : (size_t)dim * sizeof(T);
-  const size_t vbits_bytes = (size_t)EL_KPM_MAXN * EL_KPM_MAXN * sizeof(double);
-  char *buf = (char *)el::workspace(ctx, 6, 2 * vb + dbytes + 256 + vbits_bytes);
+  // a: A-tile bits; the B tile has n - a + C bits; both at most 64 KB
+  const int amax = sizeof(T) == 4 ? 14 : 13;
+  const int a = std::min(amax, std::max((n + C + 1) / 2, n + C - amax));
+  const int TBA = a, TBB = n - a + C;
+  const int64_t tilesA = dim >> a, tilesB = (int64_t)1 << (a - C);
+  const size_t vbits_bytes = 5120;   // EL_KPM_MAXN^2 doubles, rounded up to 256 bytes
+  static_assert(EL_KPM_MAXN * EL_KPM_MAXN * sizeof(double) <= 5120, "V table slot");
+  const size_t wtab_bytes = OTF ? (size_t)(tilesA + tilesB) * OTF_ROW * sizeof(double) : 0;
+  char *buf = (char *)el::workspace(ctx, 6, 2 * vb + dbytes + 256 + vbits_bytes + wtab_bytes);
   if (!buf) return EL_ENOMEM;
   void *P = buf, *Q = buf + vb;
   T *d2 = OTF ? nullptr : reinterpret_cast<T *>(buf + 2 * vb);
   int *d_err = reinterpret_cast<int *>(buf + 2 * vb + dbytes);
   double *d_vbits = reinterpret_cast<double *>(buf + 2 * vb + dbytes + 256);
-  if (OTF)
+  double *d_wtab[2] = {nullptr, nullptr};   // [KIND_A, KIND_B]
+  if constexpr (OTF) {
+    d_wtab[KIND_A] = reinterpret_cast<double *>(buf + 2 * vb + dbytes + 256 + vbits_bytes);
+    d_wtab[KIND_B] = d_wtab[KIND_A] + tilesA * OTF_ROW;
     EL_CUDA_TRY(ctx, el::copy(ctx, d_vbits, h->Vbits.data(), (size_t)n * n * sizeof(double),
                               cudaMemcpyHostToDevice));
+    DeltaBits db;
+    memset(&db, 0, sizeof db);
+    for (int k = 0; k < n && k < 32; ++k) db.v[k] = h->delta[k];
+    auto lg = [](int64_t t) { int l = 0; while (((int64_t)1 << l) < t) ++l; return l; };
+    k_otf_table<KIND_A, C><<<el::grid_for(tilesA * OTF_ROW, 256), 256, 0, ctx->stream>>>(
+        n, a, TBA, lg(tilesA), tilesA, d_vbits, db, d_wtab[KIND_A]);
+    EL_LAUNCH_CHECK(ctx);
+    k_otf_table<KIND_B, C><<<el::grid_for(tilesB * OTF_ROW, 256), 256, 0, ctx->stream>>>(
+        n, a, TBB, lg(tilesB), tilesB, d_vbits, db, d_wtab[KIND_B]);
+    EL_LAUNCH_CHECK(ctx);
+  }
   const int M = (num + 1) / 2;
   double *d_dots = (double *)el::workspace(ctx, 7, (size_t)(M + 1) * chunk * 2 * sizeof(double));
   if (!d_dots) return EL_ENOMEM;
@@ -842,10 +884,6 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     k_d2_8<T><<<el::grid_for(dim, 256), 256, 0, ctx->stream>>>(n, dim, h->d_diagV64, d_delta, c, r, d2);
     EL_LAUNCH_CHECK(ctx);
   }
-  // a: A-tile bits; the B tile has n - a + C bits; both at most 64 KB
-  const int amax = sizeof(T) == 4 ? 14 : 13;
-  const int a = std::min(amax, std::max((n + C + 1) / 2, n + C - amax));
-  const int TBA = a, TBB = n - a + C;
   const int hb = (int)std::min<int64_t>(256, (int64_t)1 << (n - a));
   CUtensorMap mA[2], mB[2];   // [P buffer, Q buffer]
   int rc = make_maps<T>(ctx, P, n, a, ng, hb, &mA[0], &mB[0]);
@@ -860,11 +898,12 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     const int TB = kind == KIND_B ? TBB : TBA;
     A.n = n; A.a = a; A.mode = mode; A.ng = ng; A.dim = dim; A.hb = hb;
     A.nbox = (int)(((int64_t)1 << (n - a)) / hb);
-    A.tiles = kind == KIND_A ? (dim >> a) : ((int64_t)1 << (a - C));
+    A.tiles = kind == KIND_A ? tilesA : tilesB;
     A.items = A.tiles * ng;
     A.log_tiles = 0;
     while (((int64_t)1 << A.log_tiles) < A.tiles) ++A.log_tiles;
     A.vbits = d_vbits;
+    A.wtab = d_wtab[kind];
     for (int k = 0; k < n && k < 32; ++k) A.delta_b[k] = h->delta[k];
     A.s2 = 2.0 / r;
     A.s2c = -2.0 * c / r;
