@@ -14,7 +14,7 @@
 //   - a B tile holds the C lowest row bits as a contiguous piece of 32 bytes
 //     (C = 3 for FP32: one DRAM sector) or 16 bytes (C = 1 for FP64), carried
 //     but not flipped, plus row bits a..N-1; its 2^(N-a) pieces lie 2^a rows
-//     apart and are fetched as boxes of 256 pieces.  The tile index
+//     apart and move as one 5-D box (one TMA instruction).  The tile index
 //     enumerates row bits C..a-1.  a = 14 (FP32) / 13 (FP64) at N = 25 keeps
 //     both tiles at 64 KB;
 //   - the t_{m-1} tile of the next work item is prefetched into a second
@@ -42,7 +42,6 @@ template <typename T> struct Cell {
   static constexpr int PU = 1;
   static constexpr int CARRY = sizeof(T) == 4 ? 3 : 1;
   static constexpr int LOGCH = sizeof(T) == 4 ? 6 : 5;
-  static constexpr int PIECE = (1 << CARRY) * (int)sizeof(T);   // bytes
 };
 
 __device__ __forceinline__ float z8(float) { return 0.f; }
@@ -62,7 +61,7 @@ enum { MODE_STEP = 0, MODE_PROLOGUE = 1, MODE_LAST = 2 };
 
 template <typename T>
 struct TmaArgs {
-  int n, a, mode, ng, log_tiles, hb, nbox;
+  int n, a, mode, ng, log_tiles;
   // FP32 passes: the diagonal from tile sums instead of a d2 array (V
   // between row bits [n][n] and delta per row bit, FP64), d2 = s2 d + s2c;
   // wtab: per tile, OTF_ROW doubles {wH_0 .. wH_{TB-1}, ..., cH}
@@ -125,18 +124,20 @@ __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, int c
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
       ::"r"(smem_u32(dst)), "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar)) : "memory");
 }
-__device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3, uint64_t *bar) {
+__device__ __forceinline__ void tma_load5(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3, int c4,
+                                          uint64_t *bar) {
   asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
-      ::"r"(smem_u32(dst)), "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar)) : "memory");
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+      ::"r"(smem_u32(dst)), "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ void tma_store3(const CUtensorMap *m, int c0, int c1, int c2, const void *src) {
   asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];"
                ::"l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src)) : "memory");
 }
-__device__ __forceinline__ void tma_store4(const CUtensorMap *m, int c0, int c1, int c2, int c3, const void *src) {
-  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
-               ::"l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src)) : "memory");
+__device__ __forceinline__ void tma_store5(const CUtensorMap *m, int c0, int c1, int c2, int c3, int c4,
+                                           const void *src) {
+  asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];"
+               ::"l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(src)) : "memory");
 }
 // Untiled bulk copy global -> shared (16-byte aligned addresses, size a
 // multiple of 16), completing on the mbarrier of the tile it travels with.
@@ -152,16 +153,15 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Tile <-> tensor-map coordinates.  A: 3-D map {256-byte chunk, chunk index,
-// probe}; B: 4-D map {low-bit piece, tile, h, probe}.
-template <int KIND, typename T, int CR = Cell<T>::CARRY>
+// probe}; B: 5-D map {low-bit piece, tile, h_lo, h_hi, probe}, one box per
+// tile (h = the row bits above a, split so that no box side exceeds 256).
+template <int KIND, typename T>
 __device__ __forceinline__ void tile_load(const TmaArgs<T> &A, void *dst, const CUtensorMap *m,
                                           uint32_t tile, int g, uint64_t *bar) {
   if (KIND == KIND_A) {
     tma_load3(dst, m, 0, (int)(tile << (A.a - Cell<T>::LOGCH)), g, bar);
   } else {
-    constexpr int PIECE = (1 << CR) * (int)sizeof(T);
-    for (int k = 0; k < A.nbox; ++k)
-      tma_load4((char *)dst + (size_t)k * A.hb * PIECE, m, 0, (int)tile, k * A.hb, g, bar);
+    tma_load5(dst, m, 0, (int)tile, 0, 0, g, bar);
   }
 }
 template <int KIND, typename T>
@@ -170,8 +170,7 @@ __device__ __forceinline__ void tile_store(const TmaArgs<T> &A, const CUtensorMa
   if (KIND == KIND_A) {
     tma_store3(m, 0, (int)(tile << (A.a - Cell<T>::LOGCH)), g, src);
   } else {
-    for (int k = 0; k < A.nbox; ++k)
-      tma_store4(m, 0, (int)tile, k * A.hb, g, (const char *)src + (size_t)k * A.hb * Cell<T>::PIECE);
+    tma_store5(m, 0, (int)tile, 0, 0, g, src);
   }
 }
 
@@ -788,7 +787,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // A map: {chunk cells (256 B), chunks, probes};
-// B map: {piece cells (2^C), 2^(a-C) tiles, 2^(n-a), probes}
+// B map: {piece cells (2^C), 2^(a-C) tiles, hb, 2^(n-a) / hb, probes}
 template <typename T>
 int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap *mA, CUtensorMap *mB,
               int C = Cell<T>::CARRY) {
@@ -809,14 +808,15 @@ int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap
     if (r != CUDA_SUCCESS) return fail(ctx, EL_ECUDA, "tensor map A encode failed (%d)", (int)r);
   }
   {
-    cuuint64_t gdim[4] = {epc, 1ull << (a - C), 1ull << (n - a), (cuuint64_t)ng};
-    cuuint64_t gstr[3] = {epc * cb, (1ull << a) * cb, dim * cb};
-    cuuint32_t box[4] = {(cuuint32_t)epc, 1, (cuuint32_t)hb, 1};
-    cuuint32_t es[4] = {1, 1, 1, 1};
+    const uint64_t hhi = (1ull << (n - a)) / (uint64_t)hb;
+    cuuint64_t gdim[5] = {epc, 1ull << (a - C), (cuuint64_t)hb, hhi, (cuuint64_t)ng};
+    cuuint64_t gstr[4] = {epc * cb, (1ull << a) * cb, (uint64_t)hb * (1ull << a) * cb, dim * cb};
+    cuuint32_t box[5] = {(cuuint32_t)epc, 1, (cuuint32_t)hb, (cuuint32_t)hhi, 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
     // 256-byte L2 promotion: a 32-byte piece brings the pieces of the next
     // tiles, which the neighbouring CTAs are about to load (measured best
     // of none / 64 / 128 / 256 bytes)
-    CUresult r = enc(mB, dt, 4, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+    CUresult r = enc(mB, dt, 5, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(ctx, EL_ECUDA, "tensor map B encode failed (%d)", (int)r);
@@ -896,8 +896,7 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     TmaArgs<T> A;
     memset(&A, 0, sizeof A);
     const int TB = kind == KIND_B ? TBB : TBA;
-    A.n = n; A.a = a; A.mode = mode; A.ng = ng; A.dim = dim; A.hb = hb;
-    A.nbox = (int)(((int64_t)1 << (n - a)) / hb);
+    A.n = n; A.a = a; A.mode = mode; A.ng = ng; A.dim = dim;
     A.tiles = kind == KIND_A ? tilesA : tilesB;
     A.items = A.tiles * ng;
     A.log_tiles = 0;
@@ -1062,8 +1061,7 @@ int hv_tiled(el_ctx *ctx, el_ham *h, el_hv_plan *P, int ix, int iy, int iz, doub
     TmaArgs<T> A;
     memset(&A, 0, sizeof A);
     const int TB = kind == KIND_B ? n - a + C : a;
-    A.n = n; A.a = a; A.ng = 1; A.dim = dim; A.hb = P->hb;
-    A.nbox = (int)(((int64_t)1 << (n - a)) / P->hb);
+    A.n = n; A.a = a; A.ng = 1; A.dim = dim;
     A.tiles = kind == KIND_A ? (dim >> a) : ((int64_t)1 << (a - C));
     A.items = A.tiles;
     for (int k = 0; k < TB && k < 16; ++k) {
