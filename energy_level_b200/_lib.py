@@ -64,6 +64,8 @@ PROTOTYPES = {
                                     C.c_int, C.c_int, _dp, _dp, _ip, _ip, _vp]),
     "el_batch_create": (C.c_int, [_vp, C.c_int, _vp, _vp, _dp, _dp, _vp, _vp, _vp, _dp, C.c_int, C.c_int,
                                   C.c_double, C.POINTER(_vp)]),
+    "el_batch_create_graph": (C.c_int, [_vp, C.c_int, _vp, _vp, _dp, _dp, _vp, _vp, _vp, _dp, _vp, _vp, _vp,
+                                        C.c_int, C.c_int, C.c_double, C.POINTER(_vp)]),
     "el_batch_run": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _u64]),
     "el_batch_run_coop": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _u64]),
     "el_batch_set_wait_limit": (C.c_int, [_vp, _vp, C.c_int32]),

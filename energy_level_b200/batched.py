@@ -23,31 +23,41 @@ _TUNED = {}
 
 
 def _layout(n, edges):
+    """Basis layout of one instance: the full basis without edges, the
+    arithmetic Zeckendorf layouts for a nearest-neighbour path or cycle, and
+    a code table for any other blockade graph.  Returns (layout, edge list)."""
     if not edges:
-        return _lib.EL_LAYOUT_FULL
+        return _lib.EL_LAYOUT_FULL, []
     es = sorted({tuple(sorted((int(a), int(b)))) for a, b in edges})
+    for a, b in es:
+        if a == b or a < 0 or b >= n:
+            raise ValueError('bad blockade edge (%d, %d) for %d sites' % (a, b, n))
     chain = [(i, i + 1) for i in range(n - 1)]
     if es == chain:
-        return _lib.EL_LAYOUT_CHAIN
+        return _lib.EL_LAYOUT_CHAIN, es
     if n >= 3 and es == sorted(chain + [(0, n - 1)]):
-        return _lib.EL_LAYOUT_RING
-    raise ValueError('batched solves support nearest-neighbour chain/ring blockade sectors '
-                     'or full bases')
+        return _lib.EL_LAYOUT_RING, es
+    return _lib.EL_LAYOUT_TABLE, es
 
 
 def pack_instances(instances):
-    """Host arrays of el_batch_create for a list of instances: [n int32,
-    layout int32, Omega float64 (concatenated), delta float64, pair offsets
-    int32 [count + 1], i int32, j int32, V float64] (one dummy entry where a
-    list is empty).  Raises the model's errors for an invalid instance."""
+    """Host arrays of el_batch_create_graph for a list of instances: [n
+    int32, layout int32, Omega float64 (concatenated), delta float64, pair
+    offsets int32 [count + 1], i int32, j int32, V float64, edge offsets
+    int32 [count + 1], edge ends int32, int32] (one dummy entry where a list
+    is empty).  Raises the model's errors for an invalid instance."""
     ns, lays, om, de, npair, pi, pj, V = [], [], [], [], [], [], [], []
+    nedge, ea, eb = [], [], []
     for inst in instances:
         n, o, d, (i, j, v) = model_columns(inst['calib'], inst.get('Om'), inst.get('delta'),
                                            inst.get('gamma'), inst.get('terms'))
         if np.any(o.imag != 0):
             raise ValueError('batched solves need real Omega')
         ns.append(n)
-        lays.append(_layout(n, inst.get('edges')))
+        lay, es = _layout(n, inst.get('edges'))
+        lays.append(lay)
+        ea.append([a for a, _ in es]); eb.append([b for _, b in es])
+        nedge.append(len(es))
         om.append(o.real)
         de.append(d)
         pi.append(i); pj.append(j); V.append(v)
@@ -55,8 +65,10 @@ def pack_instances(instances):
     arr = lambda x, t: np.ascontiguousarray(np.asarray(x, dtype=t))
     cat = lambda x, t, empty: arr(np.concatenate(x) if sum(map(len, x)) else [empty], t)
     poff = np.concatenate([[0], np.cumsum(npair, dtype=np.int64)])
+    eoff = np.concatenate([[0], np.cumsum(nedge, dtype=np.int64)])
     return [arr(ns, np.int32), arr(lays, np.int32), cat(om, np.float64, 0.0), cat(de, np.float64, 0.0),
-            arr(poff, np.int32), cat(pi, np.int32, 0), cat(pj, np.int32, 0), cat(V, np.float64, 0.0)]
+            arr(poff, np.int32), cat(pi, np.int32, 0), cat(pj, np.int32, 0), cat(V, np.float64, 0.0),
+            arr(eoff, np.int32), cat(ea, np.int32, 0), cat(eb, np.int32, 0)]
 
 
 class BatchedGroundStates:
@@ -77,11 +89,12 @@ class BatchedGroundStates:
         self.tol = float(tol if tol is not None else (1e-5 if dtype == 'float32' else 1e-10))
         k = self._keep
         h = C.c_void_p()
-        self.ctx.call('el_batch_create', C.c_int(self.count), C.c_void_p(k[0].ctypes.data),
+        self.ctx.call('el_batch_create_graph', C.c_int(self.count), C.c_void_p(k[0].ctypes.data),
                       C.c_void_p(k[1].ctypes.data), _lib.dptr(k[2]), _lib.dptr(k[3]),
                       C.c_void_p(k[4].ctypes.data), C.c_void_p(k[5].ctypes.data),
-                      C.c_void_p(k[6].ctypes.data), _lib.dptr(k[7]), C.c_int(_lib.DTYPES[dtype]),
-                      C.c_int(int(max_iter)), C.c_double(self.tol), C.byref(h))
+                      C.c_void_p(k[6].ctypes.data), _lib.dptr(k[7]), C.c_void_p(k[8].ctypes.data),
+                      C.c_void_p(k[9].ctypes.data), C.c_void_p(k[10].ctypes.data),
+                      C.c_int(_lib.DTYPES[dtype]), C.c_int(int(max_iter)), C.c_double(self.tol), C.byref(h))
         self.handle = h
         self.occupations = bool(occupations)
         if self.occupations:

@@ -13,7 +13,9 @@
 // iteration on one thread.  Convergence: residual estimate of both pairs
 // <= tol * max(1, |theta|).  H follows channels.py:58-132 (diagonal
 // delta n + V n n, sigma^x with Omega/2) on nearest-neighbour chain / ring
-// blockade sectors (Zeckendorf ranking) or full bases; this is the batched
+// blockade sectors (Zeckendorf ranking), full bases, or the blockade sector
+// of any graph (TABLE: the instance's independent sets as an ascending code
+// list, and a flip table of target rows built once at set-up); this is the batched
 // counterpart of the reference's dense batched_ground_state
 // (equilibrium.py:251-311) and of per-instance eigsh calls (eq_route.py:540).
 #include "el_internal.cuh"
@@ -32,6 +34,11 @@ struct Inst {
   int n, layout, pad0, pad1;
   int64_t dim, off;             // rows and offset into the concatenated diagonal
   double om[MAXN];              // Omega/2 per bit position
+  // TABLE layout: this instance's ascending codes [dim] and flip table
+  // [n][dim] (target row of flipping bit k of row r, -1 where the blockade
+  // forbids it); null for the arithmetic layouts
+  const uint64_t *codes;
+  const int32_t *tgt;
 };
 
 struct BatchArgs {
@@ -166,6 +173,7 @@ __device__ double last_component(const double *a, const double *b, int m, double
 
 __device__ __forceinline__ uint64_t unrank_b(const Inst &I, const uint64_t *fib, int64_t row) {
   if (I.layout == EL_LAYOUT_FULL) return (uint64_t)row;
+  if (I.layout == EL_LAYOUT_TABLE) return I.codes[row];
   uint64_t r = (uint64_t)row, c = 0;
   const int n = I.n;
   if (I.layout == EL_LAYOUT_CHAIN) {
@@ -200,6 +208,7 @@ __device__ __forceinline__ int64_t flip_b(const Inst &I, const uint64_t *fib, ui
   const uint64_t bit = 1ULL << k;
   const bool set = (code & bit) != 0;
   if (I.layout == EL_LAYOUT_FULL) return row ^ (int64_t)bit;
+  if (I.layout == EL_LAYOUT_TABLE) return (int64_t)I.tgt[(int64_t)k * I.dim + row];
   const int n = I.n;
   uint64_t adj = 0;
   if (k + 1 < n) adj |= bit << 1;
@@ -833,6 +842,35 @@ __global__ void __launch_bounds__(NT) k_lanczos_coop(const CoopArgs G) {
   }
 }
 
+// Flip tables of the TABLE instances: target row of flipping bit k of row r,
+// found by binary search in the instance's ascending code list; -1 when bit
+// k is clear and one of its graph neighbours (adj, by bit position) is set.
+__global__ void k_batch_flip_table(int count, const Inst *inst, const uint64_t *adj) {
+  for (int i = blockIdx.y; i < count; i += gridDim.y) {
+    const Inst &I = inst[i];
+    if (I.layout != EL_LAYOUT_TABLE) continue;
+    const int64_t cells = I.dim * I.n;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < cells;
+         e += (int64_t)gridDim.x * blockDim.x) {
+      const int k = (int)(e / I.dim);
+      const int64_t r = e - (int64_t)k * I.dim;
+      const uint64_t code = I.codes[r], bit = 1ULL << k;
+      int32_t t = -1;
+      if ((code & bit) || !(code & adj[(size_t)i * MAXN + k])) {
+        const uint64_t want = code ^ bit;
+        int64_t lo = 0, hi = I.dim - 1;
+        while (lo < hi) {
+          const int64_t mid = (lo + hi) >> 1;
+          if (I.codes[mid] < want) lo = mid + 1;
+          else hi = mid;
+        }
+        if (I.codes[lo] == want) t = (int32_t)lo;
+      }
+      const_cast<int32_t *>(I.tgt)[e] = t;
+    }
+  }
+}
+
 // diagonal of every instance: V part + delta part, concatenated
 __global__ void k_batch_diag(int count, const Inst *inst, const double *Vmats, const double *deltas,
                              double *diag) {
@@ -892,7 +930,33 @@ struct el_batch_impl {
   double *c_part = nullptr;
   unsigned *c_sync = nullptr;       // [0] arrival counter, [1] error flag
   int c_nctas = 0;
+  // TABLE instances: concatenated ascending codes and flip tables
+  uint64_t *d_codes = nullptr;
+  int32_t *d_tgt = nullptr;
 };
+
+// Independent sets of a graph on n bit positions (adjb[k]: the neighbours
+// of bit k) in ascending code order: bits are decided from the top down,
+// clear before set, and a bit is set only when no decided neighbour is.
+// Returns false as soon as there are more than `limit`.
+struct IndepSets {
+  int n;
+  const uint64_t *adjb;
+  int64_t limit;
+  std::vector<uint64_t> *out;
+  bool walk(int k, uint64_t code) {
+    if (k < 0) {
+      if ((int64_t)out->size() >= limit) return false;
+      out->push_back(code);
+      return true;
+    }
+    if (!walk(k - 1, code)) return false;
+    if (!(code & adjb[k]) && !walk(k - 1, code | (1ULL << k))) return false;
+    return true;
+  }
+};
+
+constexpr int64_t TABLE_MAX_ROWS = 1LL << 24;   // rows of one TABLE instance
 
 }  // namespace
 
@@ -904,6 +968,15 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
                     const double *omega, const double *delta, const int32_t *pair_off,
                     const int32_t *pi, const int32_t *pj, const double *V, int dtype,
                     int max_iter, double tol, el_batch **out) {
+  return el_batch_create_graph(ctx, count, n_sites, layouts, omega, delta, pair_off, pi, pj, V, nullptr,
+                               nullptr, nullptr, dtype, max_iter, tol, out);
+}
+
+int el_batch_create_graph(el_ctx *ctx, int count, const int32_t *n_sites, const int32_t *layouts,
+                          const double *omega, const double *delta, const int32_t *pair_off,
+                          const int32_t *pi, const int32_t *pj, const double *V, const int32_t *edge_off,
+                          const int32_t *ei, const int32_t *ej, int dtype, int max_iter, double tol,
+                          el_batch **out) {
   if (!ctx || !out || count < 1 || !n_sites || !layouts || !omega || !delta || !pair_off) return EL_EINVAL;
   *out = nullptr;
   if (dtype != EL_F32 && dtype != EL_F64) return fail(ctx, EL_EINVAL, "batched Lanczos vectors must be EL_F32 or EL_F64");
@@ -914,12 +987,36 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
       return fail(ctx, EL_EINVAL, "pair offsets must be non-negative and non-decreasing (instance %d)", i);
   if (pair_off[count] > pair_off[0] && (!pi || !pj || !V))
     return fail(ctx, EL_EINVAL, "pair arrays missing for %d pairs", pair_off[count] - pair_off[0]);
+  if (edge_off)
+    for (int i = 0; i < count; ++i)
+      if (edge_off[i] < 0 || edge_off[i + 1] < edge_off[i])
+        return fail(ctx, EL_EINVAL, "edge offsets must be non-negative and non-decreasing (instance %d)", i);
+  if (edge_off && edge_off[count] > edge_off[0] && (!ei || !ej))
+    return fail(ctx, EL_EINVAL, "edge arrays missing for %d edges", edge_off[count] - edge_off[0]);
   EL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   std::vector<int64_t> dims(count);
+  // TABLE instances: neighbours by bit position and the ascending code list
+  std::vector<uint64_t> adjb((size_t)count * MAXN, 0);
+  std::vector<std::vector<uint64_t>> tcodes(count);
   for (int i = 0; i < count; ++i) {
     const int n = n_sites[i];
     if (n < 1 || n > MAXN) return fail(ctx, EL_EINVAL, "instance %d: n must be in [1, %d]", i, MAXN);
-    if (layouts[i] == EL_LAYOUT_CHAIN) dims[i] = (int64_t)fibh(n + 2);
+    if (layouts[i] == EL_LAYOUT_TABLE) {
+      if (!edge_off) return fail(ctx, EL_EINVAL, "instance %d: a TABLE (graph blockade) instance needs its edges", i);
+      for (int q = edge_off[i]; q < edge_off[i + 1]; ++q) {
+        const int a = ei[q], c = ej[q];
+        if (a < 0 || c < 0 || a >= n || c >= n || a == c)
+          return fail(ctx, EL_EINVAL, "instance %d: bad edge (%d, %d)", i, a, c);
+        const int qa = n - 1 - a, qc = n - 1 - c;
+        adjb[(size_t)i * MAXN + qa] |= 1ULL << qc;
+        adjb[(size_t)i * MAXN + qc] |= 1ULL << qa;
+      }
+      IndepSets w{n, &adjb[(size_t)i * MAXN], TABLE_MAX_ROWS, &tcodes[i]};
+      if (!w.walk(n - 1, 0))
+        return fail(ctx, EL_EINVAL, "instance %d: blockade sector larger than %lld rows", i,
+                    (long long)TABLE_MAX_ROWS);
+      dims[i] = (int64_t)tcodes[i].size();
+    } else if (layouts[i] == EL_LAYOUT_CHAIN) dims[i] = (int64_t)fibh(n + 2);
     else if (layouts[i] == EL_LAYOUT_RING) {
       if (n < 3) return fail(ctx, EL_EINVAL, "instance %d: ring needs n >= 3", i);
       dims[i] = (int64_t)(fibh(n + 1) + fibh(n - 1));
@@ -927,7 +1024,7 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
       if (n > 24) return fail(ctx, EL_EINVAL, "instance %d: full basis in a batch limited to n <= 24", i);
       dims[i] = 1LL << n;
     } else {
-      return fail(ctx, EL_EINVAL, "instance %d: layout must be chain, ring or full", i);
+      return fail(ctx, EL_EINVAL, "instance %d: layout must be chain, ring, full or table", i);
     }
   }
   el_batch *b = new el_batch();
@@ -969,9 +1066,37 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
     b->dim_max = std::max(b->dim_max, dims[i]);
   }
   b->total_rows = off;
+  // TABLE instances: codes and flip tables, concatenated in processing order
+  int64_t tab_rows = 0, tab_cells = 0;
+  for (int p = 0; p < count; ++p) {
+    const int i = b->order[p];
+    if (layouts[i] != EL_LAYOUT_TABLE) continue;
+    tab_rows += dims[i];
+    tab_cells += dims[i] * n_sites[i];
+  }
   double *d_V = nullptr, *d_D = nullptr;
+  uint64_t *d_adj = nullptr;
   cudaError_t e = cudaSuccess;
-  if (rc == EL_OK) do {
+  if (rc == EL_OK && tab_rows > 0) do {
+    if ((e = cudaMalloc(&b->d_codes, (size_t)tab_rows * 8)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&b->d_tgt, (size_t)tab_cells * 4)) != cudaSuccess) break;
+    std::vector<uint64_t> adjp((size_t)count * MAXN, 0);
+    int64_t co = 0, to = 0;
+    for (int p = 0; p < count && e == cudaSuccess; ++p) {
+      const int i = b->order[p];
+      for (int k = 0; k < MAXN; ++k) adjp[(size_t)p * MAXN + k] = adjb[(size_t)i * MAXN + k];
+      if (layouts[i] != EL_LAYOUT_TABLE) continue;
+      inst[p].codes = b->d_codes + co;
+      inst[p].tgt = b->d_tgt + to;
+      e = el::copy(ctx, b->d_codes + co, tcodes[i].data(), (size_t)dims[i] * 8, cudaMemcpyHostToDevice);
+      co += dims[i];
+      to += dims[i] * n_sites[i];
+    }
+    if (e != cudaSuccess) break;
+    if ((e = cudaMalloc(&d_adj, adjp.size() * 8)) != cudaSuccess) break;
+    e = el::copy(ctx, d_adj, adjp.data(), adjp.size() * 8, cudaMemcpyHostToDevice);
+  } while (0);
+  if (rc == EL_OK && e == cudaSuccess) do {
     if ((e = cudaMalloc(&b->d_inst, sizeof(Inst) * count)) != cudaSuccess) break;
     if ((e = cudaMalloc(&b->d_diag, (size_t)off * 8)) != cudaSuccess) break;
     if ((e = cudaMalloc(&b->d_out, (size_t)count * 4 * 8)) != cudaSuccess) break;
@@ -982,6 +1107,11 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
     if ((e = el::copy(ctx, b->d_inst, inst.data(), sizeof(Inst) * count, cudaMemcpyHostToDevice)) != cudaSuccess) break;
     if ((e = el::copy(ctx, d_V, Vm.data(), Vm.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
     if ((e = el::copy(ctx, d_D, Dl.data(), Dl.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+    if (tab_rows > 0) {
+      k_batch_flip_table<<<dim3(256, std::min(count, 1024)), 256, 0, ctx->stream>>>(count, b->d_inst, d_adj);
+      ctx->launches++;
+      if ((e = cudaGetLastError()) != cudaSuccess) break;
+    }
     k_batch_diag<<<dim3(64, std::min(count, 1024)), 256, 0, ctx->stream>>>(count, b->d_inst, d_V, d_D, b->d_diag);
     ctx->launches++;
     if ((e = cudaGetLastError()) != cudaSuccess) break;
@@ -989,6 +1119,7 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
   } while (0);
   if (d_V) cudaFree(d_V);
   if (d_D) cudaFree(d_D);
+  if (d_adj) cudaFree(d_adj);
   if (rc == EL_OK && e != cudaSuccess) rc = el::cuda_fail(ctx, e, "el_batch_create");
   if (rc != EL_OK) { el_batch_destroy(b); return rc; }
   *out = b;
@@ -1196,6 +1327,8 @@ int el_batch_destroy(el_batch *b) {
   if (b->c_part) cudaFree(b->c_part);
   if (b->c_sync) cudaFree(b->c_sync);
   if (b->d_nat) cudaFree(b->d_nat);
+  if (b->d_codes) cudaFree(b->d_codes);
+  if (b->d_tgt) cudaFree(b->d_tgt);
   delete b;
   return EL_OK;
 }

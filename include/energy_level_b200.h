@@ -230,6 +230,19 @@ int el_batch_create(el_ctx *ctx, int count, const int32_t *n_sites, const int32_
                     const double *omega, const double *delta, const int32_t *pair_off,
                     const int32_t *pi, const int32_t *pj, const double *V, int dtype,
                     int max_iter, double tol, el_batch **out);
+/* As el_batch_create, and layouts[i] may also be EL_LAYOUT_TABLE: the
+ * blockade sector of an arbitrary graph, whose edges (site indices) are
+ * ei/ej[edge_off[i] .. edge_off[i+1]) (edges of other layouts are ignored).
+ * The sector's independent sets are enumerated on the host (at most 2^24
+ * rows per instance, else EL_EINVAL) and a flip table of target rows
+ * (4 bytes per row and site) is built on the device once.  The batched
+ * ground state of the reference for any blockade graph
+ * (equilibrium.py:251-311 with the plan of hamiltonian_plan.py:15-50). */
+int el_batch_create_graph(el_ctx *ctx, int count, const int32_t *n_sites, const int32_t *layouts,
+                          const double *omega, const double *delta, const int32_t *pair_off,
+                          const int32_t *pi, const int32_t *pj, const double *V, const int32_t *edge_off,
+                          const int32_t *ei, const int32_t *ej, int dtype, int max_iter, double tol,
+                          el_batch **out);
 /* Queue the whole batch as ONE persistent launch (CTAs pull instances from an
  * atomic queue, largest first).  threads: 256/512/1024 per CTA; ctas_per_sm:
  * 1 or 2.  Asynchronous and capturable in a CUDA graph once a first run has

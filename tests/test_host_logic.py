@@ -253,9 +253,14 @@ def test_pack_instances_matches_calib_pairs():
     insts.append(dict(calib=lone, Om=np.full(2, 2.0), delta=np.zeros(2), edges=None))
     k = batched.pack_instances(insts)
     assert [a.dtype for a in k] == [np.int32, np.int32, np.float64, np.float64,
-                                    np.int32, np.int32, np.int32, np.float64]
+                                    np.int32, np.int32, np.int32, np.float64,
+                                    np.int32, np.int32, np.int32]
     assert k[0].tolist() == [len(i["calib"]["atoms"]) for i in insts]
     assert k[1].tolist() == [_lib.EL_LAYOUT_CHAIN] * 24 + [_lib.EL_LAYOUT_FULL]
+    eoff = [0]
+    for inst in insts:
+        eoff.append(eoff[-1] + len(inst["edges"] or []))
+    assert k[8].tolist() == eoff
     assert np.array_equal(k[2], np.concatenate([np.asarray(i["Om"], float) for i in insts]))
     assert np.array_equal(k[3], np.concatenate([np.asarray(i["delta"], float) for i in insts]))
     offs, pi, pj, V = [0], [], [], []
@@ -270,6 +275,29 @@ def test_pack_instances_matches_calib_pairs():
     assert empty[4].tolist() == [0, 0] and empty[5].tolist() == [0] and empty[7].tolist() == [0.0]
     with pytest.raises(ValueError):
         batched.pack_instances([dict(calib=lone, Om=np.array([1j, 0]), delta=np.zeros(2), edges=None)])
+
+
+def test_batched_layout_of_each_blockade_graph():
+    """A path or cycle keeps the arithmetic layouts, any other graph becomes
+    a code table (its edges normalised and passed on), no edges the full
+    basis; an edge outside the instance is refused on the host."""
+    from energy_level_b200 import _lib, batched
+    assert batched._layout(5, None) == (_lib.EL_LAYOUT_FULL, [])
+    assert batched._layout(5, [(1, 2), (0, 1), (3, 2), (3, 4)])[0] == _lib.EL_LAYOUT_CHAIN
+    assert batched._layout(5, [(0, 1), (1, 2), (2, 3), (3, 4), (4, 0)])[0] == _lib.EL_LAYOUT_RING
+    lay, es = batched._layout(4, [(1, 0), (0, 2), (2, 1), (3, 2)])
+    assert lay == _lib.EL_LAYOUT_TABLE and es == [(0, 1), (0, 2), (1, 2), (2, 3)]
+    with pytest.raises(ValueError):
+        batched._layout(4, [(0, 4)])
+    with pytest.raises(ValueError):
+        batched._layout(4, [(2, 2)])
+    star = {"atoms": [{"id": i, "pos": p} for i, p in enumerate([[0.0, 0.0, 0.0], [6.0, 0.0, 0.0],
+                                                                  [0.0, 6.0, 0.0], [-6.0, 0.0, 0.0]])],
+            "pairs": [], "terms": ["I1"]}
+    k = batched.pack_instances([dict(calib=star, Om=np.ones(4), delta=np.zeros(4),
+                                     edges=[(0, 1), (0, 2), (3, 0)])])
+    assert k[1].tolist() == [_lib.EL_LAYOUT_TABLE]
+    assert k[8].tolist() == [0, 3] and k[9].tolist() == [0, 0, 0] and k[10].tolist() == [1, 2, 3]
 
 
 def test_pulse_problem_refuses_exchange_channels():
