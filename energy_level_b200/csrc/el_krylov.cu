@@ -85,31 +85,46 @@ extern "C" int el_bounds(el_ctx *ctx, el_ham *h, int max_iter, double tol,
   int ivp = 0, iv = 1, iw = 2;   // buffer indices of vp, v, w in the plan
   std::vector<double> al, be;
   double beta = 0.0, lo_prev = 0, hi_prev = 0;
+  // The stored vectors are s_j = kappa_j v_j (v_j the unit Lanczos vectors):
+  // one fused update per step forms s_{j+1} = (y - alpha s_j) / (kappa_j
+  // beta_pred) with beta_pred from the step's dots, and its norm gives the
+  // exact beta and kappa_{j+1}; no separate normalisation pass.
+  double kappa = 1.0, kappa_prev = 1.0;
   int stable = 0;
   const int maxit = (int)std::min<int64_t>(max_iter, dim);
   for (int j = 0; j < maxit; ++j) {
     if (el::cancelled(ctx)) return fail(ctx, EL_ECANCEL, "cancelled");
+    // y = H s_j - beta_j (kappa_j / kappa_{j-1}) s_{j-1} = kappa_j w_j
+    const double cz = j ? -beta * kappa / kappa_prev : 0.0;
     if (plan) {
-      rc = el::hv_tiled(ctx, h, plan, iv, iw, ivp, -beta, d_sc);
+      rc = el::hv_tiled(ctx, h, plan, iv, iw, ivp, cz, d_sc);
     } else {
       ApplyArgs A;
       memset(&A, 0, sizeof A);
       A.dtype = dtype; A.nvec = 1; A.x = v; A.z = vp; A.y = w;
-      A.a = 1.0; A.b = 0.0; A.c = -beta; A.dots = d_sc; A.want_dots = 2;
+      A.a = 1.0; A.b = 0.0; A.c = cz; A.dots = d_sc; A.want_dots = 7;
       rc = el::launch_apply(ctx, h, A);
     }
     if (rc) return rc;
     double dots[4];
     rc = sync_read(ctx, d_sc, 4, dots);
     if (rc) return rc;
-    const double alpha = dots[1];
-    rc = el::launch_axpby(ctx, dtype, dim, -alpha, 0, v, 1, 0, w, d_sc + 8);
+    const double k2 = kappa * kappa;
+    const double alpha = dots[1] / k2;
+    const double bp2 = dots[3] / k2 - alpha * alpha;   // |w_j - alpha v_j|^2 from <y,y> (dots[3])
+    const double scale_a = std::max(1.0, std::fabs(alpha));
+    const bool fused = bp2 > 1e-6 * scale_a * scale_a;  // else: form the norm directly
+    const double bpred = fused ? std::sqrt(bp2) : 1.0;
+    const double sc = 1.0 / (kappa * bpred);
+    rc = el::launch_axpby(ctx, dtype, dim, -alpha * sc, 0, v, sc, 0, w, d_sc + 8);
     if (rc) return rc;
     double n2;
     rc = sync_read(ctx, d_sc + 8, 1, &n2);
     if (rc) return rc;
     al.push_back(alpha);
-    beta = std::sqrt(std::max(n2, 0.0));
+    // |s_{j+1}|^2 = n2 and s_{j+1} = (beta / bpred) v_{j+1}
+    const double kappa_next = std::sqrt(std::max(n2, 0.0));
+    beta = kappa_next * bpred;
     const int m = (int)al.size();
     double lo = el::tridiag_eig(al.data(), be.data(), m, 0);
     double hi = el::tridiag_eig_max(al.data(), be.data(), m);
@@ -123,14 +138,18 @@ extern "C" int el_bounds(el_ctx *ctx, el_ham *h, int max_iter, double tol,
     hi_prev = hi;
     if (beta <= 1e-13 * scale) break;  // invariant subspace: exact extremes
     be.push_back(beta);
-    // v_prev <- v ; v <- w / beta
+    // s_{j-1} <- s_j ; s_j <- s_{j+1}
     std::swap(vp, v);
     std::swap(v, w);
     std::swap(ivp, iv);
     std::swap(iv, iw);
-    double inv = 1.0 / beta;
-    rc = el::launch_axpby(ctx, dtype, dim, 0, 0, nullptr, inv, 0, v, nullptr);
-    if (rc) return rc;
+    kappa_prev = kappa;
+    kappa = kappa_next;
+    if (!fused) {   // bring the vector to unit length before the next step
+      rc = el::launch_axpby(ctx, dtype, dim, 0, 0, nullptr, 1.0 / kappa, 0, v, nullptr);
+      if (rc) return rc;
+      kappa = 1.0;
+    }
   }
   if (plan) {
     rc = el::hv_tiled_error(ctx, plan);

@@ -30,7 +30,7 @@ namespace {
 
 using el::fail;
 
-constexpr int kGroup = 8;
+constexpr int kGroup = 6;   // items per launch column: 6 x 3 FP64 sums fit the registers of 2 CTAs per SM
 enum { kNoItem = 0, kNormItem, kSiteItem, kPairItem, kPauliItem };
 
 struct ObsItem {
