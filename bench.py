@@ -359,7 +359,8 @@ def run_native(args):
             "config": config_dict(cfg, {"parallelism": "replicas" if world > 1 else "single GPU"}),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_kpm_tma (one Chebyshev step of 32 probes over 2^%d rows)" % n,
+                         "kernel": "k_kpm_tma (B tiles) / k_kpm_tx_a (A tiles): one Chebyshev step of 32 probes "
+                                   "over 2^%d rows" % n,
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_s * 1e3,
                          "peak_source": peak_kind},
             "cpu_baseline": cpu,

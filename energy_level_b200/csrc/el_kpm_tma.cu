@@ -10,7 +10,8 @@
 //
 // Here every byte of tile traffic moves by TMA, not through the LSU pipe:
 //   - vectors are [probe][row] arrays (one probe per cell), so an A tile
-//     (2^a consecutive rows) is one 64 KB box;
+//     (2^a consecutive rows) is one 64 KB box (two 128-byte-swizzled 32 KB
+//     boxes for the two-layout FP32 A pass of 14-bit tiles, k_kpm_tx_a);
 //   - a B tile holds the C lowest row bits as a contiguous piece of 32 bytes
 //     (C = 3 for FP32: one DRAM sector) or 16 bytes (C = 1 for FP64), carried
 //     but not flipped, plus row bits a..N-1; its 2^(N-a) pieces lie 2^a rows
@@ -741,6 +742,293 @@ __device__ __forceinline__ void hv_finish_dots(const TmaArgs<T> &A, double sxx, 
   if (tid == 0) *A.counter = 0u;
 }
 
+// ------------------------------------------- A pass with two thread layouts
+//
+// FP32, 14-bit A tiles (N = 24, 25).  The single-layout pass gathers nine of
+// the 14 tile bits through shared memory in each of its two X applications.
+// Here the tile is held in shared memory with the TMA 128-byte swizzle
+// (float index l at l ^ (((l >> 5) & 7) << 2)), which makes two thread
+// layouts conflict-free:
+//   L1 ("columns"): cell l = tid + 512 j -- lanes hold bits 0..4, warps
+//       bits 5..8, the 32 register slots bits 9..13;
+//   L2 ("rows"): thread tid holds the 32 cells of row tid (bits 5..13 =
+//       tid, bits 0..4 in registers), read and written as eight 16-byte
+//       vectors whose swizzled positions differ across each quarter-warp.
+// An X application then gathers only bits 5..8 (L1) and takes bits 9..13
+// (L1) and 0..4 (L2) from registers; the two partial sums meet in the
+// buffer the result goes to anyway:
+//   t_m: L1 adds s X_{5..13} t_{m-1} into the p_m tile, L2 adds
+//        s X_{0..4} t_{m-1} and completes t_m (and the dot products);
+//   p_{m+1}: L2 writes d2 t_m - t_{m-1} + (2/r) X_{0..4} t_m over t_{m-1},
+//        L1 adds (2/r) X_{5..13} t_m.
+// About 21 four-byte shared-pipe moves per cell instead of 25.  The tile's
+// row of coupling sums (k_otf_table) travels with its t_{m-1} tile, as in
+// k_kpm_tma.
+__device__ __forceinline__ int swz128(int l) { return l ^ (((l >> 5) & 7) << 2); }
+
+__device__ __forceinline__ void tile_load_swz(const TmaArgs<float> &A, void *dst, const CUtensorMap *m,
+                                              uint32_t tile, int g, uint64_t *bar) {
+  tma_load3(dst, m, 0, (int)(tile << 9), g, bar);
+  tma_load3((char *)dst + 32768, m, 0, (int)((tile << 9) + 256), g, bar);
+}
+__device__ __forceinline__ void wrow_load(const TmaArgs<float> &A, double *dst, uint32_t tile, uint64_t *bar) {
+  bulk_load(dst, A.wtab + (size_t)tile * OTF_ROW, OTF_ROW * sizeof(double), bar);
+}
+__device__ __forceinline__ void tile_store_swz(const CUtensorMap *m, uint32_t tile, int g, const void *src) {
+  tma_store3(m, 0, (int)(tile << 9), g, src);
+  tma_store3(m, 0, (int)((tile << 9) + 256), g, (const char *)src + 32768);
+}
+
+__global__ void __launch_bounds__(512, 1)
+k_kpm_tx_a(const TmaArgs<float> A, const __grid_constant__ CUtensorMap mapP,
+           const __grid_constant__ CUtensorMap mapQ) {
+  typedef float T;
+  constexpr int NT = 512, R = 32, NWARP = 16, TB = 14;
+  constexpr unsigned TILE_BYTES = 65536;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  T *const Sb0 = reinterpret_cast<T *>(smem_raw);
+  T *const Sb1 = reinterpret_cast<T *>(smem_raw + TILE_BYTES);
+  T *const S2 = reinterpret_cast<T *>(smem_raw + 2 * TILE_BYTES);
+  __shared__ __align__(8) uint64_t bar[3];
+  __shared__ double wred[NWARP][2];
+  __shared__ double sV[EL_KPM_MAXN * EL_KPM_MAXN];
+  __shared__ double tJ[32];        // delta + V of the register bits 0..4 of slot c
+  __shared__ double cTJ[5 * NT];   // [k][tid]: couplings of the row bits 5..13 of tid to bit k
+  __shared__ __align__(16) double wHt[2][OTF_ROW];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ndots = A.ng * 2;
+  const int nb = A.n;
+  double *dacc = A.partials + (size_t)blockIdx.x * ndots;
+  for (int i = tid; i < ndots; i += NT) dacc[i] = 0.0;
+  for (int i = tid; i < nb * nb; i += NT) sV[i] = A.vbits[i];
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
+    fence_async_smem();
+  }
+  __syncthreads();
+  // diagonal sums of the L2 layout: thread bits = row bits 5..13, slots = bits 0..4
+  double cT = 0.0;
+  for (int x = 0; x < 9; ++x) {
+    if (!((tid >> x) & 1)) continue;
+    cT += A.delta_b[5 + x];
+    for (int x2 = 0; x2 < x; ++x2)
+      if ((tid >> x2) & 1) cT += sV[(5 + x) * nb + 5 + x2];
+  }
+  for (int k = 0; k < 5; ++k) {
+    double acc = 0.0;
+    for (int x = 0; x < 9; ++x)
+      if ((tid >> x) & 1) acc += sV[(5 + x) * nb + k];
+    cTJ[k * NT + tid] = acc;
+  }
+  if (tid < 32) {
+    double v = 0.0;
+    for (int k = 0; k < 5; ++k) {
+      if (!((tid >> k) & 1)) continue;
+      v += A.delta_b[k];
+      for (int k2 = 0; k2 < k; ++k2)
+        if ((tid >> k2) & 1) v += sV[k * nb + k2];
+    }
+    tJ[tid] = v;
+  }
+  unsigned par[3] = {0u, 0u, 0u};
+  int cur = 0;
+  int64_t item = blockIdx.x;
+  double acc_tt = 0.0, acc_tq = 0.0;
+  int gacc = item_group(A, item);
+  if (tid == 0 && item < A.items) {
+    mbar_expect(&bar[0], TILE_BYTES + OTF_ROW * 8);
+    tile_load_swz(A, Sb0, &mapQ, item_tile(A, item), gacc, &bar[0]);
+    wrow_load(A, wHt[0], item_tile(A, item), &bar[0]);
+  }
+  const int rowq = tid & 7;    // swizzle of this thread's row (L2)
+  // L1 cells tid + 512 j differ from tid only in bits 9..13, which the
+  // swizzle does not read: their positions are swz(tid) + 512 j
+  const int sw1 = swz128(tid);
+  for (; item < A.items; item += gridDim.x) {
+    const int g = item_group(A, item);
+    const uint32_t tile = item_tile(A, item);
+    const int64_t nxt = item + gridDim.x;
+    if (g != gacc) {
+      double x = acc_tt, y = acc_tq;
+      for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+        y += __shfl_xor_sync(0xffffffffu, y, o);
+      }
+      if (lane == 0) { wred[warp][0] = x; wred[warp][1] = y; }
+      acc_tt = 0.0; acc_tq = 0.0;
+      __syncthreads();
+      if (tid < 2) {
+        double sum = 0.0;
+#pragma unroll
+        for (int w = 0; w < NWARP; ++w) sum += wred[w][tid];
+        dacc[gacc * 2 + tid] += sum;
+      }
+      gacc = g;
+    }
+    T *S = cur ? Sb1 : Sb0;
+    T *Sn = cur ? Sb0 : Sb1;
+    if (tid == 0) bulk_wait_read<1>();   // the previous t_m store has read S2
+    __syncthreads();
+    if (tid == 0) {
+      mbar_expect(&bar[2], TILE_BYTES);
+      tile_load_swz(A, S2, &mapP, tile, g, &bar[2]);
+    }
+    if (cur) { mbar_wait(&bar[1], par[1], A.err); par[1] ^= 1u; }
+    else { mbar_wait(&bar[0], par[0], A.err); par[0] ^= 1u; }
+
+    // ---- L1: s X_{5..13} t_{m-1} added into the p_m tile
+    {
+      T own[R], h[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) { own[j] = S[sw1 + NT * j]; h[j] = 0.f; }
+#pragma unroll
+      for (int b = 0; b < 5; ++b) {
+        const T a = A.amp[9 + b];
+#pragma unroll
+        for (int j = 0; j < R; ++j) h[j] = fmaf(a, own[j ^ (1 << b)], h[j]);
+      }
+#pragma unroll
+      for (int k = 5; k < 9; ++k) {
+        const T a = A.amp[k];
+        const T *Sp = S + swz128(tid ^ (1 << k));
+#pragma unroll
+        for (int j = 0; j < R; ++j) h[j] = fmaf(a, Sp[NT * j], h[j]);
+      }
+      if (tid == 0 && nxt < A.items) {
+        bulk_wait_read<0>();   // the previous p_{m+1} store has read Sn
+        uint64_t *bn = cur ? &bar[0] : &bar[1];
+        mbar_expect(bn, TILE_BYTES + OTF_ROW * 8);
+        tile_load_swz(A, Sn, &mapQ, item_tile(A, nxt), item_group(A, nxt), bn);
+        wrow_load(A, wHt[cur ^ 1], item_tile(A, nxt), bn);
+      }
+      mbar_wait(&bar[2], par[2], A.err);
+      par[2] ^= 1u;
+#pragma unroll
+      for (int j = 0; j < R; ++j) S2[sw1 + NT * j] = fmaf(A.s_m, h[j], S2[sw1 + NT * j]);
+    }
+    __syncthreads();
+    // ---- L2: s X_{0..4} t_{m-1} completes t_m in this thread's row
+    T o2[R], t2[R];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int off = 32 * tid + 4 * (q ^ rowq);
+      const float4 ov = *reinterpret_cast<const float4 *>(S + off);
+      const float4 pv = *reinterpret_cast<const float4 *>(S2 + off);
+      o2[4 * q] = ov.x; o2[4 * q + 1] = ov.y; o2[4 * q + 2] = ov.z; o2[4 * q + 3] = ov.w;
+      t2[4 * q] = pv.x; t2[4 * q + 1] = pv.y; t2[4 * q + 2] = pv.z; t2[4 * q + 3] = pv.w;
+    }
+#pragma unroll
+    for (int b = 0; b < 5; ++b) {
+      const T a = A.s_m * A.amp[b];
+#pragma unroll
+      for (int c = 0; c < R; ++c) t2[c] = fmaf(a, o2[c ^ (1 << b)], t2[c]);
+    }
+    T pt[2] = {0.f, 0.f}, pq[2] = {0.f, 0.f};
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      pt[c & 1] = fmaf(t2[c], t2[c], pt[c & 1]);
+      pq[c & 1] = fmaf(t2[c], o2[c], pq[c & 1]);
+    }
+    if (A.mode != MODE_LAST) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        *reinterpret_cast<float4 *>(S2 + 32 * tid + 4 * (q ^ rowq)) =
+            make_float4(t2[4 * q], t2[4 * q + 1], t2[4 * q + 2], t2[4 * q + 3]);
+      fence_async_smem();
+      __syncthreads();
+      if (tid == 0) { tile_store_swz(&mapP, tile, g, S2); bulk_commit(); }
+      // ---- L2: p_{m+1} partial = d2 t_m - t_{m-1} + (2/r) X_{0..4} t_m over t_{m-1}
+      {
+        const double *wH = wHt[cur];
+        double base = cT + wH[OTF_ROW - 1];
+        for (int x = 0; x < 9; ++x)
+          if ((tid >> x) & 1) base += wH[5 + x];
+        double u[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) u[k] = cTJ[k * NT + tid] + wH[k];
+        // o2 (t_{m-1}) becomes the p_{m+1} partial in place
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+          double dj = base + tJ[c];
+#pragma unroll
+          for (int k = 0; k < 5; ++k)
+            if ((c >> k) & 1) dj += u[k];
+          o2[c] = fmaf((T)fma(A.s2, dj, A.s2c), t2[c], -o2[c]);
+        }
+#pragma unroll
+        for (int b = 0; b < 5; ++b) {
+          const T a = A.amp[b] * A.two_r;
+#pragma unroll
+          for (int c = 0; c < R; ++c) o2[c] = fmaf(a, t2[c ^ (1 << b)], o2[c]);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          *reinterpret_cast<float4 *>(S + 32 * tid + 4 * (q ^ rowq)) =
+              make_float4(o2[4 * q], o2[4 * q + 1], o2[4 * q + 2], o2[4 * q + 3]);
+      }
+      __syncthreads();
+      // ---- L1: (2/r) X_{5..13} t_m added into the p_{m+1} tile
+      {
+        T tl[R], h[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) { tl[j] = S2[sw1 + NT * j]; h[j] = 0.f; }
+#pragma unroll
+        for (int b = 0; b < 5; ++b) {
+          const T a = A.amp[9 + b];
+#pragma unroll
+          for (int j = 0; j < R; ++j) h[j] = fmaf(a, tl[j ^ (1 << b)], h[j]);
+        }
+#pragma unroll
+        for (int k = 5; k < 9; ++k) {
+          const T a = A.amp[k];
+          const T *Sp = S2 + swz128(tid ^ (1 << k));
+#pragma unroll
+          for (int j = 0; j < R; ++j) h[j] = fmaf(a, Sp[NT * j], h[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < R; ++j) S[sw1 + NT * j] = fmaf(A.two_r, h[j], S[sw1 + NT * j]);
+      }
+      fence_async_smem();
+      __syncthreads();
+      if (tid == 0) { tile_store_swz(&mapQ, tile, g, S); bulk_commit(); }
+    }
+    acc_tt += (double)pt[0] + (double)pt[1];
+    acc_tq += (double)pq[0] + (double)pq[1];
+    cur ^= 1;
+  }
+  {
+    double x = acc_tt, y = acc_tq;
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_xor_sync(0xffffffffu, x, o);
+      y += __shfl_xor_sync(0xffffffffu, y, o);
+    }
+    if (lane == 0) { wred[warp][0] = x; wred[warp][1] = y; }
+  }
+  __syncthreads();
+  if (tid < 2 && blockIdx.x < A.items) {
+    double sum = 0.0;
+#pragma unroll
+    for (int w = 0; w < NWARP; ++w) sum += wred[w][tid];
+    dacc[gacc * 2 + tid] += sum;
+  }
+  if (tid == 0) bulk_wait_all();
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(A.counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int i = tid; i < ndots; i += NT) {
+    double sum = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) sum += __ldcg(&A.partials[(size_t)b * ndots + i]);
+    A.dots[i] = sum;
+  }
+  if (tid == 0) *A.counter = 0u;
+}
+
 // probes -> cells [probe group][row]; probe p = g*PU + lane
 template <typename T>
 __global__ void k_cells8(int64_t dim, int ng, uint64_t seed, int64_t probe0, int nvalid,
@@ -824,6 +1112,23 @@ int make_maps(el_ctx *ctx, void *base, int n, int a, int ng, int hb, CUtensorMap
   return EL_OK;
 }
 
+// A map with the 128-byte swizzle for the two-layout A pass (FP32): rows of
+// 32 floats, boxes of 256 rows (two per 14-bit tile).
+int make_map_a_swz(el_ctx *ctx, void *base, int n, int ng, CUtensorMap *m) {
+  auto enc = encode_fn();
+  if (!enc) return fail(ctx, EL_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  const uint64_t dim = 1ull << n;
+  cuuint64_t gdim[3] = {32, dim / 32, (cuuint64_t)ng};
+  cuuint64_t gstr[2] = {128, dim * 4};
+  cuuint32_t box[3] = {32, 256, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, gdim, gstr, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ctx, EL_ECUDA, "swizzled tensor map A encode failed (%d)", (int)r);
+  return EL_OK;
+}
+
 template <typename T>
 int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
             const int8_t *probes_host, int num, double c, double r, std::vector<double> &acc) {
@@ -890,6 +1195,14 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
   if (rc) return rc;
   rc = make_maps<T>(ctx, Q, n, a, ng, hb, &mA[1], &mB[1]);
   if (rc) return rc;
+  const bool use_tx = sizeof(T) == 4 && TBA == 14;
+  CUtensorMap mAs[2];
+  if (use_tx) {
+    rc = make_map_a_swz(ctx, P, n, ng, &mAs[0]);
+    if (rc) return rc;
+    rc = make_map_a_swz(ctx, Q, n, ng, &mAs[1]);
+    if (rc) return rc;
+  }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   auto launch = [&](int kind, int mode, double s_m, int pbuf, double *dots) -> int {
@@ -925,6 +1238,14 @@ int run_tma(el_ctx *ctx, el_ham *h, int nvalid_total, int chunk, uint64_t seed,
     // 1024 threads: twice the registers per cell made 512 threads slower.
     const int lnt = (sizeof(T) == 4 && TB >= 12) ? 9 : 10;
     bool ok = false;
+    if constexpr (sizeof(T) == 4) {
+      if (use_tx && kind == KIND_A && mode != MODE_PROLOGUE) {
+        cudaFuncSetAttribute(k_kpm_tx_a, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_kpm_tx_a<<<grid, 512, smem, ctx->stream>>>(A, mAs[pbuf], mAs[pbuf ^ 1]);
+        EL_LAUNCH_CHECK(ctx);
+        return EL_OK;
+      }
+    }
 #define EL_TCASE(TBV, KV, LV)                                                                     \
   if (TB == TBV && kind == KV && lnt == LV) {                                                     \
     cudaFuncSetAttribute(k_kpm_tma<T, TBV, KV, LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
