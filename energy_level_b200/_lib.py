@@ -21,6 +21,7 @@ EL_OK, EL_EINVAL, EL_ENOMEM, EL_ENOTCONV, EL_ECANCEL, EL_ECUDA = range(6)
 EL_F32, EL_F64, EL_C64, EL_C128 = range(4)
 EL_BASIS_FULL, EL_BASIS_BLOCKADE, EL_BASIS_CHARGE = range(3)
 EL_LAYOUT_FULL, EL_LAYOUT_CHAIN, EL_LAYOUT_RING, EL_LAYOUT_TABLE = range(4)
+EL_ADJ_AUTO, EL_ADJ_STREAM, EL_ADJ_COOP = range(3)
 EL_KPM_DIRECT, EL_KPM_DOUBLING = range(2)
 EL_KPM_GENERIC_KERNEL = 0x100
 
@@ -80,6 +81,7 @@ PROTOTYPES = {
     "el_spin_observables": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _dp, _dp, _dp, _dp, _dp]),
     "el_pauli_expect": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_char_p, _dp]),
     "el_observables_noalloc": (C.c_int, [_vp, _vp, C.c_int, _vp, _dp, _dp]),
+    "el_adjoint_set_mode": (C.c_int, [_vp, C.c_int]),
     "el_adjoint_pulse": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _vp, _vp, _vp,
                                    C.c_double, _dp, _dp, _dp, _vp]),
 }

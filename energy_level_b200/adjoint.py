@@ -54,6 +54,15 @@ class PulseProblem:
         self.oshape = None if omega_shape is None else np.ascontiguousarray(omega_shape, float)
         self.dshape = None if delta_shape is None else np.ascontiguousarray(delta_shape, float)
 
+    def set_schedule(self, mode='auto'):
+        """'coop' (and 'auto', the default): the whole gradient as one
+        cooperative launch with grid barriers between its sweeps; 'stream':
+        one launch per Chebyshev and reverse term (el_adjoint_set_mode)."""
+        modes = {'auto': _lib.EL_ADJ_AUTO, 'stream': _lib.EL_ADJ_STREAM, 'coop': _lib.EL_ADJ_COOP}
+        if mode not in modes:
+            raise ValueError("schedule must be 'auto', 'stream' or 'coop'")
+        self.ctx.call('el_adjoint_set_mode', C.c_int(modes[mode]))
+
     def evaluate(self, tau, omega_k, delta_k, want_state=False):
         """(F, dF/dOmega_k, dF/dDelta_k[, psi_K])."""
         torch = _torch()

@@ -201,6 +201,85 @@ __global__ void k_diag_mul(int64_t dim, const double *O, const S *psi, S *lam, d
   }
 }
 
+// Gershgorin bounds of every step's H_k in one launch: row r contributes
+// d -+ R with d = diagV[r] + sum_{set q} (-Delta_k b_q) and R = sum over its
+// allowed flips of |Omega_k a_q / 2|, summed in the order (and with the
+// roundings) of k_gershgorin for the drive of that step.  Per block and
+// step: the block's min and max, out[(block K + k) 2 + {0, 1}].
+struct StepShapes { double a[EL_MAX_SITES], b[EL_MAX_SITES]; };   // by bit position
+
+__global__ void k_step_bounds(BasisDev B, const double *__restrict__ diagV, StepShapes sh, int K,
+                              const double *__restrict__ om, const double *__restrict__ dl, double *out) {
+  __shared__ double lo_s[256], hi_s[256];
+  for (int k = 0; k < K; ++k) {
+    const double o = om[k], d0 = dl[k];
+    double lo = 1e300, hi = -1e300;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < B.dim;
+         r += (int64_t)gridDim.x * blockDim.x) {
+      const uint64_t code = el::unrank_row(B, r);
+      double d = diagV[r], R = 0.0;
+      for (int q = 0; q < B.n; ++q) {
+        if ((code >> q) & 1ULL) d += d0 * sh.b[q];
+        const double amp = fabs(0.5 * (o * sh.a[q]));
+        if (amp == 0.0) continue;
+        if (el::flip_target(B, code, r, q) >= 0) R += amp;
+      }
+      lo = fmin(lo, d - R);
+      hi = fmax(hi, d + R);
+    }
+    lo_s[threadIdx.x] = lo;
+    hi_s[threadIdx.x] = hi;
+    __syncthreads();
+    for (int s2 = 128; s2 > 0; s2 >>= 1) {
+      if (threadIdx.x < s2) {
+        lo_s[threadIdx.x] = fmin(lo_s[threadIdx.x], lo_s[threadIdx.x + s2]);
+        hi_s[threadIdx.x] = fmax(hi_s[threadIdx.x], hi_s[threadIdx.x + s2]);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      out[((size_t)blockIdx.x * K + k) * 2] = lo_s[0];
+      out[((size_t)blockIdx.x * K + k) * 2 + 1] = hi_s[0];
+    }
+    __syncthreads();
+  }
+}
+
+// lo[k], hi[k] of every step (one launch, one copy back).
+int step_bounds(el_ctx *ctx, el_ham *h, int K, const double *omega_k, const double *delta_k,
+                const std::vector<double> &ash, const std::vector<double> &bsh, std::vector<double> &lo,
+                std::vector<double> &hi) {
+  const int n = h->n;
+  const int64_t dim = h->basis->dim;
+  int sms = 148;
+  EL_CUDA_TRY(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  const int grid = (int)std::min<int64_t>(el::grid_for(dim, 256), 2 * (int64_t)sms);
+  double *d = (double *)el::workspace(ctx, 12, ((size_t)2 * K + (size_t)grid * K * 2) * sizeof(double));
+  if (!d) return EL_ENOMEM;
+  double *d_om = d, *d_dl = d + K, *d_out = d + 2 * K;
+  std::vector<double> hom(K), hdl(K);
+  for (int k = 0; k < K; ++k) { hom[k] = omega_k[k]; hdl[k] = -delta_k[k]; }
+  EL_CUDA_TRY(ctx, el::copy(ctx, d_om, hom.data(), K * sizeof(double), cudaMemcpyHostToDevice));
+  EL_CUDA_TRY(ctx, el::copy(ctx, d_dl, hdl.data(), K * sizeof(double), cudaMemcpyHostToDevice));
+  StepShapes sh;
+  memset(&sh, 0, sizeof sh);
+  for (int q = 0; q < n; ++q) { sh.a[q] = ash[n - 1 - q]; sh.b[q] = bsh[n - 1 - q]; }
+  k_step_bounds<<<grid, 256, 0, ctx->stream>>>(el::basis_dev(h->basis), h->d_diagV64, sh, K, d_om, d_dl, d_out);
+  ctx->launches++;
+  EL_LAUNCH_CHECK(ctx);
+  std::vector<double> part((size_t)grid * K * 2);
+  EL_CUDA_TRY(ctx, el::copy(ctx, part.data(), d_out, part.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  lo.assign(K, 1e300);
+  hi.assign(K, -1e300);
+  for (int b = 0; b < grid; ++b)
+    for (int k = 0; k < K; ++k) {
+      lo[k] = std::min(lo[k], part[((size_t)b * K + k) * 2]);
+      hi[k] = std::max(hi[k], part[((size_t)b * K + k) * 2 + 1]);
+    }
+  return EL_OK;
+}
+
 template <typename S>
 int adjoint_impl(el_ctx *ctx, el_ham *h, int dtype, int K, const double *tau, const double *omega_k,
                  const double *delta_k, const double *oshape, const double *dshape, const void *psi0,
@@ -219,15 +298,18 @@ int adjoint_impl(el_ctx *ctx, el_ham *h, int dtype, int K, const double *tau, co
     for (int i = 0; i < n; ++i) { ore[i] = omega_k[k] * ash[i]; de[i] = -delta_k[k] * bsh[i]; }
     return el_ham_set_drive(ctx, h, ore.data(), oim.data(), de.data());
   };
-  // plans of all steps (bounds and coefficients)
+  // plans of all steps: the Gershgorin bounds of every step in one launch,
+  // then the expansions on the host
   std::vector<el::ChebPlan> plans(K);
   int Mmax = 1;
-  for (int k = 0; k < K; ++k) {
-    int rc = set_drive(k);
+  {
+    std::vector<double> lo, hi;
+    int rc = step_bounds(ctx, h, K, omega_k, delta_k, ash, bsh, lo, hi);
     if (rc) return rc;
-    rc = el::cheb_plan(ctx, h, tau[k], tol, &plans[k]);
-    if (rc) return rc;
-    Mmax = std::max(Mmax, plans[k].M);
+    for (int k = 0; k < K; ++k) {
+      el::cheb_plan_bounds(lo[k], hi[k], tau[k], tol, &plans[k]);
+      Mmax = std::max(Mmax, plans[k].M);
+    }
   }
   // workspace: K+1 checkpoints, Mmax+1 terms, 3 adjoint vectors, lambda
   char *buf = (char *)el::workspace(ctx, 11, (size_t)(K + 1 + Mmax + 1 + 4) * vb);
@@ -238,6 +320,33 @@ int adjoint_impl(el_ctx *ctx, el_ham *h, int dtype, int K, const double *tau, co
   char *ub = tb + (size_t)(Mmax + 1) * vb;
   void *U[3] = {ub, ub + vb, ub + 2 * vb};
   void *lam = ub + 3 * vb;
+  if (ctx->adjoint_mode != EL_ADJ_STREAM) {
+    // one cooperative launch for the whole gradient
+    std::vector<double> hg;
+    double F = 0.0;
+    int rc = el::adjoint_coop<S>(ctx, h, K, plans, Mmax, omega_k, delta_k, ash, bsh, psi0, target, obs_diag,
+                                 buf, hg, F);
+    if (rc) return rc;
+    if (psi_final) {
+      EL_CUDA_TRY(ctx, el::copy(ctx, psi_final, ckp(K), vb, cudaMemcpyDeviceToDevice));
+      EL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    rc = set_drive(0);   // the drive the stream path leaves behind
+    if (rc) return rc;
+    for (int k = 0; k < K; ++k) {
+      const el::ChebPlan &pl = plans[k];
+      double go = 0.0, gd = 0.0;
+      for (int m = 1; m <= pl.M; ++m) {
+        const double s = (m == 1) ? 1.0 : 2.0;
+        go += s * hg[((size_t)k * (Mmax + 1) + m) * 2];
+        gd += s * hg[((size_t)k * (Mmax + 1) + m) * 2 + 1];
+      }
+      gO_out[k] = 2.0 * go / pl.a;
+      gD_out[k] = 2.0 * gd / pl.a;
+    }
+    *F_out = F;
+    return EL_OK;
+  }
   double *d_g = (double *)el::workspace(ctx, 12, (size_t)K * (Mmax + 1) * 2 * sizeof(double) + 64);
   if (!d_g) return EL_ENOMEM;
   EL_CUDA_TRY(ctx, cudaMemsetAsync(d_g, 0, (size_t)K * (Mmax + 1) * 2 * sizeof(double), ctx->stream));
@@ -375,6 +484,14 @@ int adjoint_impl(el_ctx *ctx, el_ham *h, int dtype, int K, const double *tau, co
 }
 
 }  // namespace
+
+extern "C" int el_adjoint_set_mode(el_ctx *ctx, int mode) {
+  if (!ctx) return EL_EINVAL;
+  if (mode != EL_ADJ_AUTO && mode != EL_ADJ_STREAM && mode != EL_ADJ_COOP)
+    return fail(ctx, EL_EINVAL, "adjoint mode must be EL_ADJ_AUTO, EL_ADJ_STREAM or EL_ADJ_COOP");
+  ctx->adjoint_mode = mode;
+  return EL_OK;
+}
 
 extern "C" int el_adjoint_pulse(el_ctx *ctx, el_ham *h, int dtype, int K, const double *tau,
                                 const double *omega_k, const double *delta_k,

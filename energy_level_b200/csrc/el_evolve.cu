@@ -53,6 +53,11 @@ int cheb_plan(el_ctx *ctx, el_ham *h, double tau_ns, double tol, ChebPlan *plan)
   double lo, hi;
   int rc = gershgorin(ctx, h, &lo, &hi);
   if (rc) return rc;
+  cheb_plan_bounds(lo, hi, tau_ns, tol, plan);
+  return EL_OK;
+}
+
+void cheb_plan_bounds(double lo, double hi, double tau_ns, double tol, ChebPlan *plan) {
   plan->b = 0.5 * (hi + lo);
   plan->a = std::max(0.5 * (hi - lo) * (1.0 + 1e-6), 1e-12);
   const double x = plan->a * CONV * tau_ns;
@@ -80,7 +85,6 @@ int cheb_plan(el_ctx *ctx, el_ham *h, double tau_ns, double tol, ChebPlan *plan)
     plan->c_re[m] = mag * (pr * cph - pi * sph);
     plan->c_im[m] = mag * (pr * sph + pi * cph);
   }
-  return EL_OK;
 }
 
 }  // namespace el

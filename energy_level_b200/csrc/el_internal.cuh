@@ -43,6 +43,7 @@ struct el_ctx {
   // cached device workspace slots (grown on demand, freed with the context)
   void *ws_ptr[16] = {nullptr};
   size_t ws_size[16] = {0};
+  int adjoint_mode = 0;    // EL_ADJ_*: how el_adjoint_pulse schedules its sweeps
 };
 #define EL_SCALARS 4096
 
@@ -352,6 +353,17 @@ struct ChebPlan {
   std::vector<double> c_re, c_im;
 };
 int cheb_plan(el_ctx *ctx, el_ham *h, double tau_ns, double tol, ChebPlan *plan);
+// The expansion for a spectrum inside [lo, hi] (what cheb_plan does after
+// its Gershgorin bound).
+void cheb_plan_bounds(double lo, double hi, double tau_ns, double tol, ChebPlan *plan);
+// The whole adjoint gradient as one cooperative launch (el_adjoint_coop.cu):
+// vectors in buf (K+1 checkpoints, Mmax+1 terms, 3 adjoint vectors, lambda),
+// per-term dots into hg, the objective into F.
+template <typename S>
+int adjoint_coop(el_ctx *ctx, el_ham *h, int K, const std::vector<ChebPlan> &plans, int Mmax,
+                 const double *omega_k, const double *delta_k, const std::vector<double> &ash,
+                 const std::vector<double> &bsh, const void *psi0, const void *target, const double *obs_diag,
+                 void *buf, std::vector<double> &hg, double &F);
 // Tiled single-vector FP64 H x on the full basis, 20 <= N <= 25 (el_kpm_tma.cu):
 // a plan over three vector buffers, then y = H x + cz z per call with
 // <x,x>, <x,y>, 0, <y,y> in dots[0..3].

@@ -316,6 +316,16 @@ int el_adjoint_pulse(el_ctx *ctx, el_ham *ham, int dtype, int K, const double *t
                      const double *delta_shape, const void *psi0, const void *target,
                      const double *obs_diag, double tol, double *F, double *grad_omega,
                      double *grad_delta, void *psi_final);
+/* How el_adjoint_pulse schedules its sweeps over the basis (per context):
+ * EL_ADJ_AUTO (default) and EL_ADJ_COOP run the whole gradient as one
+ * cooperative launch with grid barriers between sweeps (bounded waits: a
+ * timeout returns EL_ECUDA); EL_ADJ_STREAM launches one kernel per
+ * Chebyshev term and reverse term.  Both give the same gradient up to
+ * rounding.  No counterpart in the reference (scheduling only). */
+#define EL_ADJ_AUTO   0
+#define EL_ADJ_STREAM 1
+#define EL_ADJ_COOP   2
+int el_adjoint_set_mode(el_ctx *ctx, int mode);
 /* Site occupations <n_i> (host double[n]) and squared norm of psi.  Replaces
  * the bits @ |psi|^2 reduction of engine_ed.py:259-263 (_reduce). */
 int el_observables(el_ctx *ctx, el_ham *ham, int dtype, const void *psi,

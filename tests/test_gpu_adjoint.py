@@ -94,3 +94,29 @@ def test_autograd_function(ctx):
     F2, go, gd = prob.evaluate(tau, om, de)
     assert abs(F.item() - F2) < 1e-14
     assert np.allclose(omt.grad.numpy(), 3.0 * go) and np.allclose(det.grad.numpy(), 3.0 * gd)
+
+
+@pytest.mark.parametrize("dtype,tol", [("complex128", 1e-11), ("complex64", 2e-5)])
+@pytest.mark.parametrize("ring,target", [(True, True), (False, False)])
+def test_cooperative_and_stream_schedules_agree(ctx, dtype, tol, ring, target):
+    """The one-launch cooperative gradient and the launch-per-term gradient
+    give the same F, gradients and final state (up to rounding), and the
+    schedule switch is per context."""
+    import torch
+    prob, _, _ = _problem(12 if ring else 14, ring, dtype, target)
+    tau, om, de = _pulse(16, 3)
+    prob.set_schedule("stream")
+    Fs, gos, gds, ps = prob.evaluate(tau, om, de, want_state=True)
+    prob.set_schedule("coop")
+    Fc, goc, gdc, pc = prob.evaluate(tau, om, de, want_state=True)
+    scale = max(np.abs(gos).max(), np.abs(gds).max())
+    assert abs(Fc - Fs) < tol * max(1.0, abs(Fs))
+    assert np.max(np.abs(goc - gos)) < tol * scale
+    assert np.max(np.abs(gdc - gds)) < tol * scale
+    assert float((pc - ps).abs().max()) < tol * 10
+    # the same call again gives the same bits (fixed-order sums)
+    Fc2, goc2, _ = prob.evaluate(tau, om, de)
+    assert Fc2 == Fc and np.array_equal(goc2, goc)
+    prob.set_schedule("auto")
+    with pytest.raises(ValueError):
+        prob.set_schedule("fast")
