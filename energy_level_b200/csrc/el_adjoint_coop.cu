@@ -11,7 +11,8 @@
 // pulse gradient runs on hold tens of thousands of rows, so the separate
 // launches of the stream path (about 3 K M of them) cost more than their
 // work.  Four lanes share a row (its flips split between them) as in
-// k_adjoint_step; every step's Chebyshev plan (a, b, M, c_m) is computed on
+// k_adjoint_step, and keep its flip targets in registers across all
+// sweeps; every step's Chebyshev plan (a, b, M, c_m) is computed on
 // the host first and read from device arrays.  Gradient dots go to per-CTA
 // slots [step][m][CTA] that the host adds up in a fixed order, so the
 // result does not depend on scheduling.  Grid-barrier waits are bounded: a
@@ -56,17 +57,17 @@ __device__ __forceinline__ void coop_sync(unsigned *bar, int *err, int nctas, in
   __syncthreads();
   gen += (unsigned)nctas;
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(bar, 1u);
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
     if (!*(volatile int *)err) {
       int polls = 0;
-      while (*(volatile unsigned *)bar < gen) {
+      unsigned v;
+      for (;;) {
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+        if (v >= gen) break;
         if (++polls > poll_limit) { atomicExch(err, 1); break; }
-        if (*(volatile int *)err) break;
-        __nanosleep(32);
+        if ((polls & 255) == 0 && *(volatile int *)err) break;
       }
     }
-    __threadfence();
   }
   __syncthreads();
 }
@@ -114,6 +115,45 @@ __device__ __forceinline__ void block_sum2(double a, double b, double *red, doub
   __syncthreads();
 }
 
+// A lane's share of its row when every row fits one pass of the grid (and
+// the row has at most 8 flips per lane): the row, the targets and
+// amplitudes of the lane's flips and the row's b-weighted occupation,
+// formed once for all sweeps and kept in registers -- ranking the row and
+// its flip targets again in every sweep cost more than the sweep's loads.
+template <typename S>
+struct RowCache {
+  int64_t r;
+  bool active;
+  int64_t tg[8];   // slot q: the flip of bit lane + CL q, -1 where blocked or absent
+  S amp[8];
+  S nb;
+};
+
+template <typename S>
+__device__ __forceinline__ void row_cache(const CoopAdj<S> &P, RowCache<S> &c) {
+  const int lane = threadIdx.x & (CL - 1);
+  const int64_t mine = (int64_t)blockIdx.x * (CNT / CL) + threadIdx.x / CL;
+  c.active = mine < P.B.dim;
+  c.r = c.active ? mine : 0;
+  const uint64_t code = el::unrank_row(P.B, c.r);
+  S nb = S(0);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int k = lane + CL * q;
+    c.tg[q] = -1;
+    c.amp[q] = S(0);
+    if (k >= P.B.n) continue;
+    if ((code >> k) & 1ULL) nb += P.bsh[k];
+    const S amp = P.ahalf[k];
+    if (amp == S(0)) continue;
+    c.tg[q] = el::flip_target(P.B, code, c.r, k);
+    c.amp[q] = amp;
+  }
+#pragma unroll
+  for (int off = CL / 2; off > 0; off >>= 1) nb += __shfl_xor_sync(0xffffffffu, nb, off);
+  c.nb = nb;
+}
+
 // One sweep over the basis:  y = alpha H_k x + beta x - z + conj-weighted
 // lambda (cl = (clr, cli)), with optional accumulation into acc (mode 1:
 // acc = w0 x + w y; mode 2: acc += w y) and optional gradient dots against t.
@@ -126,17 +166,38 @@ struct Sweep {
 };
 
 template <typename S>
-__device__ __forceinline__ void sweep(const CoopAdj<S> &P, S om, S dl, const Sweep<S> &W, double &gO, double &gD) {
+__device__ __forceinline__ void sweep(const CoopAdj<S> &P, S om, S dl, const Sweep<S> &W, double &gO, double &gD,
+                                      const RowCache<S> &rc, bool cached) {
   const int64_t dim = P.B.dim;
   const int lane = threadIdx.x & (CL - 1);
   const int64_t rpb = CNT / CL;
   for (int64_t base = (int64_t)blockIdx.x * rpb; base < dim; base += (int64_t)gridDim.x * rpb) {
-    const int64_t mine = base + threadIdx.x / CL;
-    const bool active = mine < dim;
-    const int64_t r = active ? mine : 0;
-    const uint64_t code = el::unrank_row(P.B, r);
+    int64_t r;
+    bool active;
     S sre, sim, nb;
-    row_flips<S>(P, code, r, lane, W.x, sre, sim, nb);
+    if (cached) {
+      r = rc.r;
+      active = rc.active;
+      sre = S(0); sim = S(0);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        if (rc.tg[q] < 0) continue;
+        sre += rc.amp[q] * W.x[2 * rc.tg[q]];
+        sim += rc.amp[q] * W.x[2 * rc.tg[q] + 1];
+      }
+#pragma unroll
+      for (int off = CL / 2; off > 0; off >>= 1) {
+        sre += __shfl_xor_sync(0xffffffffu, sre, off);
+        sim += __shfl_xor_sync(0xffffffffu, sim, off);
+      }
+      nb = rc.nb;
+    } else {
+      const int64_t mine = base + threadIdx.x / CL;
+      active = mine < dim;
+      r = active ? mine : 0;
+      const uint64_t code = el::unrank_row(P.B, r);
+      row_flips<S>(P, code, r, lane, W.x, sre, sim, nb);
+    }
     if (lane != 0 || !active) continue;
     const S xr = W.x[2 * r], xi = W.x[2 * r + 1];
     const S dsum = P.diagV[r] + dl * nb;
@@ -174,6 +235,11 @@ __global__ void __launch_bounds__(CNT) k_adjoint_coop(const CoopAdj<S> P) {
   unsigned gen = 0;
   auto sync = [&]() { coop_sync(P.bar, P.err, P.nctas, P.poll_limit, gen); };
   double g0 = 0.0, g1 = 0.0;
+  // rows cached per lane when one pass of the grid covers the basis (and no
+  // lane has more than 8 flips)
+  RowCache<S> cache;
+  const bool one_pass = dim <= (int64_t)gridDim.x * (CNT / CL) && P.B.n <= 8 * CL;
+  if (one_pass) row_cache<S>(P, cache);
   // ---- forward: psi_{k+1} = sum_m c_m T_m(Htil_k) psi_k
   for (int k = 0; k < P.K; ++k) {
     const S a = (S)P.pa[k], b = (S)P.pb[k];
@@ -186,7 +252,7 @@ __global__ void __launch_bounds__(CNT) k_adjoint_coop(const CoopAdj<S> P) {
     W.x = x0; W.y = P.term + vs; W.acc = out; W.acc_mode = 1;
     W.alpha = S(1) / a; W.beta = -b / a;
     W.w0r = (S)c[0]; W.w0i = (S)c[1]; W.wr = (S)c[2]; W.wi = (S)c[3];
-    sweep<S>(P, om, dl, W, g0, g1);
+    sweep<S>(P, om, dl, W, g0, g1, cache, one_pass);
     sync();
     for (int m = 2; m <= M; ++m) {
       Sweep<S> V{};
@@ -196,7 +262,7 @@ __global__ void __launch_bounds__(CNT) k_adjoint_coop(const CoopAdj<S> P) {
       V.acc = out; V.acc_mode = 2;
       V.alpha = S(2) / a; V.beta = S(-2) * b / a;
       V.wr = (S)c[2 * m]; V.wi = (S)c[2 * m + 1];
-      sweep<S>(P, om, dl, V, g0, g1);
+      sweep<S>(P, om, dl, V, g0, g1, cache, one_pass);
       sync();
     }
   }
@@ -253,7 +319,7 @@ __global__ void __launch_bounds__(CNT) k_adjoint_coop(const CoopAdj<S> P) {
       V.y = P.term + (size_t)m * vs;
       V.alpha = (m == 1 ? S(1) : S(2)) / a;
       V.beta = (m == 1 ? -b : S(-2) * b) / a;
-      sweep<S>(P, om, dl, V, g0, g1);
+      sweep<S>(P, om, dl, V, g0, g1, cache, one_pass);
       sync();
     }
     // u_M = conj(c_M) lambda
@@ -281,7 +347,7 @@ __global__ void __launch_bounds__(CNT) k_adjoint_coop(const CoopAdj<S> P) {
       V.alpha = s / a;
       V.beta = -s * b / a;
       double gO = 0.0, gD = 0.0;
-      sweep<S>(P, om, dl, V, gO, gD);
+      sweep<S>(P, om, dl, V, gO, gD, cache, one_pass);
       block_sum2(gO, gD, red, P.part + (((size_t)k * (P.Mmax + 1) + (m + 1)) * P.nctas + blockIdx.x) * 2);
       sync();
     }
