@@ -561,17 +561,19 @@ __device__ __forceinline__ void grid_barrier(const CoopArgs &G, unsigned &gen) {
   __syncthreads();
   gen += (unsigned)G.nctas;
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(G.bar, 1u);
+    // release this CTA's writes with the arrival, acquire the others' with
+    // the poll that sees the count complete
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(G.bar) : "memory");
     if (!*(volatile int *)G.err) {
       int polls = 0;
-      while (*(volatile unsigned *)G.bar < gen) {
+      unsigned v;
+      for (;;) {
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(G.bar) : "memory");
+        if (v >= gen) break;
         if (++polls > G.poll_limit) { atomicExch(G.err, 1); break; }
-        if (*(volatile int *)G.err) break;
-        __nanosleep(64);
+        if ((polls & 255) == 0 && *(volatile int *)G.err) break;
       }
     }
-    __threadfence();
   }
   __syncthreads();
 }
