@@ -1034,12 +1034,20 @@ def native_adjoint20(h, args):
                       "pulse_steps": len(tau), "T_ns": float(np.sum(tau)), "objective": "|<Z2|psi(T)>|^2",
                       "parameters": 2 * len(tau), "form": "adjoint through the Chebyshev steps, complex64, "
                       "terms recomputed per step", "l2": "dim 15,127: L2-resident (latency-bound)"})
-    # every launch of the gradient is counted as one sweep of a Chebyshev or
-    # reverse term over the basis (state, two recurrence vectors, adjoint,
-    # accumulator: 5 complex64 vectors and the FP32 diagonal) -- an estimate
-    rl = roofline(launches / steps * p32.basis.dim * (5 * 8 + 4), el / steps,
-                  kernel="k_apply_row / k_adjoint_step (estimate: every launch one term sweep)")
-    rl["note"] = "dim 15,127: L2-resident and launch-latency-bound"
+    # sweeps of one gradient: the launches of the launch-per-term schedule
+    # (each is one sweep of a Chebyshev or reverse term over the basis:
+    # state, two recurrence vectors, adjoint, accumulator -- 5 complex64
+    # vectors -- and the FP32 diagonal); the chosen schedule runs the same
+    # sweeps as phases of one cooperative launch
+    p32.set_schedule("stream")
+    l0 = h.ctx.launches
+    p32.evaluate(tau, om, Delta)
+    torch.cuda.synchronize()
+    sweeps = h.ctx.launches - l0
+    p32.set_schedule("auto")
+    rl = roofline(sweeps * p32.basis.dim * (5 * 8 + 4), el / steps,
+                  kernel="k_adjoint_coop (the whole gradient: %d sweeps as phases of one cooperative launch)" % sweeps)
+    rl["note"] = "dim 15,127: L2-resident, bound by the latency of a sweep and its grid barrier"
     line.update({
         "roofline": rl,
         "e2e": {"value": h.world / e2e_s, "unit": "grads/s",

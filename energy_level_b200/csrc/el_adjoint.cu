@@ -211,18 +211,27 @@ struct StepShapes { double a[EL_MAX_SITES], b[EL_MAX_SITES]; };   // by bit posi
 __global__ void k_step_bounds(BasisDev B, const double *__restrict__ diagV, StepShapes sh, int K,
                               const double *__restrict__ om, const double *__restrict__ dl, double *out) {
   __shared__ double lo_s[256], hi_s[256];
+  // with one row per thread (the pulse problems' small bases) the row's
+  // code and its allowed flips are found once for all steps
+  const bool one = B.dim <= (int64_t)gridDim.x * blockDim.x;
+  const int64_t r1 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t code1 = 0, flips1 = 0;
+  if (one && r1 < B.dim) {
+    code1 = el::unrank_row(B, r1);
+    for (int q = 0; q < B.n; ++q)
+      if (el::flip_target(B, code1, r1, q) >= 0) flips1 |= 1ULL << q;
+  }
   for (int k = 0; k < K; ++k) {
     const double o = om[k], d0 = dl[k];
     double lo = 1e300, hi = -1e300;
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < B.dim;
-         r += (int64_t)gridDim.x * blockDim.x) {
-      const uint64_t code = el::unrank_row(B, r);
+    for (int64_t r = r1; r < B.dim; r += (int64_t)gridDim.x * blockDim.x) {
+      const uint64_t code = one ? code1 : el::unrank_row(B, r);
       double d = diagV[r], R = 0.0;
       for (int q = 0; q < B.n; ++q) {
         if ((code >> q) & 1ULL) d += d0 * sh.b[q];
         const double amp = fabs(0.5 * (o * sh.a[q]));
         if (amp == 0.0) continue;
-        if (el::flip_target(B, code, r, q) >= 0) R += amp;
+        if (one ? ((flips1 >> q) & 1ULL) != 0 : el::flip_target(B, code, r, q) >= 0) R += amp;
       }
       lo = fmin(lo, d - R);
       hi = fmax(hi, d + R);
