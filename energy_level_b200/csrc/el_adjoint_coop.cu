@@ -227,7 +227,9 @@ __device__ __forceinline__ void sweep(const CoopAdj<S> &P, S om, S dl, const Swe
 }
 
 template <typename S>
-__global__ void __launch_bounds__(CNT) k_adjoint_coop(const CoopAdj<S> P) {
+// Two CTAs per SM (at most 128 registers): the pulse problems' bases then
+// fit one pass of the grid, which the register cache of the rows needs.
+__global__ void __launch_bounds__(CNT, 2) k_adjoint_coop(const CoopAdj<S> P) {
   __shared__ double red[2 * (CNT / 32)];
   __shared__ double s_ov[2];
   const int64_t dim = P.B.dim;
