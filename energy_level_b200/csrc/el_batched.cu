@@ -171,9 +171,9 @@ __device__ double last_component(const double *a, const double *b, int m, double
   return fabs(x[m - 1]);
 }
 
-__device__ __forceinline__ uint64_t unrank_b(const Inst &I, const uint64_t *fib, int64_t row) {
+// Code of a row by the layout's arithmetic (FULL, CHAIN, RING).
+__device__ __forceinline__ uint64_t unrank_arith(const Inst &I, const uint64_t *fib, int64_t row) {
   if (I.layout == EL_LAYOUT_FULL) return (uint64_t)row;
-  if (I.layout == EL_LAYOUT_TABLE) return I.codes[row];
   uint64_t r = (uint64_t)row, c = 0;
   const int n = I.n;
   if (I.layout == EL_LAYOUT_CHAIN) {
@@ -188,6 +188,14 @@ __device__ __forceinline__ uint64_t unrank_b(const Inst &I, const uint64_t *fib,
   c = 1ULL << (n - 1);
   for (int k = n - 3; k >= 1; --k) { const uint64_t w = fib[k + 1]; if (r >= w) { c |= 1ULL << k; r -= w; } }
   return c;
+}
+
+// Code of a row: from the instance's code list where it has one (TABLE
+// instances, and chain / ring sectors, whose codes are listed once at
+// set-up so that no Lanczos step ranks its rows again), else arithmetic.
+__device__ __forceinline__ uint64_t unrank_b(const Inst &I, const uint64_t *fib, int64_t row) {
+  if (I.codes) return I.codes[row];
+  return unrank_arith(I, fib, row);
 }
 
 __device__ __forceinline__ int64_t ring_rank(const uint64_t *fib, int n, uint64_t c) {
@@ -844,6 +852,23 @@ __global__ void __launch_bounds__(NT) k_lanczos_coop(const CoopArgs G) {
   }
 }
 
+// Code lists of the chain and ring instances (the arithmetic unranking, once).
+__global__ void k_batch_fill_codes(int count, const Inst *inst) {
+  __shared__ uint64_t fib[MAXN + 3];
+  if (threadIdx.x == 0) {
+    fib[0] = 0; fib[1] = 1;
+    for (int i = 2; i < MAXN + 3; ++i) fib[i] = fib[i - 1] + fib[i - 2];
+  }
+  __syncthreads();
+  for (int i = blockIdx.y; i < count; i += gridDim.y) {
+    const Inst &I = inst[i];
+    if (I.layout != EL_LAYOUT_CHAIN && I.layout != EL_LAYOUT_RING) continue;
+    uint64_t *out = const_cast<uint64_t *>(I.codes);
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < I.dim; r += (int64_t)gridDim.x * blockDim.x)
+      out[r] = unrank_arith(I, fib, r);
+  }
+}
+
 // Flip tables of the TABLE instances: target row of flipping bit k of row r,
 // found by binary search in the instance's ascending code list; -1 when bit
 // k is clear and one of its graph neighbours (adj, by bit position) is set.
@@ -935,6 +960,7 @@ struct el_batch_impl {
   // TABLE instances: concatenated ascending codes and flip tables
   uint64_t *d_codes = nullptr;
   int32_t *d_tgt = nullptr;
+  uint64_t *d_scodes = nullptr;     // chain / ring instances: codes in rank order
 };
 
 // Independent sets of a graph on n bit positions (adjb[k]: the neighbours
@@ -1068,10 +1094,12 @@ int el_batch_create_graph(el_ctx *ctx, int count, const int32_t *n_sites, const 
     b->dim_max = std::max(b->dim_max, dims[i]);
   }
   b->total_rows = off;
-  // TABLE instances: codes and flip tables, concatenated in processing order
-  int64_t tab_rows = 0, tab_cells = 0;
+  // TABLE instances: codes and flip tables; chain / ring instances: codes;
+  // concatenated in processing order
+  int64_t tab_rows = 0, tab_cells = 0, seq_rows = 0;
   for (int p = 0; p < count; ++p) {
     const int i = b->order[p];
+    if (layouts[i] == EL_LAYOUT_CHAIN || layouts[i] == EL_LAYOUT_RING) seq_rows += dims[i];
     if (layouts[i] != EL_LAYOUT_TABLE) continue;
     tab_rows += dims[i];
     tab_cells += dims[i] * n_sites[i];
@@ -1079,7 +1107,17 @@ int el_batch_create_graph(el_ctx *ctx, int count, const int32_t *n_sites, const 
   double *d_V = nullptr, *d_D = nullptr;
   uint64_t *d_adj = nullptr;
   cudaError_t e = cudaSuccess;
-  if (rc == EL_OK && tab_rows > 0) do {
+  if (rc == EL_OK && seq_rows > 0) do {
+    if ((e = cudaMalloc(&b->d_scodes, (size_t)seq_rows * 8)) != cudaSuccess) break;
+    int64_t so = 0;
+    for (int p = 0; p < count; ++p) {
+      const int i = b->order[p];
+      if (layouts[i] != EL_LAYOUT_CHAIN && layouts[i] != EL_LAYOUT_RING) continue;
+      inst[p].codes = b->d_scodes + so;
+      so += dims[i];
+    }
+  } while (0);
+  if (rc == EL_OK && e == cudaSuccess && tab_rows > 0) do {
     if ((e = cudaMalloc(&b->d_codes, (size_t)tab_rows * 8)) != cudaSuccess) break;
     if ((e = cudaMalloc(&b->d_tgt, (size_t)tab_cells * 4)) != cudaSuccess) break;
     std::vector<uint64_t> adjp((size_t)count * MAXN, 0);
@@ -1109,6 +1147,11 @@ int el_batch_create_graph(el_ctx *ctx, int count, const int32_t *n_sites, const 
     if ((e = el::copy(ctx, b->d_inst, inst.data(), sizeof(Inst) * count, cudaMemcpyHostToDevice)) != cudaSuccess) break;
     if ((e = el::copy(ctx, d_V, Vm.data(), Vm.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
     if ((e = el::copy(ctx, d_D, Dl.data(), Dl.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+    if (seq_rows > 0) {
+      k_batch_fill_codes<<<dim3(64, std::min(count, 1024)), 256, 0, ctx->stream>>>(count, b->d_inst);
+      ctx->launches++;
+      if ((e = cudaGetLastError()) != cudaSuccess) break;
+    }
     if (tab_rows > 0) {
       k_batch_flip_table<<<dim3(256, std::min(count, 1024)), 256, 0, ctx->stream>>>(count, b->d_inst, d_adj);
       ctx->launches++;
@@ -1330,6 +1373,7 @@ int el_batch_destroy(el_batch *b) {
   if (b->c_sync) cudaFree(b->c_sync);
   if (b->d_nat) cudaFree(b->d_nat);
   if (b->d_codes) cudaFree(b->d_codes);
+  if (b->d_scodes) cudaFree(b->d_scodes);
   if (b->d_tgt) cudaFree(b->d_tgt);
   delete b;
   return EL_OK;
