@@ -877,6 +877,26 @@ k_kpm_tx_a(const TmaArgs<float> A, const __grid_constant__ CUtensorMap mapP,
     }
     if (cur) { mbar_wait(&bar[1], par[1], A.err); par[1] ^= 1u; }
     else { mbar_wait(&bar[0], par[0], A.err); par[0] ^= 1u; }
+    // the diagonal of this thread's row-layout cells (FP64 sums, rounded
+    // once), formed here so that it overlaps the first gathers
+    T dvr[R];
+    {
+      const double *wH = wHt[cur];
+      double base = cT + wH[OTF_ROW - 1];
+      for (int x = 0; x < 9; ++x)
+        if ((tid >> x) & 1) base += wH[5 + x];
+      double u[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) u[k] = cTJ[k * NT + tid] + wH[k];
+#pragma unroll
+      for (int c = 0; c < R; ++c) {
+        double dj = base + tJ[c];
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+          if ((c >> k) & 1) dj += u[k];
+        dvr[c] = (T)fma(A.s2, dj, A.s2c);
+      }
+    }
 
     // ---- L1: s X_{5..13} t_{m-1} added into the p_m tile
     {
@@ -941,22 +961,9 @@ k_kpm_tx_a(const TmaArgs<float> A, const __grid_constant__ CUtensorMap mapP,
       if (tid == 0) { tile_store_swz(&mapP, tile, g, S2); bulk_commit(); }
       // ---- L2: p_{m+1} partial = d2 t_m - t_{m-1} + (2/r) X_{0..4} t_m over t_{m-1}
       {
-        const double *wH = wHt[cur];
-        double base = cT + wH[OTF_ROW - 1];
-        for (int x = 0; x < 9; ++x)
-          if ((tid >> x) & 1) base += wH[5 + x];
-        double u[5];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) u[k] = cTJ[k * NT + tid] + wH[k];
         // o2 (t_{m-1}) becomes the p_{m+1} partial in place
 #pragma unroll
-        for (int c = 0; c < R; ++c) {
-          double dj = base + tJ[c];
-#pragma unroll
-          for (int k = 0; k < 5; ++k)
-            if ((c >> k) & 1) dj += u[k];
-          o2[c] = fmaf((T)fma(A.s2, dj, A.s2c), t2[c], -o2[c]);
-        }
+        for (int c = 0; c < R; ++c) o2[c] = fmaf(dvr[c], t2[c], -o2[c]);
 #pragma unroll
         for (int b = 0; b < 5; ++b) {
           const T a = A.amp[b] * A.two_r;
